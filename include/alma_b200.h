@@ -1,0 +1,206 @@
+/*
+ * alma_b200.h — C ABI of the B200-native ALMA nonbonded-energy / MC-ΔE engine.
+ *
+ * Plain pointers and sizes only.  Every device pointer is caller-allocated
+ * device memory; every call is asynchronous on the given CUDA stream
+ * (passed as void*, a cudaStream_t) unless its comment says otherwise.
+ * Every entry point returns 0 on success or a negative ALMA_E* code;
+ * alma_last_error() returns a thread-local message for the last failure.
+ *
+ * Reference interfaces replaced (noira-913/Protein-Structure-Analysis):
+ *   src/physics_engine.cpp      — CPU engine, module `protein_physics`
+ *   src/physics_engine_cuda.cu  — CUDA engine, module `protein_physics_cuda`
+ * The reference binds these through pybind11 (physics_engine.cpp:3692-3888,
+ * physics_engine_cuda.cu:1287-1396); the Python package protein_physics_b200
+ * re-exposes the same Python surface over this ABI.
+ *
+ * Batched layout: a batch holds `nsys` independent systems (chains or
+ * replicas) concatenated atom-wise; atom_off[nsys+1] gives each system's
+ * first atom.  All atom indices in topology / neighbor arrays are global
+ * (batch) indices.  A single chain is a batch with nsys = 1.
+ */
+#ifndef ALMA_B200_H
+#define ALMA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ALMA_ABI_VERSION 1
+
+enum {
+    ALMA_OK = 0,
+    ALMA_EINVAL = -1,    /* bad argument (null pointer, size, index)       */
+    ALMA_ECUDA = -2,     /* CUDA runtime error                             */
+    ALMA_ECAPACITY = -3, /* caller buffer too small (see the call's doc)   */
+    ALMA_EDEVICE = -4,   /* device-side status flag set (see alma_status)  */
+    ALMA_ENODEV = -5     /* no usable sm_100 device                        */
+};
+
+/* Precision of the pair arithmetic.  Accumulations (Born-radius integral,
+ * energies, ΔE) and the Metropolis test are FP64 in both modes; pair
+ * distances and the 12 Å / 14 Å cutoff tests are always FP64. */
+enum { ALMA_PREC_MIXED = 0, ALMA_PREC_FP64 = 1 };
+
+/* Device status word bits (AlmaBatch.status): sticky error flags. */
+enum {
+    ALMA_ST_NL_OVERFLOW = 1,    /* neighbor list exceeded its capacity       */
+    ALMA_ST_CELL_OVERFLOW = 2,  /* cell grid exceeded its capacity           */
+    ALMA_ST_BAD_INDEX = 4,      /* topology index out of range               */
+    ALMA_ST_NONFINITE = 8       /* non-finite coordinate or energy seen      */
+};
+
+/* Energy-model constants (physics_engine.cpp:181-196).  Passed by value;
+ * alma_params_reference() fills the reference preset. */
+typedef struct {
+    double coulomb, eps_water, eps_prot, kappa;
+    double gamma_sa, beta_sa, probe_r;
+    double pair_cut2;          /* 12 Å squared: pair terms use r² <= this   */
+    double nl_rcut2;           /* 14 Å squared: list membership r² < this   */
+    double half_skin2;         /* drift² that triggers a rebuild            */
+    double hard_scale, hard_cap, hard_frac;
+    double k_ss, r0_ss;
+} AlmaParams;
+
+/* A batch of systems resident on the device (all pointers device memory). */
+typedef struct {
+    int32_t nsys;
+    int32_t natoms;
+    const int32_t *atom_off; /* [nsys+1]                                    */
+    double *xyz;             /* [natoms*4] FP64 x,y,z,(unused)              */
+    const float *prm;        /* [natoms*4] charge, R*, epsilon, (unused)    */
+    const double *prm64;     /* [natoms*4] charge, R*, epsilon, (unused)    */
+    double *born;            /* [natoms] effective Born radii               */
+    uint32_t *status;        /* [1] sticky ALMA_ST_* flags                  */
+} AlmaBatch;
+
+/* Flat topology of the batch (physics_engine.cpp:3746-3841 exports). */
+typedef struct {
+    const int64_t *excl_ptr;  /* [natoms+1] 1-2/1-3/SS exclusions, j > i    */
+    const int32_t *excl_cols;
+    int32_t nrb;              /* rotatable bonds, all systems               */
+    const int32_t *rb_off;    /* [nsys+1]                                   */
+    const int32_t *rb_ij;     /* [nrb*2] axis atoms                         */
+    const int32_t *rb_kind;   /* [nrb] 0 phi, 1 psi, 2 sidechain, 3 fixed   */
+    const double *rb_scale;   /* [nrb] lever-arm scale                      */
+    const int64_t *side_ptr;  /* [nrb+1] j-side: explicit atoms, sorted     */
+    const int32_t *side_idx;
+    const int32_t *side_lo;   /* [nrb] j-side: plus the atom range [lo, hi) */
+    const int32_t *side_hi;
+    int32_t ndih;
+    const int32_t *dih_off;   /* [nsys+1]                                   */
+    const int32_t *dih_abcd;  /* [ndih*4]                                   */
+    const int32_t *term_off;  /* [ndih+1]                                   */
+    const double *term_v2;
+    const int32_t *term_n;
+    const double *term_gamma;
+    int32_t nss;
+    const int32_t *ss_off;    /* [nsys+1]                                   */
+    const int32_t *ss_ij;     /* [nss*2]                                    */
+    int32_t ncp;
+    const int32_t *cp_off;    /* [nsys+1] crankshaft pairs                  */
+    const int32_t *cp;        /* [ncp*2] (phi rot bond, psi rot bond)        */
+    int32_t ncsp;
+    const int32_t *csp_off;   /* [nsys+1] concerted sidechain pairs         */
+    const int32_t *csp;       /* [ncsp*2]                                   */
+} AlmaTopo;
+
+/* Neighbor list: for every atom a full row (all j != i with r² < 14²) and
+ * a half row (j > i), both in the reference's cell-scan order
+ * (NeighborList::build, physics_engine.cpp:293-342).  Row i occupies
+ * cols[ptr[i] .. ptr[i]+len[i]).  Each system owns the region
+ * [base[s], base[s+1]) of the column arrays, so one system can be rebuilt
+ * without touching the others.  Column entries carry the exclusion flag in
+ * bit 31 (atom index = entry & 0x7fffffff).  need[2*s+0/1] receives the
+ * full/half entry counts of system s at its last build; when a count
+ * exceeds the region, the rows of that system are not written and
+ * ALMA_ST_NL_OVERFLOW is raised. */
+typedef struct {
+    int64_t *full_ptr;        /* [natoms] */
+    int32_t *full_len;        /* [natoms] */
+    uint32_t *full_cols;      /* [full_base[nsys]] */
+    const int64_t *full_base; /* [nsys+1] */
+    int64_t *half_ptr;        /* [natoms] */
+    int32_t *half_len;        /* [natoms] */
+    uint32_t *half_cols;      /* [half_base[nsys]] */
+    const int64_t *half_base; /* [nsys+1] */
+    double *ref_xyz;          /* [natoms*4] positions at the last build     */
+    int64_t *need;            /* [nsys*2]                                   */
+} AlmaNL;
+
+/* ---- library ------------------------------------------------------------ */
+int alma_abi_version(void);
+const char *alma_last_error(void);
+/* Reference preset (P1: 0.6 sigma smooth capped hard core, gamma 0.00542). */
+void alma_params_reference(AlmaParams *p);
+/* Bytes of device workspace alma_nl_build needs for a batch. */
+size_t alma_nl_workspace_bytes(int32_t nsys, int32_t natoms, int64_t max_cells);
+
+/* ---- host topology helper ------------------------------------------------ */
+/* j_side for each bond (bi, bj): atoms reached by a DFS from bj that never
+ * enters bi, listed in DFS visiting order (BondTopology::j_side,
+ * physics_engine.cpp:1731-1745).  Host memory.  side_ptr[nb+1]; returns
+ * ALMA_ECAPACITY when cap < total (side_ptr still filled). */
+int alma_topo_sides(int32_t n, const int64_t *adj_ptr, const int32_t *adj_idx, int32_t nb,
+                    const int32_t *bonds, int64_t *side_ptr, int32_t *side_idx, int64_t cap);
+/* The same sets in the engine's compact form: the longest run of
+ * consecutive atom indices [lo[b], hi[b]) plus the other atoms, sorted, in
+ * (ex_ptr[nb+1], ex_idx); count[b] = set size.  ALMA_ECAPACITY when
+ * ex_cap < total explicit atoms (ex_ptr still filled). */
+int alma_topo_sides_compact(int32_t n, const int64_t *adj_ptr, const int32_t *adj_idx, int32_t nb,
+                            const int32_t *bonds, int32_t *lo, int32_t *hi, int64_t *count,
+                            int64_t *ex_ptr, int32_t *ex_idx, int64_t ex_cap);
+
+/* ---- device kernels ------------------------------------------------------ */
+/* Neighbor list for every system of the batch (replaces
+ * NeighborList::build, physics_engine.cpp:293-342).  sys_mask: device
+ * uint8[nsys]; only systems with a nonzero entry are rebuilt (NULL: all).
+ * workspace: device scratch of alma_nl_workspace_bytes(nsys, natoms,
+ * max_cells) bytes. */
+int alma_nl_build(const AlmaBatch *b, const AlmaTopo *t, AlmaNL *nl, const uint8_t *sys_mask,
+                  void *workspace, int64_t max_cells, void *stream);
+
+/* Effective Born radii over the full rows (replaces born_radii,
+ * physics_engine.cpp:2024-2039, and born_sum/born_finalize kernels,
+ * physics_engine_cuda.cu:537-578).  Writes b->born. */
+int alma_born_radii(const AlmaBatch *b, const AlmaNL *nl, const AlmaParams *p, int prec,
+                    void *stream);
+
+/* Per-system energy terms (replaces total_e / calculate_potential,
+ * physics_engine.cpp:2205-2248, and pair_energy_kernel,
+ * physics_engine_cuda.cu:587-617).  terms: device double[nsys*5] =
+ * {sasa, dihedral, disulfide, pair sum, total} per system.  t may be NULL
+ * (no exclusions / dihedrals / disulfides).  atom_e: optional device
+ * double[natoms] scratch (NULL: allocated internally per call is NOT done —
+ * it must be given). */
+int alma_energy(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *nl, const AlmaParams *p,
+                int prec, double *atom_e, double *terms, void *stream);
+
+/* Device scratch for the move / MC kernels: alma_move_scratch_bytes(natoms)
+ * bytes, zeroed once by alma_move_scratch_init; every call leaves it zeroed.
+ * Calls that share a scratch buffer must not overlap on the GPU. */
+size_t alma_move_scratch_bytes(int32_t natoms);
+int alma_move_scratch_init(void *scratch, int32_t natoms, void *stream);
+
+/* ΔE of one proposal per system, replayed for a given move (the ΔE core of
+ * try_torsion / try_crankshaft / the concerted sidechain move,
+ * physics_engine.cpp:2328-2501, :2798-2878; cross_pair_energy_kernel,
+ * physics_engine_cuda.cu:629-661).  move_kind[s]: 0 torsion (move_a =
+ * rot-bond index within system s), 1 crankshaft (move_a = crank-pair
+ * index), 2 concerted sidechain (move_a = pair index), -1 none.
+ * move_delta[2*s+0..1]: angle(s) in radians (the second is used by kind 2).
+ * Outputs per system: dE[s], dterms[4*s..] = {Δcross, Δsasa, Δdih, Δss};
+ * NaN for a degenerate proposal (empty side, zero-length axis).  When
+ * apply != 0 the proposal is committed (coordinates and Born radii of the
+ * moved atoms), as an accepted Metropolis step would.  Device arrays. */
+int alma_move_dE(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *nl, const AlmaParams *p,
+                 int prec, void *scratch, const int32_t *move_kind, const int32_t *move_a,
+                 const double *move_delta, int apply, double *dE, double *dterms, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ALMA_B200_H */

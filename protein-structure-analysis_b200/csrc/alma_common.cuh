@@ -1,0 +1,199 @@
+// Shared device code of the ALMA B200 engine: constants, pair arithmetic,
+// the Philox counter RNG, warp/block reductions, error plumbing.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "alma_b200.h"
+
+#define ALMA_WARP 32
+#define ALMA_EXCL_BIT 0x80000000u
+#define ALMA_IDX_MASK 0x7fffffffu
+
+// ---------------------------------------------------------------------------
+// host-side error state (alma_host.cpp)
+// ---------------------------------------------------------------------------
+int alma_set_error(int code, const char *fmt, ...);
+int alma_cuda_error(cudaError_t e, const char *what);
+
+#define ALMA_CUDA_TRY(expr)                                        \
+    do {                                                           \
+        cudaError_t _e = (expr);                                   \
+        if (_e != cudaSuccess) return alma_cuda_error(_e, #expr);  \
+    } while (0)
+
+#define ALMA_LAUNCH_CHECK(what)                                        \
+    do {                                                               \
+        cudaError_t _e = cudaGetLastError();                           \
+        if (_e != cudaSuccess) return alma_cuda_error(_e, what);       \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// energy model (physics_engine.cpp:181-196, :2007-2011, :2148-2164)
+// ---------------------------------------------------------------------------
+struct DevParams {
+    double coulomb_over_epsw;  // COULOMB / EPS_WATER
+    double kappa;
+    double gb_coef;            // -0.5 (1/eps_prot - 1/eps_water) COULOMB
+    double gamma_sa, beta_sa, probe_r;
+    double pair_cut2, nl_rcut2, half_skin2;
+    double hard_scale, hard_cap, hard_frac;
+    double k_ss, r0_ss;
+};
+
+inline DevParams make_dev_params(const AlmaParams &p) {
+    DevParams d;
+    d.coulomb_over_epsw = p.coulomb / p.eps_water;
+    d.kappa = p.kappa;
+    d.gb_coef = -0.5 * (1.0 / p.eps_prot - 1.0 / p.eps_water) * p.coulomb;
+    d.gamma_sa = p.gamma_sa;
+    d.beta_sa = p.beta_sa;
+    d.probe_r = p.probe_r;
+    d.pair_cut2 = p.pair_cut2;
+    d.nl_rcut2 = p.nl_rcut2;
+    d.half_skin2 = p.half_skin2;
+    d.hard_scale = p.hard_scale;
+    d.hard_cap = p.hard_cap;
+    d.hard_frac = p.hard_frac;
+    d.k_ss = p.k_ss;
+    d.r0_ss = p.r0_ss;
+    return d;
+}
+
+// Math shims so the pair code is written once for float and double.  The
+// float versions are CUDA's accurate single-precision functions (no
+// fast-math intrinsics); division and sqrt are IEEE-rounded.
+__device__ __forceinline__ float m_exp(float x) { return expf(x); }
+__device__ __forceinline__ double m_exp(double x) { return exp(x); }
+__device__ __forceinline__ float m_log(float x) { return logf(x); }
+__device__ __forceinline__ double m_log(double x) { return log(x); }
+__device__ __forceinline__ float m_sqrt(float x) { return sqrtf(x); }
+__device__ __forceinline__ double m_sqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float m_abs(float x) { return fabsf(x); }
+__device__ __forceinline__ double m_abs(double x) { return fabs(x); }
+
+// One nonbonded pair: Debye-Hückel + GB + LJ 12-6 + smooth capped hard core.
+// r2 is the FP64 squared distance (rounded to R); q = qi*qj product; the
+// caller has already applied the exclusion and 12 Å tests.
+template <typename R>
+__device__ __forceinline__ R pair_energy(const DevParams &P, R r2, R qp, R sig, R eps_prod,
+                                         R ai, R aj) {
+    const R r = m_sqrt(r2);
+    const R edh = (R)P.coulomb_over_epsw * qp / r * m_exp(-(R)P.kappa * r);
+    const R aa = ai * aj;
+    const R fgb = m_sqrt(r2 + aa * m_exp(-r2 / ((R)4 * aa)));
+    const R egb = (R)P.gb_coef * qp / fgb;
+    const R eps = m_sqrt(eps_prod);
+    const R sr = sig / r;
+    const R s2 = sr * sr;
+    const R s6 = s2 * s2 * s2;
+    R E = edh + egb + (R)4 * eps * (s6 * s6 - s6);
+    const R r_cut = sig * (R)P.hard_frac;
+    if (r < r_cut) {
+        const R t = r_cut / r;
+        const R t2 = t * t;
+        const R t6 = t2 * t2 * t2;
+        const R x = t6 * t6 - (R)1;
+        const R h = (R)P.hard_scale * x * x;
+        E += h < (R)P.hard_cap ? h : (R)P.hard_cap;
+    }
+    return E;
+}
+
+// HCT descreening integral of atom j (radius rj) on atom i (radius ri).
+template <typename R>
+__device__ __forceinline__ R hct_term(R r, R r2, R ri, R rj) {
+    const R d = m_abs(r - rj);
+    const R L = d > ri ? d : ri;
+    const R U = r + rj;
+    if (ri >= U) return (R)0;
+    return (R)1 / L - (R)1 / U + (r2 - rj * rj + ri * ri) / ((R)2 * r * ri * ri) * m_log(L / U) * (R)0.5 / r;
+}
+
+__device__ __forceinline__ double dist2(const double *xyz, int i, int j) {
+    const double4 a = *reinterpret_cast<const double4 *>(xyz + 4 * (size_t)i);
+    const double4 b = *reinterpret_cast<const double4 *>(xyz + 4 * (size_t)j);
+    const double dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
+    return dx * dx + dy * dy + dz * dz;
+}
+
+__device__ __forceinline__ double4 ld_xyz(const double *xyz, int i) {
+    return *reinterpret_cast<const double4 *>(xyz + 4 * (size_t)i);
+}
+
+__device__ __forceinline__ double d2_of(double4 a, double4 b) {
+    const double dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
+    return dx * dx + dy * dy + dz * dz;
+}
+
+// ---------------------------------------------------------------------------
+// reductions (fixed order: deterministic for a given launch shape)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Block-wide sum; every thread gets the result.  smem: >= 32 doubles.
+__device__ __forceinline__ double block_sum(double v, double *smem) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    v = warp_sum(v);
+    __syncthreads();
+    if (lane == 0) smem[wid] = v;
+    __syncthreads();
+    double t = (threadIdx.x < (unsigned)nw) ? smem[threadIdx.x] : 0.0;
+    if (wid == 0) t = warp_sum(t);
+    if (threadIdx.x == 0) smem[0] = t;
+    __syncthreads();
+    t = smem[0];
+    __syncthreads();
+    return t;
+}
+
+// ---------------------------------------------------------------------------
+// Philox4x32-10 counter-based RNG (Salmon, Moraes, Dror, Shaw, "Parallel
+// random numbers: as easy as 1, 2, 3", SC'11).  Written from the published
+// round function; the oracle's MC driver carries the same restatement.
+// ---------------------------------------------------------------------------
+struct Philox4 {
+    uint32_t v[4];
+};
+
+__host__ __device__ __forceinline__ void philox_mulhilo(uint32_t a, uint32_t b, uint32_t &hi, uint32_t &lo) {
+    const uint64_t p = (uint64_t)a * (uint64_t)b;
+    hi = (uint32_t)(p >> 32);
+    lo = (uint32_t)p;
+}
+
+__host__ __device__ __forceinline__ Philox4 philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
+                                                           uint32_t k0, uint32_t k1) {
+    const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u, W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+    for (int r = 0; r < 10; ++r) {
+        uint32_t hi0, lo0, hi1, lo1;
+        philox_mulhilo(M0, c0, hi0, lo0);
+        philox_mulhilo(M1, c2, hi1, lo1);
+        const uint32_t n0 = hi1 ^ c1 ^ k0, n1 = lo1, n2 = hi0 ^ c3 ^ k1, n3 = lo0;
+        c0 = n0; c1 = n1; c2 = n2; c3 = n3;
+        k0 += W0; k1 += W1;
+    }
+    Philox4 o;
+    o.v[0] = c0; o.v[1] = c1; o.v[2] = c2; o.v[3] = c3;
+    return o;
+}
+
+// 53-bit uniform double in [0, 1) from two 32-bit words.
+__host__ __device__ __forceinline__ double u01_from(uint32_t a, uint32_t b) {
+    return (double)(((uint64_t)(a >> 5) << 26) | (uint64_t)(b >> 6)) * (1.0 / 9007199254740992.0);
+}
+
+__device__ __forceinline__ void set_status(uint32_t *status, uint32_t bit) {
+    if (status) atomicOr(status, bit);
+}

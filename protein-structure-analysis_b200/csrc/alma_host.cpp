@@ -1,0 +1,151 @@
+// Host-side pieces of the C ABI: error state, parameter presets, and the
+// topology j-side walk.
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <algorithm>
+#include <vector>
+
+#include "alma_b200.h"
+
+namespace {
+thread_local char g_err[512] = "";
+}
+
+int alma_set_error(int code, const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+int alma_cuda_error(cudaError_t e, const char *what) {
+    return alma_set_error(ALMA_ECUDA, "%s: %s (%s)", what, cudaGetErrorName(e), cudaGetErrorString(e));
+}
+
+extern "C" {
+
+int alma_abi_version(void) { return ALMA_ABI_VERSION; }
+
+const char *alma_last_error(void) { return g_err; }
+
+// Reference preset: physics_engine.cpp:181-196 (hard core 0.6 sigma, smooth
+// and capped at 5000, gamma_SA 0.00542, kappa 0.1257) and the disulfide
+// restraint constants at :1948-1950.
+void alma_params_reference(AlmaParams *p) {
+    p->coulomb = 332.0636;
+    p->eps_water = 78.5;
+    p->eps_prot = 1.0;
+    p->kappa = 0.1257;
+    p->gamma_sa = 0.00542;
+    p->beta_sa = 0.92;
+    p->probe_r = 1.4;
+    p->pair_cut2 = 12.0 * 12.0;
+    p->nl_rcut2 = (12.0 + 2.0) * (12.0 + 2.0);
+    p->half_skin2 = (2.0 * 0.5) * (2.0 * 0.5);
+    p->hard_scale = 1.0e4;
+    p->hard_cap = 5.0e3;
+    p->hard_frac = 0.6;
+    p->k_ss = 600.0;
+    p->r0_ss = 2.044;
+}
+
+// DFS from bj that never enters bi; stack order as BondTopology::j_side
+// (physics_engine.cpp:1731-1745): pop the top, skip if visited, record,
+// push all neighbours in adjacency order.
+int alma_topo_sides(int32_t n, const int64_t *adj_ptr, const int32_t *adj_idx, int32_t nb,
+                    const int32_t *bonds, int64_t *side_ptr, int32_t *side_idx, int64_t cap) {
+    if (n < 0 || nb < 0 || !adj_ptr || (nb > 0 && (!bonds || !side_ptr)))
+        return alma_set_error(ALMA_EINVAL, "alma_topo_sides: bad arguments");
+    std::vector<uint32_t> stamp((size_t)n, 0u);
+    std::vector<int32_t> stk;
+    stk.reserve(64);
+    int64_t k = 0;
+    side_ptr[0] = 0;
+    for (int32_t b = 0; b < nb; ++b) {
+        const int32_t bi = bonds[2 * b], bj = bonds[2 * b + 1];
+        const uint32_t mark = (uint32_t)b + 1u;
+        if (bi < 0 || bi >= n || bj < 0 || bj >= n) {
+            side_ptr[b + 1] = k;
+            continue;
+        }
+        stamp[(size_t)bi] = mark;
+        stk.clear();
+        stk.push_back(bj);
+        while (!stk.empty()) {
+            int32_t cur = stk.back();
+            stk.pop_back();
+            if (stamp[(size_t)cur] == mark) continue;
+            stamp[(size_t)cur] = mark;
+            if (k < cap && side_idx) side_idx[k] = cur;
+            ++k;
+            for (int64_t e = adj_ptr[cur]; e < adj_ptr[cur + 1]; ++e) stk.push_back(adj_idx[e]);
+        }
+        side_ptr[b + 1] = k;
+    }
+    if (k > cap) return alma_set_error(ALMA_ECAPACITY, "alma_topo_sides: need %lld entries", (long long)k);
+    return ALMA_OK;
+}
+
+// Same walk, compact output: each side as its longest run of consecutive
+// atom indices [lo, hi) plus the remaining atoms, sorted, in the CSR
+// (ex_ptr, ex_idx).  count[b] = side size.  For residue-ordered chains a
+// backbone side is a handful of explicit atoms plus one long range.
+int alma_topo_sides_compact(int32_t n, const int64_t *adj_ptr, const int32_t *adj_idx, int32_t nb,
+                            const int32_t *bonds, int32_t *lo_out, int32_t *hi_out, int64_t *count,
+                            int64_t *ex_ptr, int32_t *ex_idx, int64_t ex_cap) {
+    if (n < 0 || nb < 0 || !adj_ptr || (nb > 0 && (!bonds || !lo_out || !hi_out || !count || !ex_ptr)))
+        return alma_set_error(ALMA_EINVAL, "alma_topo_sides_compact: bad arguments");
+    std::vector<uint32_t> stamp((size_t)n, 0u);
+    std::vector<int32_t> stk, side;
+    int64_t k = 0;
+    ex_ptr[0] = 0;
+    for (int32_t b = 0; b < nb; ++b) {
+        const int32_t bi = bonds[2 * b], bj = bonds[2 * b + 1];
+        const uint32_t mark = (uint32_t)b + 1u;
+        side.clear();
+        if (bi >= 0 && bi < n && bj >= 0 && bj < n) {
+            stamp[(size_t)bi] = mark;
+            stk.clear();
+            stk.push_back(bj);
+            while (!stk.empty()) {
+                int32_t cur = stk.back();
+                stk.pop_back();
+                if (stamp[(size_t)cur] == mark) continue;
+                stamp[(size_t)cur] = mark;
+                side.push_back(cur);
+                for (int64_t e = adj_ptr[cur]; e < adj_ptr[cur + 1]; ++e) stk.push_back(adj_idx[e]);
+            }
+        }
+        std::sort(side.begin(), side.end());
+        // longest run of consecutive indices
+        size_t best_b = 0, best_len = 0;
+        for (size_t s0 = 0; s0 < side.size();) {
+            size_t s1 = s0 + 1;
+            while (s1 < side.size() && side[s1] == side[s1 - 1] + 1) ++s1;
+            if (s1 - s0 > best_len) { best_len = s1 - s0; best_b = s0; }
+            s0 = s1;
+        }
+        count[b] = (int64_t)side.size();
+        if (best_len >= 2) {
+            lo_out[b] = side[best_b];
+            hi_out[b] = side[best_b] + (int32_t)best_len;
+        } else {
+            lo_out[b] = hi_out[b] = 0;
+            best_len = 0;
+        }
+        for (size_t s0 = 0; s0 < side.size(); ++s0) {
+            if (best_len && s0 >= best_b && s0 < best_b + best_len) continue;
+            if (k < ex_cap && ex_idx) ex_idx[k] = side[s0];
+            ++k;
+        }
+        ex_ptr[b + 1] = k;
+    }
+    if (k > ex_cap) return alma_set_error(ALMA_ECAPACITY, "alma_topo_sides_compact: need %lld entries", (long long)k);
+    return ALMA_OK;
+}
+
+}  // extern "C"

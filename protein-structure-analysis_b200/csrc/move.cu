@@ -1,0 +1,110 @@
+// Move ΔE entry point: one given proposal per system, one CTA per system.
+#include "move.cuh"
+
+namespace alma {
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+static size_t carve_scratch(MoveScratch *w, char *base, int32_t natoms) {
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        char *p = base ? base + off : nullptr;
+        off += align256(bytes);
+        return p;
+    };
+    MoveScratch t;
+    t.group = (int8_t *)take((size_t)natoms);
+    t.mark = (uint8_t *)take((size_t)natoms);
+    t.xyz_new = (double *)take(sizeof(double) * 4 * (size_t)natoms);
+    t.born_new = (double *)take(sizeof(double) * (size_t)natoms);
+    t.dE_atom = (double *)take(sizeof(double) * 2 * (size_t)natoms);
+    t.affected = (int32_t *)take(sizeof(int32_t) * (size_t)natoms);
+    if (w) *w = t;
+    return off;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(MOVE_THREADS) move_dE_kernel(MoveCtx C, const int32_t *__restrict__ kind,
+                                                               const int32_t *__restrict__ a,
+                                                               const double *__restrict__ delta, int apply,
+                                                               double *__restrict__ dE, double *__restrict__ dterms) {
+    __shared__ MoveDesc M;
+    __shared__ double sm[32];
+    __shared__ int naff;
+    const int s = blockIdx.x;
+    const int k = kind[s];
+    if (threadIdx.x == 0) {
+        if (k >= 0) decode_move(M, C.t, C.b.xyz, s, k, a[s], delta + 2 * (size_t)s);
+        else M.degenerate = 1;
+    }
+    __syncthreads();
+    if (M.degenerate) {
+        if (threadIdx.x == 0) {
+            const double nan = __longlong_as_double(0x7ff8000000000000ll);
+            dE[s] = nan;
+            for (int q = 0; q < 4; ++q) dterms[4 * (size_t)s + q] = nan;
+        }
+        return;
+    }
+    const MoveResult r = move_eval<R>(C, M, s, sm, &naff);
+    if (threadIdx.x == 0) {
+        dE[s] = r.dE;
+        dterms[4 * (size_t)s + 0] = r.dcross;
+        dterms[4 * (size_t)s + 1] = r.dsasa;
+        dterms[4 * (size_t)s + 2] = r.ddih;
+        dterms[4 * (size_t)s + 3] = r.dss;
+    }
+    move_finish(C, M, s, &naff, apply);
+}
+
+}  // namespace alma
+
+using namespace alma;
+
+extern "C" size_t alma_move_scratch_bytes(int32_t natoms) { return carve_scratch(nullptr, nullptr, natoms); }
+
+extern "C" int alma_move_scratch_init(void *scratch, int32_t natoms, void *stream) {
+    if (!scratch || natoms < 0) return alma_set_error(ALMA_EINVAL, "alma_move_scratch_init: bad arguments");
+    ALMA_CUDA_TRY(cudaMemsetAsync(scratch, 0, carve_scratch(nullptr, nullptr, natoms), (cudaStream_t)stream));
+    return ALMA_OK;
+}
+
+int alma_check_move_args(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *nl, const AlmaParams *p,
+                         void *scratch, const char *who) {
+    if (!b || !t || !nl || !p || !scratch || b->nsys <= 0 || !b->atom_off || !b->xyz || !b->prm || !b->prm64 ||
+        !b->born)
+        return alma_set_error(ALMA_EINVAL, "%s: null argument", who);
+    if (!nl->full_ptr || !nl->full_len || !nl->full_cols || !nl->half_ptr || !nl->half_len || !nl->half_cols)
+        return alma_set_error(ALMA_EINVAL, "%s: neighbor list not set", who);
+    if (!t->rb_off || !t->side_ptr || !t->dih_off || !t->ss_off || !t->cp_off || !t->csp_off)
+        return alma_set_error(ALMA_EINVAL, "%s: topology offsets not set", who);
+    return ALMA_OK;
+}
+
+MoveCtx alma_make_move_ctx(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *nl, const AlmaParams *p,
+                           void *scratch) {
+    MoveCtx C;
+    C.P = make_dev_params(*p);
+    C.b = *b;
+    C.t = *t;
+    C.nl = *nl;
+    carve_scratch(&C.w, (char *)scratch, b->natoms);
+    return C;
+}
+
+extern "C" int alma_move_dE(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *nl, const AlmaParams *p, int prec,
+                            void *scratch, const int32_t *move_kind, const int32_t *move_a, const double *move_delta,
+                            int apply, double *dE, double *dterms, void *stream) {
+    int rc = alma_check_move_args(b, t, nl, p, scratch, "alma_move_dE");
+    if (rc) return rc;
+    if (!move_kind || !move_a || !move_delta || !dE || !dterms)
+        return alma_set_error(ALMA_EINVAL, "alma_move_dE: null move buffer");
+    const MoveCtx C = alma_make_move_ctx(b, t, nl, p, scratch);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (prec == ALMA_PREC_FP64)
+        move_dE_kernel<double><<<b->nsys, MOVE_THREADS, 0, st>>>(C, move_kind, move_a, move_delta, apply, dE, dterms);
+    else
+        move_dE_kernel<float><<<b->nsys, MOVE_THREADS, 0, st>>>(C, move_kind, move_a, move_delta, apply, dE, dterms);
+    ALMA_LAUNCH_CHECK("alma_move_dE");
+    return ALMA_OK;
+}

@@ -1,0 +1,443 @@
+// ΔE of one torsion-space proposal, evaluated by one CTA for one system.
+//
+// Semantics follow the reference proposal core (try_torsion,
+// physics_engine.cpp:2328-2399; try_crankshaft :2407-2501; concerted
+// sidechain move :2798-2878):
+//   ΔE = Δ(cross-pair sum) + Δ(SASA of the whole structure)
+//      + Δ(boundary dihedral records) + Δ(disulfide pairs touching a moved atom)
+// where cross pairs are neighbor-list pairs whose atoms are in different
+// move groups (0 = fixed), not excluded, with r² <= 12² (:2312-2323), the
+// "after" sum uses the moved atoms' half-list Born radii (update_born
+// :2043-2051) and the fixed atoms' unchanged radii.
+//
+// Work is proportional to the move, not to the structure:
+//   * cross pairs come from the moved atoms' full rows only, old and new
+//     geometry evaluated in the same pass (each fixed partner once, pairs
+//     between two moving groups once, from the lower index);
+//   * SASA is recomputed only for atoms whose half row holds an atom of a
+//     different group (moved atoms, plus fixed atoms that list a moved atom)
+//     — every other atom's SASA is unchanged bit for bit;
+//   * dihedral records are tested for a mixed group pattern.
+// Per-atom contributions land in dE_atom[2*i] (cross) / dE_atom[2*i+1]
+// (SASA) and are summed in atom order, so the result is deterministic.
+#pragma once
+#include "alma_common.cuh"
+
+namespace alma {
+
+constexpr int MOVE_THREADS = 512;
+constexpr int MAX_ROT = 2;
+
+// Global scratch for the move kernels; every array is all-zero between
+// proposals (each proposal clears what it set).
+struct MoveScratch {
+    int8_t *group;      // [natoms]
+    uint8_t *mark;      // [natoms]
+    double *xyz_new;    // [natoms*4]
+    double *born_new;   // [natoms]
+    double *dE_atom;    // [natoms*2]
+    int32_t *affected;  // [natoms] compaction list (per-system region)
+};
+
+// A j-side: sorted explicit atoms side_idx[eb, ee) plus the range [lo, hi).
+struct SideRef {
+    int64_t eb, ee;
+    int32_t lo, hi;
+};
+
+__device__ __forceinline__ SideRef side_ref(const AlmaTopo &t, int k) {
+    SideRef S;
+    S.eb = t.side_ptr[k];
+    S.ee = t.side_ptr[k + 1];
+    S.lo = t.side_lo[k];
+    S.hi = t.side_hi[k];
+    return S;
+}
+
+__device__ __forceinline__ int64_t side_count(const SideRef &S) { return (S.ee - S.eb) + (int64_t)(S.hi - S.lo); }
+
+__device__ __forceinline__ int side_atom(const SideRef &S, const int32_t *side_idx, int64_t k) {
+    const int64_t ne = S.ee - S.eb;
+    return k < ne ? side_idx[S.eb + k] : S.lo + (int)(k - ne);
+}
+
+__device__ __forceinline__ bool contains_sorted(const int32_t *a, int64_t beg, int64_t end, int v) {
+    int64_t lo = beg, hi = end;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (a[mid] < v) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo < end && a[lo] == v;
+}
+
+__device__ __forceinline__ bool side_has(const SideRef &S, const int32_t *side_idx, int v) {
+    return (v >= S.lo && v < S.hi) || contains_sorted(side_idx, S.eb, S.ee, v);
+}
+
+struct Rot {
+    double o[3], u[3], c, s;
+    SideRef side;  // rotated atoms
+};
+
+struct MoveDesc {
+    int kind;            // -1 none
+    int nrot;
+    Rot rot[MAX_ROT];
+    int nmem;            // member lists (define move groups 1..nmem)
+    SideRef mem[2];
+    int degenerate;      // 1: zero-length axis / empty side (no proposal)
+};
+
+// Rodrigues rotation about unit axis u anchored at o (physics_engine.cpp:1848-1862).
+__device__ __forceinline__ void rodrigues(double &px, double &py, double &pz, const Rot &R) {
+    const double vx = px - R.o[0], vy = py - R.o[1], vz = pz - R.o[2];
+    const double dot = R.u[0] * vx + R.u[1] * vy + R.u[2] * vz;
+    const double cx = R.u[1] * vz - R.u[2] * vy;
+    const double cy = R.u[2] * vx - R.u[0] * vz;
+    const double cz = R.u[0] * vy - R.u[1] * vx;
+    const double k = 1.0 - R.c;
+    px = R.o[0] + vx * R.c + cx * R.s + R.u[0] * dot * k;
+    py = R.o[1] + vy * R.c + cy * R.s + R.u[1] * dot * k;
+    pz = R.o[2] + vz * R.c + cz * R.s + R.u[2] * dot * k;
+}
+
+// Axis from atom ai to aj at the given positions; false when degenerate.
+__device__ __forceinline__ bool make_axis(Rot &R, double4 pi, double4 pj, double delta) {
+    R.o[0] = pi.x; R.o[1] = pi.y; R.o[2] = pi.z;
+    double ux = pj.x - pi.x, uy = pj.y - pi.y, uz = pj.z - pi.z;
+    const double l = sqrt(ux * ux + uy * uy + uz * uz);
+    if (l < 1e-10) return false;
+    ux /= l; uy /= l; uz /= l;
+    R.u[0] = ux; R.u[1] = uy; R.u[2] = uz;
+    R.c = cos(delta);
+    R.s = sin(delta);
+    return true;
+}
+
+// Thread 0 only: decode (kind, a, delta) of system s into a MoveDesc.
+// kind 0 torsion (a = rot-bond index local to s), 1 crankshaft (crank-pair
+// index), 2 concerted sidechain pair (pair index; delta[0], delta[1]).
+__device__ inline void decode_move(MoveDesc &M, const AlmaTopo &t, const double *xyz, int s, int kind, int a,
+                                   const double *delta) {
+    M.kind = kind;
+    M.nrot = 0;
+    M.nmem = 0;
+    M.degenerate = 1;
+    if (kind == 0) {
+        const int k = t.rb_off[s] + a;
+        M.mem[0] = side_ref(t, k);
+        M.nmem = 1;
+        if (side_count(M.mem[0]) == 0) return;
+        Rot &R = M.rot[0];
+        if (!make_axis(R, ld_xyz(xyz, t.rb_ij[2 * k]), ld_xyz(xyz, t.rb_ij[2 * k + 1]), delta[0])) return;
+        R.side = M.mem[0];
+        M.nrot = 1;
+        M.degenerate = 0;
+    } else if (kind == 1) {
+        const int cpi = t.cp_off[s] + a;
+        const int kphi = t.rb_off[s] + t.cp[2 * cpi], kpsi = t.rb_off[s] + t.cp[2 * cpi + 1];
+        M.mem[0] = side_ref(t, kphi);
+        M.nmem = 1;
+        const SideRef psi = side_ref(t, kpsi);
+        if (side_count(M.mem[0]) == 0 || side_count(psi) == 0) return;
+        Rot &R1 = M.rot[0];
+        if (!make_axis(R1, ld_xyz(xyz, t.rb_ij[2 * kphi]), ld_xyz(xyz, t.rb_ij[2 * kphi + 1]), delta[0])) return;
+        R1.side = M.mem[0];
+        // psi axis from the post-phi positions of its two atoms (:2447-2452)
+        const int bi = t.rb_ij[2 * kpsi], bj = t.rb_ij[2 * kpsi + 1];
+        double4 pb4 = ld_xyz(xyz, bi), pj4 = ld_xyz(xyz, bj);
+        if (side_has(R1.side, t.side_idx, bi)) rodrigues(pb4.x, pb4.y, pb4.z, R1);
+        if (side_has(R1.side, t.side_idx, bj)) rodrigues(pj4.x, pj4.y, pj4.z, R1);
+        Rot &R2 = M.rot[1];
+        if (!make_axis(R2, pb4, pj4, 0.0)) return;
+        R2.c = R1.c;   // cos(-d) = cos(d)
+        R2.s = -R1.s;  // the reference passes (cosD, -sinD)
+        R2.side = psi;
+        M.nrot = 2;
+        M.degenerate = 0;
+    } else if (kind == 2) {
+        const int pi = t.csp_off[s] + a;
+        const int ka = t.rb_off[s] + t.csp[2 * pi], kb = t.rb_off[s] + t.csp[2 * pi + 1];
+        M.mem[0] = side_ref(t, ka);
+        M.mem[1] = side_ref(t, kb);
+        M.nmem = 2;
+        if (side_count(M.mem[0]) == 0 || side_count(M.mem[1]) == 0) return;
+        for (int r = 0; r < 2; ++r) {
+            const int k = r == 0 ? ka : kb;
+            Rot &R = M.rot[r];
+            if (!make_axis(R, ld_xyz(xyz, t.rb_ij[2 * k]), ld_xyz(xyz, t.rb_ij[2 * k + 1]), delta[r])) return;
+            R.side = M.mem[r];
+        }
+        M.nrot = 2;
+        M.degenerate = 0;
+    }
+}
+
+template <typename R>
+__device__ __forceinline__ void prm_of(const float *prm, const double *prm64, int i, R &q, R &rad, R &eps) {
+    if constexpr (sizeof(R) == 4) {
+        const float4 p = *reinterpret_cast<const float4 *>(prm + 4 * (size_t)i);
+        q = p.x; rad = p.y; eps = p.z;
+    } else {
+        const double4 p = *reinterpret_cast<const double4 *>(prm64 + 4 * (size_t)i);
+        q = p.x; rad = p.y; eps = p.z;
+    }
+}
+
+struct MoveResult {
+    double dE, dcross, dsasa, ddih, dss;
+};
+
+__device__ __forceinline__ double4 pos_new(const double *xyz, const double *xyz_new, const int8_t *group, int j) {
+    return group[j] ? ld_xyz(xyz_new, j) : ld_xyz(xyz, j);
+}
+
+__device__ __forceinline__ double dih_angle4(double4 A, double4 B, double4 C, double4 D) {
+    const double b1x = A.x - B.x, b1y = A.y - B.y, b1z = A.z - B.z;
+    const double b2x = C.x - B.x, b2y = C.y - B.y, b2z = C.z - B.z;
+    const double b3x = D.x - C.x, b3y = D.y - C.y, b3z = D.z - C.z;
+    const double n1x = b1y * b2z - b1z * b2y, n1y = b1z * b2x - b1x * b2z, n1z = b1x * b2y - b1y * b2x;
+    const double n2x = b2y * b3z - b2z * b3y, n2y = b2z * b3x - b2x * b3z, n2z = b2x * b3y - b2y * b3x;
+    const double m1x = n1y * b2z - n1z * b2y, m1y = n1z * b2x - n1x * b2z, m1z = n1x * b2y - n1y * b2x;
+    return atan2(m1x * n2x + m1y * n2y + m1z * n2z, n1x * n2x + n1y * n2y + n1z * n2z);
+}
+
+struct MoveCtx {
+    DevParams P;
+    AlmaBatch b;
+    AlmaTopo t;
+    AlmaNL nl;
+    MoveScratch w;
+};
+
+// Number of member atoms and the k-th one (concatenated member lists).
+__device__ __forceinline__ int64_t n_members(const MoveDesc &M) {
+    int64_t n = 0;
+    for (int g = 0; g < M.nmem; ++g) n += side_count(M.mem[g]);
+    return n;
+}
+
+__device__ __forceinline__ int member(const MoveDesc &M, const int32_t *side_idx, int64_t k, int &g) {
+    for (g = 0; g < M.nmem - 1; ++g) {
+        const int64_t len = side_count(M.mem[g]);
+        if (k < len) break;
+        k -= len;
+    }
+    return side_atom(M.mem[g], side_idx, k);
+}
+
+// Whole-CTA evaluation of a decoded, non-degenerate proposal of system s.
+// smem_d: >= 32 doubles; s_nAff: shared counter.  Leaves group/xyz_new/
+// born_new set for the members (the caller commits or discards, then calls
+// move_clear).
+template <typename R>
+__device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, double *smem_d, int *s_naff) {
+    const AlmaBatch &b = C.b;
+    const AlmaTopo &t = C.t;
+    const MoveScratch &w = C.w;
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int lane = tid & 31, wid = tid >> 5, nw = nthr >> 5;
+    const int a0 = b.atom_off[s], a1 = b.atom_off[s + 1];
+    const int64_t nm = n_members(M);
+
+    // P1: group flags and starting copies of the member coordinates.
+    for (int64_t k = tid; k < nm; k += nthr) {
+        int g;
+        const int m = member(M, t.side_idx, k, g);
+        w.group[m] = (int8_t)(g + 1);
+        *reinterpret_cast<double4 *>(w.xyz_new + 4 * (size_t)m) = ld_xyz(b.xyz, m);
+    }
+    if (tid == 0) *s_naff = 0;
+    __syncthreads();
+    // P2: the rotations, in order, on the proposal copy.
+    for (int r = 0; r < M.nrot; ++r) {
+        const Rot &Ro = M.rot[r];
+        const int64_t nr = side_count(Ro.side);
+        for (int64_t k = tid; k < nr; k += nthr) {
+            const int m = side_atom(Ro.side, t.side_idx, k);
+            double4 p = ld_xyz(w.xyz_new, m);
+            rodrigues(p.x, p.y, p.z, Ro);
+            *reinterpret_cast<double4 *>(w.xyz_new + 4 * (size_t)m) = p;
+        }
+        __syncthreads();
+    }
+    // P3: half-list Born radii of the members at the new geometry, and
+    // marks on fixed atoms whose half row holds a member (SASA changes).
+    for (int64_t k = wid; k < nm; k += nw) {
+        int g;
+        const int m = member(M, t.side_idx, k, g);
+        const double4 pm = ld_xyz(w.xyz_new, m);
+        R qm, rm, em;
+        prm_of<R>(b.prm, b.prm64, m, qm, rm, em);
+        double sum = 0.0;
+        for (int64_t e = C.nl.half_ptr[m] + lane; e < C.nl.half_ptr[m] + C.nl.half_len[m]; e += 32) {
+            const int j = (int)(C.nl.half_cols[e] & ALMA_IDX_MASK);
+            R qj, rj, ej;
+            prm_of<R>(b.prm, b.prm64, j, qj, rj, ej);
+            const double r2d = d2_of(pm, pos_new(b.xyz, w.xyz_new, w.group, j));
+            const R r2 = (R)r2d;
+            sum += (double)hct_term<R>(m_sqrt(r2), r2, rm, rj);
+        }
+        sum = warp_sum(sum);
+        if (lane == 0) w.born_new[m] = 1.0 / fmax(1.0 / b.prm64[4 * (size_t)m + 1] - 0.5 * sum, 2.0);
+        for (int64_t e = C.nl.full_ptr[m] + lane; e < C.nl.full_ptr[m] + C.nl.full_len[m]; e += 32) {
+            const int j = (int)(C.nl.full_cols[e] & ALMA_IDX_MASK);
+            if (j < m && w.group[j] == 0) w.mark[j] = 1;
+        }
+    }
+    __syncthreads();
+    // P4: cross pairs from the members' full rows, before and after.
+    for (int64_t k = wid; k < nm; k += nw) {
+        int g;
+        const int m = member(M, t.side_idx, k, g);
+        const int gm = g + 1;
+        const double4 pmo = ld_xyz(b.xyz, m), pmn = ld_xyz(w.xyz_new, m);
+        R qm, rm, em;
+        prm_of<R>(b.prm, b.prm64, m, qm, rm, em);
+        const R amo = (R)b.born[m], amn = (R)w.born_new[m];
+        double acc = 0.0;
+        for (int64_t e = C.nl.full_ptr[m] + lane; e < C.nl.full_ptr[m] + C.nl.full_len[m]; e += 32) {
+            const uint32_t ent = C.nl.full_cols[e];
+            if (ent & ALMA_EXCL_BIT) continue;
+            const int j = (int)(ent & ALMA_IDX_MASK);
+            const int gj = w.group[j];
+            if (gj == gm || (gj != 0 && j < m)) continue;
+            R qj, rj, ej;
+            prm_of<R>(b.prm, b.prm64, j, qj, rj, ej);
+            const R qp = qm * qj, sig = rm + rj, ep = em * ej;
+            const double4 pjo = ld_xyz(b.xyz, j);
+            const double r2o = d2_of(pmo, pjo);
+            const R ajo = (R)b.born[j];
+            if (r2o <= C.P.pair_cut2) acc -= (double)pair_energy<R>(C.P, (R)r2o, qp, sig, ep, amo, ajo);
+            const double4 pjn = gj ? ld_xyz(w.xyz_new, j) : pjo;
+            const double r2n = d2_of(pmn, pjn);
+            const R ajn = gj ? (R)w.born_new[j] : ajo;
+            if (r2n <= C.P.pair_cut2) acc += (double)pair_energy<R>(C.P, (R)r2n, qp, sig, ep, amn, ajn);
+        }
+        acc = warp_sum(acc);
+        if (lane == 0) w.dE_atom[2 * (size_t)m] = acc;
+    }
+    // Affected fixed atoms -> compaction list (order irrelevant: results go
+    // to per-atom slots and are summed in atom order).
+    for (int i = a0 + tid; i < a1; i += nthr) {
+        if (w.mark[i]) {
+            const int slot = atomicAdd(s_naff, 1);
+            w.affected[a0 + slot] = i;
+        }
+    }
+    __syncthreads();
+    // P5: SASA of every affected atom (members + marked), old and new, in
+    // row order.
+    const int64_t naff = nm + *s_naff;
+    const double pi4 = 4.0 * 3.14159265358979323846, pi2 = 2.0 * 3.14159265358979323846;
+    for (int64_t k = wid; k < naff; k += nw) {
+        int i;
+        if (k < nm) {
+            int g;
+            i = member(M, t.side_idx, k, g);
+        } else {
+            i = w.affected[a0 + (k - nm)];
+        }
+        const bool moved = w.group[i] != 0;
+        const double4 pio = ld_xyz(b.xyz, i), pin = moved ? ld_xyz(w.xyz_new, i) : pio;
+        const double rsi = b.prm64[4 * (size_t)i + 1] + C.P.probe_r;
+        const double cs = pi2 * rsi * rsi;
+        double sao = pi4 * rsi * rsi, san = sao;
+        const int64_t beg = C.nl.half_ptr[i], end = C.nl.half_ptr[i] + C.nl.half_len[i];
+        for (int64_t e0 = beg; e0 < end; e0 += 32) {
+            const int64_t e = e0 + lane;
+            double co = 0.0, cn = 0.0;
+            bool ho = false, hn = false;
+            if (e < end) {
+                const int j = (int)(C.nl.half_cols[e] & ALMA_IDX_MASK);
+                const double rsj = b.prm64[4 * (size_t)j + 1] + C.P.probe_r;
+                const double dc = rsi + rsj;
+                const double4 pjo = ld_xyz(b.xyz, j);
+                const double ro = sqrt(d2_of(pio, pjo));
+                if (ro < dc) { ho = true; co = cs * ((dc - ro) / (2.0 * rsi)); }
+                const double4 pjn = w.group[j] ? ld_xyz(w.xyz_new, j) : pjo;
+                const double rn = sqrt(d2_of(pin, pjn));
+                if (rn < dc) { hn = true; cn = cs * ((dc - rn) / (2.0 * rsi)); }
+            }
+            unsigned mo = __ballot_sync(0xffffffffu, ho), mn = __ballot_sync(0xffffffffu, hn);
+            while (mo) {
+                const int l = __ffs(mo) - 1;
+                mo &= mo - 1;
+                sao -= fmin(sao * 0.85, __shfl_sync(0xffffffffu, co, l));
+            }
+            while (mn) {
+                const int l = __ffs(mn) - 1;
+                mn &= mn - 1;
+                san -= fmin(san * 0.85, __shfl_sync(0xffffffffu, cn, l));
+            }
+        }
+        if (lane == 0) w.dE_atom[2 * (size_t)i + 1] = C.P.gamma_sa * (fmax(0.0, san) - fmax(0.0, sao));
+    }
+    // P6: boundary dihedral records and disulfides of system s.
+    double ddih = 0.0, dss = 0.0;
+    for (int r = t.dih_off[s] + tid; r < t.dih_off[s + 1]; r += nthr) {
+        const int4 q = *reinterpret_cast<const int4 *>(t.dih_abcd + 4 * (size_t)r);
+        const int sa = w.group[q.x] != 0, sb = w.group[q.y] != 0, sc = w.group[q.z] != 0, sd = w.group[q.w] != 0;
+        if (!(sa || sb || sc || sd) || (sa && sb && sc && sd)) continue;
+        const double po = dih_angle4(ld_xyz(b.xyz, q.x), ld_xyz(b.xyz, q.y), ld_xyz(b.xyz, q.z), ld_xyz(b.xyz, q.w));
+        const double pn = dih_angle4(pos_new(b.xyz, w.xyz_new, w.group, q.x), pos_new(b.xyz, w.xyz_new, w.group, q.y),
+                                     pos_new(b.xyz, w.xyz_new, w.group, q.z), pos_new(b.xyz, w.xyz_new, w.group, q.w));
+        double eo = 0.0, en = 0.0;
+        for (int k = t.term_off[r]; k < t.term_off[r + 1]; ++k) {
+            const double n = (double)t.term_n[k];
+            eo += t.term_v2[k] * (1.0 + cos(n * po - t.term_gamma[k]));
+            en += t.term_v2[k] * (1.0 + cos(n * pn - t.term_gamma[k]));
+        }
+        ddih += en - eo;
+    }
+    for (int k = t.ss_off[s] + tid; k < t.ss_off[s + 1]; k += nthr) {
+        const int i = t.ss_ij[2 * k], j = t.ss_ij[2 * k + 1];
+        if (w.group[i] == 0 && w.group[j] == 0) continue;
+        const double dro = sqrt(d2_of(ld_xyz(b.xyz, i), ld_xyz(b.xyz, j))) - C.P.r0_ss;
+        const double drn = sqrt(d2_of(pos_new(b.xyz, w.xyz_new, w.group, i), pos_new(b.xyz, w.xyz_new, w.group, j))) - C.P.r0_ss;
+        dss += C.P.k_ss * drn * drn - C.P.k_ss * dro * dro;
+    }
+    __syncthreads();
+    // P7: deterministic sums.
+    double c = 0.0, sa = 0.0;
+    for (int i = a0 + tid; i < a1; i += nthr) {
+        c += w.dE_atom[2 * (size_t)i];
+        sa += w.dE_atom[2 * (size_t)i + 1];
+    }
+    MoveResult res;
+    res.dcross = block_sum(c, smem_d);
+    res.dsasa = block_sum(sa, smem_d);
+    res.ddih = block_sum(ddih, smem_d);
+    res.dss = block_sum(dss, smem_d);
+    res.dE = res.dcross + res.dsasa + res.ddih + res.dss;
+    return res;
+}
+
+// Commit (accept != 0) the members' proposal and clear all scratch.
+__device__ inline void move_finish(const MoveCtx &C, const MoveDesc &M, int s, const int *s_naff, int accept) {
+    const MoveScratch &w = C.w;
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int a0 = C.b.atom_off[s];
+    const int64_t nm = n_members(M);
+    for (int64_t k = tid; k < nm; k += nthr) {
+        int g;
+        const int m = member(M, C.t.side_idx, k, g);
+        if (accept) {
+            *reinterpret_cast<double4 *>(C.b.xyz + 4 * (size_t)m) = ld_xyz(w.xyz_new, m);
+            C.b.born[m] = w.born_new[m];
+        }
+        w.group[m] = 0;
+        w.dE_atom[2 * (size_t)m] = 0.0;
+        w.dE_atom[2 * (size_t)m + 1] = 0.0;
+    }
+    const int naff = *s_naff;
+    for (int k = tid; k < naff; k += nthr) {
+        const int i = w.affected[a0 + k];
+        w.mark[i] = 0;
+        w.dE_atom[2 * (size_t)i + 1] = 0.0;
+    }
+    __syncthreads();
+}
+
+}  // namespace alma

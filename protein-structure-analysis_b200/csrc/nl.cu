@@ -1,0 +1,391 @@
+// Neighbor-list build on the device.
+//
+// Reproduces NeighborList::build (physics_engine.cpp:293-342) bit-exactly,
+// including row order: a 14 Å+1e-6 cubic cell grid over the system's
+// bounding box padded by one cell, atoms binned by floor((x-lo)/cs), and
+// each row listing the atoms of the 27 neighbour cells in (dz, dy, dx)
+// order, ascending atom index inside a cell, keeping r² < 14² (FP64).
+// The half row keeps j > i (the reference's nb[i]); the full row keeps every
+// j != i (used by Born radii and the move kernels, where the order is
+// irrelevant).  Each entry carries the 1-2/1-3/SS exclusion flag in bit 31.
+//
+// Pipeline (all stream-ordered, no host sync):
+//   grid   : one CTA per system — FP64 bounding box, cell-grid shape
+//   offsets: one CTA — per-system cell offsets, capacity check
+//   bin    : atom -> cell, cell histogram
+//   scan   : cell starts
+//   scatter: atoms into cells, then a per-cell rank sort (ascending index)
+//   count  : warp per atom — row lengths
+//   rowscan: one CTA per system — row pointers inside the system's region
+//   fill   : warp per atom — rows, ballot-compacted in scan order
+// Every stage honours an optional per-system mask, so systems can be
+// rebuilt independently (the MC driver rebuilds only chains that drifted).
+#include <cstdio>
+
+#include "alma_common.cuh"
+#include "alma_scan.cuh"
+
+namespace alma {
+
+struct SysGrid {
+    double xlo, ylo, zlo, cs;
+    int32_t nx, ny, nz, pad;
+    int64_t cell_off;  // first global cell of this system
+    int64_t ncell;
+};
+
+struct NLWork {
+    SysGrid *grid;        // [nsys]
+    int32_t *cell_of;     // [natoms] local cell index
+    int32_t *cell_count;  // [max_cells]
+    int32_t *cell_fill;   // [max_cells]
+    int64_t *cell_start;  // [max_cells+1]
+    int32_t *cell_atoms;  // [natoms]
+    int32_t *full_cnt;    // [natoms]
+    int32_t *half_cnt;    // [natoms]
+    int64_t *tile_sums;   // scan scratch
+    int64_t *total_cells; // [1]
+    int32_t *ok;          // [1] 1 when the grid fit
+    int32_t *sys_ok;      // [nsys] 1 when the system's rows fit its region
+};
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+static size_t carve(NLWork *w, char *base, int32_t nsys, int32_t natoms, int64_t max_cells) {
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        char *p = base ? base + off : nullptr;
+        off += align256(bytes);
+        return p;
+    };
+    const int64_t big = (max_cells + 1 > (int64_t)natoms + 1) ? max_cells + 1 : (int64_t)natoms + 1;
+    const int64_t ntiles = scan_num_tiles(big) + 1;
+    NLWork t;
+    t.grid = (SysGrid *)take(sizeof(SysGrid) * (size_t)(nsys > 0 ? nsys : 1));
+    t.cell_of = (int32_t *)take(sizeof(int32_t) * (size_t)natoms);
+    t.cell_count = (int32_t *)take(sizeof(int32_t) * (size_t)max_cells);
+    t.cell_fill = (int32_t *)take(sizeof(int32_t) * (size_t)max_cells);
+    t.cell_start = (int64_t *)take(sizeof(int64_t) * (size_t)(max_cells + 1));
+    t.cell_atoms = (int32_t *)take(sizeof(int32_t) * (size_t)natoms);
+    t.full_cnt = (int32_t *)take(sizeof(int32_t) * (size_t)natoms);
+    t.half_cnt = (int32_t *)take(sizeof(int32_t) * (size_t)natoms);
+    t.tile_sums = (int64_t *)take(sizeof(int64_t) * (size_t)ntiles);
+    t.total_cells = (int64_t *)take(sizeof(int64_t));
+    t.ok = (int32_t *)take(sizeof(int32_t));
+    t.sys_ok = (int32_t *)take(sizeof(int32_t) * (size_t)(nsys > 0 ? nsys : 1));
+    if (w) *w = t;
+    return off;
+}
+
+__device__ __forceinline__ int sys_of_atom(const int32_t *atom_off, int nsys, int i) {
+    int lo = 0, hi = nsys - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (atom_off[mid] <= i) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// One CTA per system: bounding box and grid shape (physics_engine.cpp:299-316).
+// A system outside the mask gets a 1x1x1 grid that no atom uses.
+__global__ void nl_grid_kernel(const int32_t *__restrict__ atom_off, const uint8_t *__restrict__ mask,
+                               const double *__restrict__ xyz, double nl_rcut2, SysGrid *__restrict__ grid) {
+    __shared__ double red[6][32];
+    const int s = blockIdx.x;
+    const int a0 = atom_off[s], a1 = (mask && !mask[s]) ? atom_off[s] : atom_off[s + 1];
+    double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
+    for (int i = a0 + threadIdx.x; i < a1; i += blockDim.x) {
+        const double4 p = ld_xyz(xyz, i);
+        mn[0] = fmin(mn[0], p.x); mx[0] = fmax(mx[0], p.x);
+        mn[1] = fmin(mn[1], p.y); mx[1] = fmax(mx[1], p.y);
+        mn[2] = fmin(mn[2], p.z); mx[2] = fmax(mx[2], p.z);
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int d = 0; d < 3; ++d) {
+        double a = mn[d], b = mx[d];
+        for (int o = 16; o > 0; o >>= 1) {
+            a = fmin(a, __shfl_xor_sync(0xffffffffu, a, o));
+            b = fmax(b, __shfl_xor_sync(0xffffffffu, b, o));
+        }
+        if (lane == 0) { red[d][wid] = a; red[3 + d][wid] = b; }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int nw = blockDim.x >> 5;
+        double lo[3], hi[3];
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = red[d][0]; hi[d] = red[3 + d][0];
+            for (int w = 1; w < nw; ++w) { lo[d] = fmin(lo[d], red[d][w]); hi[d] = fmax(hi[d], red[3 + d][w]); }
+        }
+        SysGrid g;
+        g.cs = sqrt(nl_rcut2) + 1e-6;
+        const double mg = g.cs;
+        g.xlo = lo[0] - mg; g.ylo = lo[1] - mg; g.zlo = lo[2] - mg;
+        const double lx = hi[0] - g.xlo + 2.0 * mg, ly = hi[1] - g.ylo + 2.0 * mg, lz = hi[2] - g.zlo + 2.0 * mg;
+        g.nx = max(1, (int)ceil(lx / g.cs));
+        g.ny = max(1, (int)ceil(ly / g.cs));
+        g.nz = max(1, (int)ceil(lz / g.cs));
+        if (a1 <= a0) { g.nx = g.ny = g.nz = 1; }
+        g.pad = 0;
+        g.ncell = (int64_t)g.nx * g.ny * g.nz;
+        g.cell_off = 0;
+        grid[s] = g;
+    }
+}
+
+__global__ void nl_offsets_kernel(int nsys, SysGrid *__restrict__ grid, int64_t max_cells,
+                                  int64_t *__restrict__ total_cells, int32_t *__restrict__ ok,
+                                  uint32_t *__restrict__ status) {
+    if (threadIdx.x != 0) return;
+    int64_t acc = 0;
+    for (int s = 0; s < nsys; ++s) {
+        grid[s].cell_off = acc;
+        acc += grid[s].ncell;
+    }
+    *total_cells = acc;
+    const int fits = acc <= max_cells;
+    *ok = fits;
+    if (!fits) set_status(status, ALMA_ST_CELL_OVERFLOW);
+}
+
+__global__ void nl_bin_kernel(const int32_t *__restrict__ atom_off, int nsys, int natoms,
+                              const uint8_t *__restrict__ mask, const double *__restrict__ xyz,
+                              const SysGrid *__restrict__ grid, const int32_t *__restrict__ ok,
+                              int32_t *__restrict__ cell_of, int32_t *__restrict__ cell_count) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= natoms || !*ok) return;
+    const int s = sys_of_atom(atom_off, nsys, i);
+    if (mask && !mask[s]) return;
+    const SysGrid g = grid[s];
+    const double4 p = ld_xyz(xyz, i);
+    const int cx = min(g.nx - 1, max(0, (int)floor((p.x - g.xlo) / g.cs)));
+    const int cy = min(g.ny - 1, max(0, (int)floor((p.y - g.ylo) / g.cs)));
+    const int cz = min(g.nz - 1, max(0, (int)floor((p.z - g.zlo) / g.cs)));
+    const int c = cx + g.nx * (cy + g.ny * cz);
+    cell_of[i] = c;
+    atomicAdd(&cell_count[g.cell_off + c], 1);
+}
+
+__global__ void nl_scatter_kernel(const int32_t *__restrict__ atom_off, int nsys, int natoms,
+                                  const uint8_t *__restrict__ mask, const SysGrid *__restrict__ grid,
+                                  const int32_t *__restrict__ ok, const int32_t *__restrict__ cell_of,
+                                  const int64_t *__restrict__ cell_start, int32_t *__restrict__ cell_fill,
+                                  int32_t *__restrict__ cell_atoms) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= natoms || !*ok) return;
+    const int s = sys_of_atom(atom_off, nsys, i);
+    if (mask && !mask[s]) return;
+    const int64_t c = grid[s].cell_off + cell_of[i];
+    const int slot = atomicAdd(&cell_fill[c], 1);
+    cell_atoms[cell_start[c] + slot] = i;
+}
+
+// Sorts every cell's atom list ascending (the reference pushes atoms in
+// index order).  Rank sort: each element's position is the number of
+// smaller elements (indices are distinct).
+constexpr int SORT_SMEM = 2048;
+__global__ void nl_cellsort_kernel(const int64_t *__restrict__ total_cells, const int32_t *__restrict__ ok,
+                                   const int64_t *__restrict__ cell_start, int32_t *__restrict__ cell_atoms,
+                                   int32_t *__restrict__ spill) {
+    __shared__ int32_t buf[SORT_SMEM];
+    if (!*ok) return;
+    const int64_t nc = *total_cells;
+    for (int64_t c = blockIdx.x; c < nc; c += gridDim.x) {
+        const int64_t b = cell_start[c];
+        const int m = (int)(cell_start[c + 1] - b);
+        if (m <= 1) continue;
+        int32_t *src = cell_atoms + b;
+        if (m <= SORT_SMEM) {
+            for (int k = threadIdx.x; k < m; k += blockDim.x) buf[k] = src[k];
+            __syncthreads();
+            for (int k = threadIdx.x; k < m; k += blockDim.x) {
+                const int32_t v = buf[k];
+                int rank = 0;
+                for (int q = 0; q < m; ++q) rank += buf[q] < v;
+                src[rank] = v;
+            }
+            __syncthreads();
+        } else {
+            // Oversized cell: rank in global memory through the spill buffer
+            // (same positions as cell_atoms), then copy back.
+            int32_t *tmp = spill + b;
+            for (int k = threadIdx.x; k < m; k += blockDim.x) {
+                const int32_t v = src[k];
+                int rank = 0;
+                for (int q = 0; q < m; ++q) rank += src[q] < v;
+                tmp[rank] = v;
+            }
+            __syncthreads();
+            for (int k = threadIdx.x; k < m; k += blockDim.x) src[k] = tmp[k];
+            __syncthreads();
+        }
+    }
+}
+
+__device__ __forceinline__ bool excluded(const int64_t *__restrict__ excl_ptr, const int32_t *__restrict__ excl_cols,
+                                         int i, int j) {
+    if (!excl_ptr) return false;
+    int lo_i = i < j ? i : j, hi_j = i < j ? j : i;
+    int64_t lo = excl_ptr[lo_i], hi = excl_ptr[lo_i + 1];
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (excl_cols[mid] < hi_j) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo < excl_ptr[lo_i + 1] && excl_cols[lo] == hi_j;
+}
+
+// One CTA per system: row pointers inside the system's region, overflow
+// check.  PASS 0 full rows, PASS 1 half rows.
+__global__ void nl_rowscan_kernel(const int32_t *__restrict__ atom_off, const uint8_t *__restrict__ mask,
+                                  const int32_t *__restrict__ full_cnt, const int32_t *__restrict__ half_cnt,
+                                  AlmaNL nl, int32_t *__restrict__ sys_ok, uint32_t *__restrict__ status) {
+    __shared__ int64_t sm[33];
+    const int s = blockIdx.x;
+    if (mask && !mask[s]) return;
+    const int a0 = atom_off[s], a1 = atom_off[s + 1];
+    for (int pass = 0; pass < 2; ++pass) {
+        const int32_t *cnt = pass == 0 ? full_cnt : half_cnt;
+        int64_t *ptr = pass == 0 ? nl.full_ptr : nl.half_ptr;
+        int32_t *len = pass == 0 ? nl.full_len : nl.half_len;
+        const int64_t base = pass == 0 ? nl.full_base[s] : nl.half_base[s];
+        const int64_t cap = (pass == 0 ? nl.full_base[s + 1] : nl.half_base[s + 1]) - base;
+        int64_t carry = 0;
+        for (int b0 = a0; b0 < a1; b0 += blockDim.x) {
+            const int i = b0 + threadIdx.x;
+            const int64_t v = i < a1 ? cnt[i] : 0;
+            int64_t ex;
+            const int64_t tot = block_exclusive_scan(v, ex, sm);
+            if (i < a1) {
+                ptr[i] = base + carry + ex;
+                len[i] = (int32_t)v;
+            }
+            carry += tot;
+        }
+        if (threadIdx.x == 0) {
+            nl.need[2 * s + pass] = carry;
+            if (carry > cap) {
+                sys_ok[s] = 0;
+                set_status(status, ALMA_ST_NL_OVERFLOW);
+            } else if (pass == 0) {
+                sys_ok[s] = 1;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Warp per atom.  PASS 0 counts, PASS 1 writes.
+template <int PASS>
+__global__ void nl_rows_kernel(const int32_t *__restrict__ atom_off, int nsys, int natoms, const uint8_t *__restrict__ mask,
+                               const double *__restrict__ xyz, double rcut2, const SysGrid *__restrict__ grid,
+                               const int32_t *__restrict__ ok, const int32_t *__restrict__ cell_of,
+                               const int64_t *__restrict__ cell_start, const int32_t *__restrict__ cell_atoms,
+                               int32_t *__restrict__ full_cnt, int32_t *__restrict__ half_cnt,
+                               const int64_t *__restrict__ excl_ptr, const int32_t *__restrict__ excl_cols,
+                               AlmaNL nl, const int32_t *__restrict__ sys_ok) {
+    const int warps_per_block = blockDim.x >> 5;
+    const int i = blockIdx.x * warps_per_block + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (i >= natoms || !*ok) return;
+    const int s = sys_of_atom(atom_off, nsys, i);
+    if (mask && !mask[s]) return;
+    if (PASS == 1 && !sys_ok[s]) return;
+    const SysGrid g = grid[s];
+    const int c = cell_of[i];
+    const int cx = c % g.nx, cy = (c / g.nx) % g.ny, cz = c / (g.nx * g.ny);
+    const double4 pi = ld_xyz(xyz, i);
+    int64_t fo = 0, ho = 0;
+    if (PASS == 1) {
+        fo = nl.full_ptr[i];
+        ho = nl.half_ptr[i];
+        if (lane == 0) *reinterpret_cast<double4 *>(nl.ref_xyz + 4 * (size_t)i) = pi;
+    }
+    int nfull = 0, nhalf = 0;
+    for (int dz = -1; dz <= 1; ++dz) {
+        const int cz2 = cz + dz;
+        if (cz2 < 0 || cz2 >= g.nz) continue;
+        for (int dy = -1; dy <= 1; ++dy) {
+            const int cy2 = cy + dy;
+            if (cy2 < 0 || cy2 >= g.ny) continue;
+            for (int dx = -1; dx <= 1; ++dx) {
+                const int cx2 = cx + dx;
+                if (cx2 < 0 || cx2 >= g.nx) continue;
+                const int64_t cell = g.cell_off + cx2 + (int64_t)g.nx * (cy2 + (int64_t)g.ny * cz2);
+                const int64_t beg = cell_start[cell], end = cell_start[cell + 1];
+                for (int64_t k0 = beg; k0 < end; k0 += 32) {
+                    const int64_t k = k0 + lane;
+                    int j = -1;
+                    bool in = false;
+                    if (k < end) {
+                        j = cell_atoms[k];
+                        in = (j != i) && d2_of(pi, ld_xyz(xyz, j)) < rcut2;
+                    }
+                    const unsigned mf = __ballot_sync(0xffffffffu, in);
+                    const unsigned mh = __ballot_sync(0xffffffffu, in && j > i);
+                    if (PASS == 1 && in) {
+                        const unsigned lt = (1u << lane) - 1u;
+                        const uint32_t e = (uint32_t)j | (excluded(excl_ptr, excl_cols, i, j) ? ALMA_EXCL_BIT : 0u);
+                        nl.full_cols[fo + nfull + __popc(mf & lt)] = e;
+                        if (j > i) nl.half_cols[ho + nhalf + __popc(mh & lt)] = e;
+                    }
+                    nfull += __popc(mf);
+                    nhalf += __popc(mh);
+                }
+            }
+        }
+    }
+    if (PASS == 0 && lane == 0) {
+        full_cnt[i] = nfull;
+        half_cnt[i] = nhalf;
+    }
+}
+
+}  // namespace alma
+
+using namespace alma;
+
+extern "C" size_t alma_nl_workspace_bytes(int32_t nsys, int32_t natoms, int64_t max_cells) {
+    return carve(nullptr, nullptr, nsys, natoms, max_cells);
+}
+
+extern "C" int alma_nl_build(const AlmaBatch *b, const AlmaTopo *t, AlmaNL *nl, const uint8_t *sys_mask,
+                             void *workspace, int64_t max_cells, void *stream) {
+    if (!b || !nl || !workspace || b->nsys <= 0 || b->natoms < 0 || max_cells <= 0)
+        return alma_set_error(ALMA_EINVAL, "alma_nl_build: bad arguments");
+    if (!nl->full_ptr || !nl->full_len || !nl->half_ptr || !nl->half_len || !nl->full_base || !nl->half_base ||
+        !nl->ref_xyz || !nl->need || !b->xyz || !b->atom_off)
+        return alma_set_error(ALMA_EINVAL, "alma_nl_build: null buffer");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int nsys = b->nsys, natoms = b->natoms;
+    NLWork w;
+    carve(&w, (char *)workspace, nsys, natoms, max_cells);
+    if (natoms == 0) return ALMA_OK;
+    ALMA_CUDA_TRY(cudaMemsetAsync(w.cell_count, 0, sizeof(int32_t) * (size_t)max_cells, st));
+    ALMA_CUDA_TRY(cudaMemsetAsync(w.cell_fill, 0, sizeof(int32_t) * (size_t)max_cells, st));
+    const double rcut2 = (12.0 + 2.0) * (12.0 + 2.0);
+    nl_grid_kernel<<<nsys, 256, 0, st>>>(b->atom_off, sys_mask, b->xyz, rcut2, w.grid);
+    nl_offsets_kernel<<<1, 32, 0, st>>>(nsys, w.grid, max_cells, w.total_cells, w.ok, b->status);
+    const int tb = 256, nb = (natoms + tb - 1) / tb;
+    nl_bin_kernel<<<nb, tb, 0, st>>>(b->atom_off, nsys, natoms, sys_mask, b->xyz, w.grid, w.ok, w.cell_of,
+                                     w.cell_count);
+    exclusive_scan<int32_t>(w.cell_count, w.cell_start, max_cells, w.tile_sums, st);
+    nl_scatter_kernel<<<nb, tb, 0, st>>>(b->atom_off, nsys, natoms, sys_mask, w.grid, w.ok, w.cell_of, w.cell_start,
+                                         w.cell_fill, w.cell_atoms);
+    // Oversized cells (> SORT_SMEM atoms) sort through half_cnt as spill
+    // space: it holds natoms ints and is only written later by the count pass.
+    nl_cellsort_kernel<<<1184, 256, 0, st>>>(w.total_cells, w.ok, w.cell_start, w.cell_atoms, w.half_cnt);
+    const int wpb = 8, rb = (natoms + wpb - 1) / wpb;
+    const int64_t *ep = t ? t->excl_ptr : nullptr;
+    const int32_t *ec = t ? t->excl_cols : nullptr;
+    nl_rows_kernel<0><<<rb, wpb * 32, 0, st>>>(b->atom_off, nsys, natoms, sys_mask, b->xyz, rcut2, w.grid, w.ok,
+                                               w.cell_of, w.cell_start, w.cell_atoms, w.full_cnt, w.half_cnt, ep, ec,
+                                               *nl, w.sys_ok);
+    nl_rowscan_kernel<<<nsys, 1024, 0, st>>>(b->atom_off, sys_mask, w.full_cnt, w.half_cnt, *nl, w.sys_ok, b->status);
+    nl_rows_kernel<1><<<rb, wpb * 32, 0, st>>>(b->atom_off, nsys, natoms, sys_mask, b->xyz, rcut2, w.grid, w.ok,
+                                               w.cell_of, w.cell_start, w.cell_atoms, w.full_cnt, w.half_cnt, ep, ec,
+                                               *nl, w.sys_ok);
+    ALMA_LAUNCH_CHECK("alma_nl_build");
+    return ALMA_OK;
+}

@@ -1,0 +1,509 @@
+"""Seeded synthetic all-atom chains (the benchmark inputs).
+
+Chains are built by NeRF (natural extension reference frame) from the
+internal-coordinate templates in data/residue_ic.json: backbone bond
+lengths/angles, per-residue sidechain and hydrogen geometry, with phi, psi,
+omega and the chi angles chosen by the caller.  Atom names follow the
+reference's residue bond templates, so BondTopology.build gives the
+reference exclusions / rotatable bonds.  Charges, R* and epsilon come from
+data/ff_params.json (the reference's amber_params ff14SB lookup).
+
+Workloads (residue counts and shapes of the reference's benchmark
+configurations, all seeded):
+  * ``chain(n_res, seed)``      — phi ~ N(-60, 15), psi ~ N(-45, 15) deg,
+                                  chi from the wells {60, 180, 300} +- U(10)
+  * ``compact_chain(...)``      — the same, then collapsed by seeded torsion
+                                  Monte Carlo on a radius-of-gyration restraint
+                                  plus a soft heavy-atom clash penalty
+  * ``coil_chain(...)``         — helix/coil phi-psi mixture
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_DATA = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
+with open(os.path.join(_DATA, "residue_ic.json")) as _f:
+    _IC = json.load(_f)
+with open(os.path.join(_DATA, "ff_params.json")) as _f:
+    _FF = json.load(_f)
+
+RESIDUES = ["ALA", "ARG", "ASN", "ASP", "CYS", "GLN", "GLU", "GLY", "HID", "ILE",
+            "LEU", "LYS", "MET", "PHE", "PRO", "SER", "THR", "TRP", "TYR", "VAL"]
+ROTAMER_WELLS = (60.0, 180.0, 300.0)
+
+
+@dataclass
+class Chain:
+    """A synthetic chain: particle arrays plus the topology inputs."""
+    xyz: np.ndarray        # [n, 3] float64, Å
+    charge: np.ndarray     # [n]
+    radius: np.ndarray     # [n] R* (Å)
+    epsilon: np.ndarray    # [n] kcal/mol
+    resnames: list
+    atomnames: list
+    res_idx: list
+    sequence: list
+
+    @property
+    def n(self):
+        return int(self.xyz.shape[0])
+
+
+def _place(a, b, c, bond, ang_deg, dih_deg):
+    """Atom d with |cd| = bond, angle bcd = ang, dihedral abcd = dih (NeRF)."""
+    ang, dih = math.radians(ang_deg), math.radians(dih_deg)
+    bc = c - b
+    bc /= np.linalg.norm(bc)
+    n = np.cross(b - a, bc)
+    n /= np.linalg.norm(n)
+    m = np.cross(n, bc)
+    d2 = np.array([-bond * math.cos(ang), bond * math.sin(ang) * math.cos(dih), bond * math.sin(ang) * math.sin(dih)])
+    return c + d2[0] * bc + d2[1] * m + d2[2] * n
+
+
+def n_chi(resname):
+    return len(_IC["residues"][resname]["chi_template"])
+
+
+def _place_residue(res, N, CA, C, phi, psi, chis):
+    """Positions of every template atom of one residue from its backbone."""
+    T = _IC["residues"][res]
+    pos = {"N": N, "CA": CA, "C": C}
+    tors = {"phi": phi, "psi": psi}
+    chi_t = T["chi_template"]
+    for k, key in enumerate(sorted(chi_t)):
+        tors[key] = float(chis[k]) if chis is not None and k < len(chis) else float(chi_t[key])
+    for name, p1, p2, p3, bond, ang_deg, var, off in T["atoms"]:
+        d = off + (tors[var] if var else 0.0)
+        pos[name] = _place(pos[p3], pos[p2], pos[p1], bond, ang_deg, d)
+    order = ["N", "CA", "C"] + [a[0] for a in T["atoms"]]
+    return order, np.array([pos[nm] for nm in order])
+
+
+def build(sequence, phi, psi, omega=None, chis=None):
+    """NeRF build.  sequence: residue names; phi/psi/omega: degrees per
+    residue; chis: per residue list of chi angles (degrees).  Returns a Chain."""
+    n_res = len(sequence)
+    bb = _IC["backbone"]
+    omega = np.full(n_res, 180.0) if omega is None else np.asarray(omega, float)
+    blocks, names, resn, ridx = [], [], [], []
+    prev = None  # (N, CA, C) of the previous residue
+    for r, res in enumerate(sequence):
+        T = _IC["residues"][res]
+        ph = float(phi[r]) if res != "PRO" else float(T["phi_template"])
+        if prev is None:
+            N = np.zeros(3)
+            CA = np.array([bb["b_n_ca"], 0.0, 0.0])
+            ang = math.radians(bb["a_n_ca_c"])
+            C = CA + bb["b_ca_c"] * np.array([-math.cos(ang), math.sin(ang), 0.0])
+        else:
+            pN, pCA, pC = prev
+            N = _place(pN, pCA, pC, bb["b_c_n"], bb["a_ca_c_n"], float(psi[r - 1]))
+            CA = _place(pCA, pC, N, bb["b_n_ca"], bb["a_c_n_ca"], float(omega[r - 1]))
+            C = _place(pC, N, CA, bb["b_ca_c"], bb["a_n_ca_c"], ph)
+        order, P = _place_residue(res, N, CA, C, ph, float(psi[r]), chis[r] if chis is not None else None)
+        blocks.append(P)
+        names += order
+        resn += [res] * len(order)
+        ridx += [r] * len(order)
+        prev = (N, CA, C)
+    xyz = np.concatenate(blocks).astype(np.float64)
+    q = np.empty(len(names))
+    rad = np.empty(len(names))
+    eps = np.empty(len(names))
+    for k, (res, name) in enumerate(zip(resn, names)):
+        q[k], rad[k], eps[k] = _FF["%s:%s" % (res, name)]
+    ch = Chain(xyz, q, rad, eps, resn, names, ridx, list(sequence))
+    ch.phi = np.array([float(phi[r]) if sequence[r] != "PRO" else float(_IC["residues"]["PRO"]["phi_template"])
+                       for r in range(n_res)])
+    ch.psi = np.asarray(psi, float).copy()
+    ch.chis = [list(c) for c in chis] if chis is not None else None
+    return ch
+
+
+def _clash_pairs(ch, xyz, heavy_cut=2.2, any_cut=1.3):
+    """Non-bonded close pairs (atoms >= 2 residues apart, or in the same or
+    adjacent residue but not within three bonds along the residue graph is
+    approximated by the residue gap test only)."""
+    from scipy.spatial import cKDTree
+    ridx = np.asarray(ch.res_idx)
+    pairs = cKDTree(xyz).query_pairs(heavy_cut, output_type="ndarray")
+    if len(pairs) == 0:
+        return pairs
+    i, j = pairs[:, 0], pairs[:, 1]
+    far = np.abs(ridx[i] - ridx[j]) >= 2
+    d = np.linalg.norm(xyz[i] - xyz[j], axis=1)
+    hv = np.array([not a.startswith("H") for a in ch.atomnames])
+    bad = far & ((hv[i] & hv[j]) | (d < any_cut))
+    return pairs[bad]
+
+
+def repack(ch, rng, passes=4):
+    """Seeded greedy rotamer repacking: for residues in a clash, try every
+    chi-well combination of the first three chis (others kept) and keep the
+    one with the fewest clashes."""
+    if ch.chis is None:
+        return ch
+    xyz = ch.xyz.copy()
+    ridx = np.asarray(ch.res_idx)
+    first = np.searchsorted(ridx, np.arange(len(ch.sequence) + 1))
+    chis = [list(c) for c in ch.chis]
+    for _ in range(passes):
+        bad = _clash_pairs(ch, xyz)
+        if len(bad) == 0:
+            break
+        residues = sorted(set(ridx[bad[:, 0]].tolist()) | set(ridx[bad[:, 1]].tolist()))
+        for r in residues:
+            res = ch.sequence[r]
+            m = n_chi(res)
+            if m == 0:
+                continue
+            a0, a1 = first[r], first[r + 1]
+            N, CA, C = xyz[a0], xyz[a0 + 1], xyz[a0 + 2]
+            best, best_cost = None, None
+            k = min(m, 3)
+            for combo in np.ndindex(*([3] * k)):
+                trial = list(chis[r])
+                for q in range(k):
+                    trial[q] = ROTAMER_WELLS[combo[q]] + rng.uniform(-10.0, 10.0)
+                _, P = _place_residue(res, N, CA, C, float(ch.phi[r]), float(ch.psi[r]), trial)
+                x2 = xyz.copy()
+                x2[a0:a1] = P
+                sel = _clash_pairs(ch, x2)
+                cost = int(np.sum((ridx[sel[:, 0]] == r) | (ridx[sel[:, 1]] == r))) if len(sel) else 0
+                if best_cost is None or cost < best_cost:
+                    best, best_cost, best_P = trial, cost, P
+                if cost == 0:
+                    break
+            chis[r] = best
+            xyz[a0:a1] = best_P
+    out = Chain(xyz, ch.charge, ch.radius, ch.epsilon, ch.resnames, ch.atomnames, ch.res_idx, ch.sequence)
+    out.phi, out.psi, out.chis = ch.phi, ch.psi, chis
+    return out
+
+
+def random_sequence(n_res, rng):
+    return [RESIDUES[k] for k in rng.integers(0, len(RESIDUES), size=n_res)]
+
+
+def _draw_chis(res, rng):
+    m = n_chi(res)
+    return list(rng.choice(ROTAMER_WELLS, size=m) + rng.uniform(-10.0, 10.0, size=m))
+
+
+_BB_ATOMS = ("N", "CA", "C", "O", "H", "HA", "CB", "CD")  # placed from phi/psi only (CD: PRO)
+_INTRA = {}
+
+
+def _intra_pairs(res, order):
+    """(i, j) index pairs of one residue's atoms >= 4 bonds apart (may clash)."""
+    if res in _INTRA:
+        return _INTRA[res]
+    from .topology import BOND_TEMPLATES
+    adj = {}
+    for a, b in BOND_TEMPLATES[res]:
+        adj.setdefault(a, []).append(b)
+        adj.setdefault(b, []).append(a)
+    idx = {nm: k for k, nm in enumerate(order)}
+    pairs = []
+    for a in order:
+        dist = {a: 0}
+        q = [a]
+        while q:
+            x = q.pop(0)
+            for y in adj.get(x, []):
+                if y not in dist:
+                    dist[y] = dist[x] + 1
+                    q.append(y)
+        for b in order:
+            if idx[b] > idx[a] and dist.get(b, 99) >= 4:
+                pairs.append((idx[a], idx[b]))
+    _INTRA[res] = np.array(pairs, dtype=int).reshape(-1, 2)
+    return _INTRA[res]
+
+
+def _intra_cost(res, order, P, heavy_cut, any_cut):
+    pr = _intra_pairs(res, order)
+    if len(pr) == 0:
+        return 0
+    d = np.linalg.norm(P[pr[:, 0]] - P[pr[:, 1]], axis=1)
+    hv = np.array([not nm.startswith("H") for nm in order])
+    hh = hv[pr[:, 0]] & hv[pr[:, 1]]
+    return int(np.sum(d < any_cut) + np.sum((d < heavy_cut) & hh & (d >= any_cut)))
+
+
+class _Grid:
+    """Uniform spatial hash for clash queries (cell = query radius)."""
+
+    def __init__(self, cell):
+        self.cell = cell
+        self.cells = {}
+        self.pts = []
+        self.heavy = []
+        self.res = []
+
+    def add(self, P, hv, r):
+        base = len(self.pts)
+        for k in range(P.shape[0]):
+            key = tuple(np.floor(P[k] / self.cell).astype(int))
+            self.cells.setdefault(key, []).append(base + k)
+            self.pts.append(P[k])
+            self.heavy.append(bool(hv[k]))
+            self.res.append(r)
+
+    def cost(self, P, hv, r, heavy_cut, any_cut, min_gap=2):
+        c = 0
+        for k in range(P.shape[0]):
+            key = np.floor(P[k] / self.cell).astype(int)
+            for dx in (-1, 0, 1):
+                for dy in (-1, 0, 1):
+                    for dz in (-1, 0, 1):
+                        for j in self.cells.get((key[0] + dx, key[1] + dy, key[2] + dz), ()):
+                            if abs(self.res[j] - r) < min_gap:
+                                continue
+                            d = np.linalg.norm(P[k] - self.pts[j])
+                            if d < any_cut or (d < heavy_cut and hv[k] and self.heavy[j]):
+                                c += 1
+        return c
+
+
+def grow(sequence, draw_phipsi, rng, tries=12, heavy_cut=2.2, any_cut=1.3, back=3):
+    """Two-phase seeded build.
+
+    1. Backbone (N CA C O H HA CB) residue by residue: (phi, psi of the
+       previous residue) are redrawn up to `tries` times while a new atom
+       clashes with backbone atoms >= 2 residues away (heavy-heavy closer
+       than heavy_cut, any pair closer than any_cut); when every draw
+       clashes the last `back` residues are regrown (bounded budget).
+    2. Sidechains, in a seeded random residue order: the drawn chis are kept
+       when clash-free, otherwise every well combination of the first three
+       chis is tried and the least clashing kept.
+    draw_phipsi(r) -> (phi, psi) in degrees."""
+    n_res = len(sequence)
+    bb = _IC["backbone"]
+    phi = np.zeros(n_res)
+    psi = np.zeros(n_res)
+    frames = [None] * n_res
+    bbpos = [None] * n_res
+    budget = 30 * n_res + 100
+    fails = np.zeros(n_res, int)
+
+    def backbone_atoms(r, N, CA, C, ph, ps):
+        order, P = _place_residue(sequence[r], N, CA, C, ph, ps, None)
+        keep = [k for k, nm in enumerate(order) if nm in _BB_ATOMS and not (nm == "CD" and sequence[r] != "PRO")]
+        return P[keep], np.array([not order[k].startswith("H") for k in keep])
+
+    grid = None
+    grid_upto = -1
+    r = 0
+    while r < n_res:
+        if grid is None or grid_upto > r - 2:
+            grid = _Grid(max(heavy_cut, any_cut))
+            grid_upto = -1
+        while grid_upto < r - 2:
+            grid_upto += 1
+            grid.add(bbpos[grid_upto][0], bbpos[grid_upto][1], grid_upto)
+        best = None
+        for t in range(tries):
+            ph, ps = draw_phipsi(r)
+            if sequence[r] == "PRO":
+                ph = float(_IC["residues"]["PRO"]["phi_template"])
+            ps_prev = psi[r - 1] if r > 0 else 0.0
+            if r > 0 and t >= tries // 2:
+                ps_prev = draw_phipsi(r - 1)[1]
+            if r == 0:
+                N = np.zeros(3)
+                CA = np.array([bb["b_n_ca"], 0.0, 0.0])
+                ang = math.radians(bb["a_n_ca_c"])
+                C = CA + bb["b_ca_c"] * np.array([-math.cos(ang), math.sin(ang), 0.0])
+            else:
+                pN, pCA, pC = frames[r - 1]
+                N = _place(pN, pCA, pC, bb["b_c_n"], bb["a_ca_c_n"], ps_prev)
+                CA = _place(pCA, pC, N, bb["b_n_ca"], bb["a_c_n_ca"], 180.0)
+                C = _place(pC, N, CA, bb["b_ca_c"], bb["a_n_ca_c"], ph)
+            P, hv = backbone_atoms(r, N, CA, C, ph, ps)
+            cost = grid.cost(P, hv, r, heavy_cut, any_cut) if r >= 2 else 0
+            if best is None or cost < best[0]:
+                best = (cost, ph, ps, ps_prev, P, hv, (N, CA, C))
+            if cost == 0:
+                break
+        cost, ph, ps, ps_prev, P, hv, frame = best
+        budget -= 1
+        if cost > 0 and budget > 0 and r >= 2:
+            fails[r] += 1
+            r -= min(r - 1, back * int(fails[r]))
+            continue
+        if r > 0 and ps_prev != psi[r - 1]:
+            psi[r - 1] = ps_prev
+            pN, pCA, pC = frames[r - 1]
+            bbpos[r - 1] = backbone_atoms(r - 1, pN, pCA, pC, phi[r - 1], ps_prev)
+        phi[r], psi[r] = ph, ps
+        bbpos[r], frames[r] = (P, hv), frame
+        r += 1
+    return pack_sidechains(sequence, phi, psi, frames, bbpos, rng, heavy_cut, any_cut)
+
+
+def pack_sidechains(sequence, phi, psi, frames, bbpos, rng, heavy_cut=2.2, any_cut=1.3):
+    """Greedy seeded sidechain placement on a fixed backbone: in a random
+    residue order, keep the drawn chis when clash-free, else try every well
+    combination of the first three chis and keep the least clashing."""
+    n_res = len(sequence)
+    chis = [_draw_chis(res, rng) for res in sequence]
+    grid = _Grid(max(heavy_cut, any_cut))
+    for rr in range(n_res):
+        grid.add(bbpos[rr][0], bbpos[rr][1], rr)
+    for rr in rng.permutation(n_res):
+        res = sequence[rr]
+        m = n_chi(res)
+        N, CA, C = frames[rr]
+        order, P = _place_residue(res, N, CA, C, phi[rr], psi[rr], chis[rr])
+        sc = [k for k, nm in enumerate(order) if nm not in _BB_ATOMS or (nm == "CD" and res != "PRO")]
+        if not sc:
+            continue
+        hv = np.array([not order[k].startswith("H") for k in sc])
+        cost = grid.cost(P[sc], hv, rr, heavy_cut, any_cut, min_gap=1) + _intra_cost(res, order, P, heavy_cut, any_cut)
+        if cost and m:
+            best = (cost, chis[rr], P)
+            for combo in np.ndindex(*([3] * min(m, 3))):
+                trial = list(chis[rr])
+                for q, w in enumerate(combo):
+                    trial[q] = ROTAMER_WELLS[w] + rng.uniform(-10.0, 10.0)
+                _, P2 = _place_residue(res, N, CA, C, phi[rr], psi[rr], trial)
+                c2 = (grid.cost(P2[sc], hv, rr, heavy_cut, any_cut, min_gap=1)
+                      + _intra_cost(res, order, P2, heavy_cut, any_cut))
+                if c2 < best[0]:
+                    best = (c2, trial, P2)
+                if c2 == 0:
+                    break
+            chis[rr], P = best[1], best[2]
+        grid.add(P[sc], hv, rr)
+    return build(sequence, phi, psi, chis=chis)
+
+
+def _chis(sequence, rng):
+    return [_draw_chis(res, rng) for res in sequence]
+
+
+def chain(n_res, seed, phi_mu=-60.0, psi_mu=-45.0, sd=15.0):
+    """phi ~ N(phi_mu, sd), psi ~ N(psi_mu, sd), chi from rotamer wells,
+    conditioned on no steric clash (seeded rejection, see grow)."""
+    rng = np.random.default_rng(seed)
+    seq = random_sequence(n_res, rng)
+    return grow(seq, lambda r: (rng.normal(phi_mu, sd), rng.normal(psi_mu, sd)), rng)
+
+
+def coil_chain(n_res, seed, helix_frac=0.5):
+    """Helix/coil mixture: helical segments phi/psi ~ N(-60,-45; 10), coil
+    segments from the beta / PPII basins."""
+    rng = np.random.default_rng(seed)
+    seq = random_sequence(n_res, rng)
+    kind = np.empty(n_res, int)
+    r = 0
+    while r < n_res:
+        seg = int(rng.integers(4, 16))
+        kind[r:r + seg] = 0 if rng.random() < helix_frac else 1
+        r += seg
+
+    def draw(k):
+        if kind[k] == 0:
+            return rng.normal(-60, 10), rng.normal(-45, 10)
+        if rng.random() < 0.5:
+            return rng.normal(-120, 15), rng.normal(130, 15)
+        return rng.normal(-70, 15), rng.normal(145, 15)
+
+    return grow(seq, draw, rng)
+
+
+def radius_of_gyration(xyz):
+    c = xyz - xyz.mean(axis=0)
+    return float(np.sqrt((c * c).sum(axis=1).mean()))
+
+
+def _frames(ch):
+    """(N, CA, C) per residue and the backbone-phase atoms of a built chain."""
+    ridx = np.asarray(ch.res_idx)
+    first = np.searchsorted(ridx, np.arange(len(ch.sequence) + 1))
+    frames, bbpos = [], []
+    for r, res in enumerate(ch.sequence):
+        a0, a1 = first[r], first[r + 1]
+        names = ch.atomnames[a0:a1]
+        frames.append((ch.xyz[a0], ch.xyz[a0 + 1], ch.xyz[a0 + 2]))
+        keep = [k for k, nm in enumerate(names) if nm in _BB_ATOMS and not (nm == "CD" and res != "PRO")]
+        bbpos.append((ch.xyz[a0:a1][keep], np.array([not names[k].startswith("H") for k in keep])))
+    return frames, bbpos
+
+
+def _torsion(a, b, c, d):
+    b1, b2, b3 = b - a, c - b, d - c
+    n1, n2 = np.cross(b1, b2), np.cross(b2, b3)
+    return math.degrees(math.atan2(np.linalg.norm(b2) * np.dot(b1, n2), np.dot(n1, n2)))
+
+
+def collapse(ch: Chain, seed, rg_target, moves=4000, k_rg=1.0, ca_clash=4.2, k_clash=5.0, temp=1.0):
+    """Seeded backbone collapse: torsion Monte Carlo on the C-alpha trace
+    (phi/psi pivots) with the energy k_rg (Rg_CA - rg_target)^2 +
+    k_clash sum (ca_clash - d)^2 over C-alpha pairs >= 3 residues apart, then
+    a rebuild from the resulting phi/psi and a sidechain repack.  Rg is
+    measured on C-alpha atoms."""
+    from scipy.spatial import cKDTree
+
+    rng = np.random.default_rng(seed)
+    n_res = len(ch.sequence)
+    ridx = np.asarray(ch.res_idx)
+    first = np.searchsorted(ridx, np.arange(n_res + 1))
+    bbn = np.stack([ch.xyz[first[r]:first[r] + 3] for r in range(n_res)])  # [n_res, 3(N,CA,C), 3]
+    X = bbn.reshape(-1, 3).copy()
+
+    def energy(X):
+        ca = X[1::3]
+        e = k_rg * (radius_of_gyration(ca) - rg_target) ** 2
+        pairs = cKDTree(ca).query_pairs(ca_clash, output_type="ndarray")
+        if len(pairs):
+            far = np.abs(pairs[:, 0] - pairs[:, 1]) >= 3
+            d = np.linalg.norm(ca[pairs[far, 0]] - ca[pairs[far, 1]], axis=1)
+            e += k_clash * float(((ca_clash - d) ** 2).sum())
+        return e
+
+    E = energy(X)
+    for _ in range(moves):
+        r = int(rng.integers(1, n_res - 1))
+        is_phi = rng.random() < 0.5 and ch.sequence[r] != "PRO"
+        a, b = (3 * r, 3 * r + 1) if is_phi else (3 * r + 1, 3 * r + 2)
+        side = np.arange(b + 1, X.shape[0])
+        if side.size > X.shape[0] // 2:
+            side = np.arange(0, a)
+        delta = math.radians(rng.uniform(-90.0, 90.0))
+        o = X[a]
+        u = X[b] - o
+        u /= np.linalg.norm(u)
+        v = X[side] - o
+        c, s = math.cos(delta), math.sin(delta)
+        trial = X.copy()
+        trial[side] = o + v * c + np.cross(u, v) * s + np.outer(v @ u, u) * (1 - c)
+        Et = energy(trial)
+        if Et < E or rng.random() < math.exp(-(Et - E) / temp):
+            X, E = trial, Et
+    N, CA, C = X[0::3], X[1::3], X[2::3]
+    phi = ch.phi.copy()
+    psi = ch.psi.copy()
+    for r in range(n_res):
+        if r > 0 and ch.sequence[r] != "PRO":
+            phi[r] = _torsion(C[r - 1], N[r], CA[r], C[r])
+        if r + 1 < n_res:
+            psi[r] = _torsion(N[r], CA[r], C[r], N[r + 1])
+    bb_only = build(ch.sequence, phi, psi, chis=ch.chis)
+    frames, bbpos = _frames(bb_only)
+    return pack_sidechains(ch.sequence, phi, psi, frames, bbpos, rng)
+
+
+def compact_chain(n_res, seed, rg_target=None, moves=4000):
+    """A collapsed chain (default C-alpha Rg target 2.2 * n_res^0.38 Å)."""
+    ch = coil_chain(n_res, seed)
+    if rg_target is None:
+        rg_target = 2.2 * n_res ** 0.38
+    return collapse(ch, seed + 7919, rg_target, moves=moves)

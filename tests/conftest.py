@@ -1,0 +1,80 @@
+import json
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PKG_DIR = os.path.join(ROOT, "protein-structure-analysis_b200")
+ORACLE_DIR = os.path.join(ROOT, "oracle")
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+for p in (PKG_DIR, ORACLE_DIR, ROOT):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA sm_100 device")
+
+
+def _ensure_built():
+    lib = os.path.join(PKG_DIR, "protein_physics_b200", "libalma_b200.so")
+    if not os.path.exists(lib):
+        subprocess.run([sys.executable, os.path.join(PKG_DIR, "build.py")], check=True)
+    if not os.path.exists(os.path.join(ORACLE_DIR, "alma_oracle.so")):
+        subprocess.run(["make", "-s", "-C", ORACLE_DIR, "oracle"], check=True)
+
+
+_ensure_built()
+
+
+class Golden:
+    """One golden system: inputs + reference outputs (tests/golden/*.npz)."""
+
+    def __init__(self, name):
+        self.name = name
+        d = np.load(os.path.join(GOLDEN, name + ".npz"))
+        self.d = {k: d[k] for k in d.files}
+        with open(os.path.join(GOLDEN, name + ".names.json")) as f:
+            m = json.load(f)
+        self.resnames, self.atomnames, self.res_idx = m["resnames"], m["atomnames"], m["res_idx"]
+
+    def __getitem__(self, k):
+        return self.d[k]
+
+    @property
+    def n(self):
+        return int(self.d["xyz"].shape[0])
+
+    def topology(self):
+        from protein_physics_b200.topology import BondTopology
+        T = BondTopology()
+        T.build(self.resnames, self.atomnames, self.res_idx)
+        for i, j in self.d["ss_in"]:
+            T.add_disulfide(int(i), int(j))
+        T.identify_concerted_sidechain_pairs(self.d["xyz"])
+        return T
+
+
+GOLDEN_SYSTEMS = ("xq8", "insulin", "synth64")
+
+
+@pytest.fixture(scope="session", params=GOLDEN_SYSTEMS)
+def golden(request):
+    return Golden(request.param)
+
+
+@pytest.fixture(scope="session")
+def oracle():
+    from oracle import Oracle
+    return Oracle()
+
+
+def gpu_available():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False

@@ -1,0 +1,81 @@
+"""The C-ABI library loads and exports every entry point include/*.h
+declares; host-side helpers behave (no GPU needed)."""
+import ctypes
+import glob
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+
+def declared_symbols():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        src = open(h).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        for m in re.finditer(r"^\s*(?:const\s+)?[\w\s\*]+?\b(alma_\w+)\s*\(", src, flags=re.M):
+            names.add(m.group(1))
+    return sorted(names)
+
+
+def test_library_exports_every_declared_symbol():
+    from protein_physics_b200 import _lib
+    L = _lib.lib()
+    syms = declared_symbols()
+    assert len(syms) >= 10
+    missing = [s for s in syms if not hasattr(L, s)]
+    assert not missing, missing
+    assert L.alma_abi_version() == 1
+
+
+def test_reference_params():
+    from protein_physics_b200 import _lib
+    p = _lib.reference_params()
+    assert p.coulomb == 332.0636 and p.kappa == 0.1257 and p.gamma_sa == 0.00542 and p.hard_frac == 0.6
+    assert p.nl_rcut2 == 196.0 and p.pair_cut2 == 144.0 and p.half_skin2 == 1.0
+
+
+def test_errors_are_reported():
+    from protein_physics_b200 import _lib
+    L = _lib.lib()
+    rc = L.alma_nl_build(None, None, None, None, None, 0, None)
+    assert rc == _lib.ALMA_EINVAL
+    assert b"alma_nl_build" in L.alma_last_error()
+    with pytest.raises(ValueError):
+        _lib.check(rc, "x")
+
+
+def test_topo_sides_dfs_order():
+    from protein_physics_b200 import _lib
+    # path 0-1-2-3 with a branch 2-4: side of (1,2) from 2 = [2, 4, 3] (stack order)
+    adj = [[1], [0, 2], [1, 3, 4], [2], [2]]
+    ptr = np.zeros(6, np.int64)
+    ptr[1:] = np.cumsum([len(a) for a in adj])
+    idx = np.array([j for a in adj for j in a], np.int32)
+    sides = _lib.topo_sides(5, ptr, idx, [(1, 2), (0, 1), (2, 1)])
+    assert sides[0] == [2, 4, 3]
+    assert sorted(sides[1]) == [1, 2, 3, 4]
+    assert sorted(sides[2]) == [0, 1]
+    lo, hi, cnt, ex_ptr, ex_idx = _lib.topo_sides_compact(5, ptr, idx, [(1, 2), (0, 1), (2, 1)])
+    assert list(cnt) == [3, 4, 2]
+    assert (lo[0], hi[0]) == (2, 5) and ex_ptr[1] == 0
+    assert (lo[1], hi[1]) == (1, 5)
+
+
+def test_workspace_sizes_are_monotone():
+    from protein_physics_b200 import _lib
+    L = _lib.lib()
+    assert L.alma_nl_workspace_bytes(1, 1000, 10000) < L.alma_nl_workspace_bytes(2, 2000, 20000)
+    assert L.alma_move_scratch_bytes(100) < L.alma_move_scratch_bytes(1000)
+
+
+def test_engine_fails_loudly_without_gpu():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from protein_physics_b200 import Particle, PhysicsEngine
+    with pytest.raises(RuntimeError):
+        PhysicsEngine().calculate_potential([Particle(0, 0, 0, 1.0), Particle(3, 0, 0, -1.0)])

@@ -1,0 +1,167 @@
+"""GPU parity: the sm_100a kernels (through the C ABI) against the oracle
+and the reference's golden vectors.
+
+Bars (the reference's own path is FP64):
+  * neighbor lists, exclusion flags: bit-exact, row order included;
+  * FP64 mode: energies 1e-10 relative, Born radii 1e-12 relative,
+    move ΔE 1e-7 kcal/mol absolute (summation order differs only);
+  * mixed mode (FP32 pair terms, FP64 accumulation): total energy 1e-6
+    relative; move ΔE 1e-4 kcal/mol absolute on the PDB systems.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def _batch(golden, precision="mixed", topo=True):
+    from protein_physics_b200.device import DeviceBatch
+    from protein_physics_b200.topology import flatten
+    flat = flatten(golden.topology()) if topo else None
+    return DeviceBatch([(golden["xyz"], golden["q"], golden["r"], golden["eps"], flat)], precision=precision)
+
+
+def test_nl_bit_exact(golden, oracle):
+    b = _batch(golden)
+    b.build_nl()
+    rp, cols, flags = b.nl_host(0, half=True)
+    ptr, ocols = oracle.nl_build(golden["xyz"])
+    assert np.array_equal(rp, ptr)
+    assert np.array_equal(cols, ocols)  # row order included (SASA depends on it)
+    # exclusion flags = the topology's exclusion test
+    from oracle import TopoArrays
+    from protein_physics_b200.topology import flatten
+    T = golden.topology()
+    ex = np.array([T.is_excluded(i, int(j)) for i in range(golden.n) for j in ocols[ptr[i]:ptr[i + 1]]], np.uint8)
+    assert np.array_equal(flags, ex)
+    # full rows: both directions, same sets
+    frp, fcols, _ = b.nl_host(0, half=False)
+    for i in range(0, golden.n, max(1, golden.n // 97)):
+        half_i = set(ocols[ptr[i]:ptr[i + 1]].tolist())
+        lower = {k for k in range(i) if i in set(ocols[ptr[k]:ptr[k + 1]].tolist())}
+        assert set(fcols[frp[i]:frp[i + 1]].tolist()) == half_i | lower
+
+
+@pytest.mark.parametrize("precision,rtol", [("fp64", 1e-12), ("mixed", 2e-6)])
+def test_born_radii(golden, oracle, precision, rtol):
+    b = _batch(golden, precision)
+    b.build_nl()
+    b.born_radii()
+    a = b.born[:golden.n].cpu().numpy()
+    np.testing.assert_allclose(a, golden["born"], rtol=rtol, atol=0)
+
+
+@pytest.mark.parametrize("precision,rtol", [("fp64", 1e-10), ("mixed", 1e-6)])
+def test_energy_terms(golden, precision, rtol):
+    b = _batch(golden, precision)
+    terms = b.energy_terms()[0].cpu().numpy()
+    ref = golden["energy_topo"]
+    assert abs(terms[4] - ref[4]) <= rtol * abs(ref[4])
+    np.testing.assert_allclose(terms[:3], ref[:3], rtol=1e-10, atol=1e-9)  # SASA/dihedral/SS are FP64 always
+    b2 = _batch(golden, precision, topo=False)
+    t2 = b2.energy_terms()[0].cpu().numpy()
+    assert abs(t2[4] - golden["energy_notopo"][4]) <= rtol * abs(golden["energy_notopo"][4])
+
+
+def test_bridge_case():
+    import json
+    import os
+    from conftest import GOLDEN
+    from protein_physics_b200 import Particle, PhysicsEngine
+    g = json.load(open(os.path.join(GOLDEN, "bridge.json")))
+    P = [Particle(*x, q) for x, q in zip(g["xyz"], g["q"])]
+    assert PhysicsEngine(precision="fp64").calculate_potential(P) == pytest.approx(g["energy"], rel=1e-12)
+    assert PhysicsEngine().calculate_potential(P) == pytest.approx(g["energy"], rel=1e-6)
+
+
+def _move_args(golden, T, kind, code):
+    if kind == 0:
+        return 0, int(code)
+    phi_k, psi_k = divmod(int(code), 100000)
+    return 1, sorted(T.concerted_pairs).index((phi_k, psi_k))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_move_dE_vs_reference(golden, precision):
+    T = golden.topology()
+    b = _batch(golden, precision)
+    b.build_nl()
+    b.born_radii()
+    errs = []
+    for kind, code, delta, dE_ref, *terms_ref in golden["moves"]:
+        k, a = _move_args(golden, T, int(kind), code)
+        dE, dterms = b.move_dE([k], [a], [[delta, 0.0]])
+        dE = float(dE[0].item())
+        dterms = dterms[0].cpu().numpy()
+        if precision == "fp64":
+            assert dE == pytest.approx(dE_ref, abs=1e-7 + 1e-12 * abs(dE_ref))
+            np.testing.assert_allclose(dterms, terms_ref, atol=1e-7, rtol=1e-12)
+        else:
+            scale = np.sum(np.abs(terms_ref))
+            tol = 1e-4 if golden.name != "synth64" else max(1e-4, 2e-7 * scale)
+            assert abs(dE - dE_ref) <= tol, (kind, code, dE, dE_ref)
+            np.testing.assert_allclose(dterms[1:], terms_ref[1:], atol=1e-8, rtol=1e-11)  # SASA/dih/SS FP64
+        errs.append(abs(dE - dE_ref))
+    # the state must be unchanged after non-applied proposals
+    assert np.array_equal(b.coords(0), golden["xyz"])
+
+
+def test_move_apply_matches_oracle(golden, oracle):
+    from oracle import TopoArrays
+    from protein_physics_b200.topology import flatten
+    T = golden.topology()
+    flat = flatten(T)
+    b = _batch(golden, "fp64")
+    b.build_nl()
+    b.born_radii()
+    x, q, r, e = golden["xyz"], golden["q"], golden["r"], golden["eps"]
+    nl = oracle.nl_build(x)
+    a = oracle.born_radii(x, r, nl)
+    k = int(np.argmax([len(s) for s in T.rot_bond_sides]) // 2)
+    side = T.rot_bond_sides[k]
+    group = np.zeros(golden.n, np.int8)
+    group[side] = 1
+    dE_o, _, new_xyz, new_a = oracle.move_dE(x, q, r, e, nl, a, TopoArrays(flat), [(T.rot_bonds[k].i, T.rot_bonds[k].j,
+                                                                                    0.2, side)], group)
+    dE, _ = b.move_dE([0], [k], [[0.2, 0.0]], apply=True)
+    assert float(dE[0]) == pytest.approx(dE_o, abs=1e-7)
+    np.testing.assert_allclose(b.coords(0), new_xyz, rtol=0, atol=1e-12)
+    np.testing.assert_allclose(b.born[:golden.n].cpu().numpy(), new_a, rtol=1e-12, atol=0)
+
+
+def test_batched_equals_single():
+    from conftest import Golden
+    from protein_physics_b200.device import DeviceBatch
+    from protein_physics_b200.topology import flatten
+    gs = [Golden(n) for n in ("xq8", "insulin", "synth64")]
+    systems = [(g["xyz"], g["q"], g["r"], g["eps"], flatten(g.topology())) for g in gs]
+    B = DeviceBatch(systems)
+    tb = B.energy_terms().cpu().numpy()
+    for s, sysd in enumerate(systems):
+        S = DeviceBatch([sysd])
+        ts = S.energy_terms().cpu().numpy()[0]
+        assert np.array_equal(ts, tb[s])  # bit-identical: same per-atom work, same reduction order
+        rp_b, c_b, f_b = B.nl_host(s)
+        rp_s, c_s, f_s = S.nl_host(0)
+        assert np.array_equal(rp_b, rp_s) and np.array_equal(c_b, c_s) and np.array_equal(f_b, f_s)
+
+
+def test_deterministic():
+    from conftest import Golden
+    g = Golden("xq8")
+    r1 = _batch(g).energy_terms().cpu().numpy()
+    r2 = _batch(g).energy_terms().cpu().numpy()
+    assert np.array_equal(r1, r2)
+
+
+def test_dropin_api(golden):
+    from protein_physics_b200 import Particle, PhysicsEngine
+    P = [Particle(*x, q, r, e) for x, q, r, e in zip(golden["xyz"], golden["q"], golden["r"], golden["eps"])]
+    eng = PhysicsEngine()
+    E = eng.calculate_potential(P, golden.topology())
+    assert E == pytest.approx(golden["energy_topo"][4], rel=1e-6)
+    assert eng.calculate_potential(P) == pytest.approx(golden["energy_notopo"][4], rel=1e-6)
+    assert eng.calculate_potential([]) == 0.0
+    assert "B200" in PhysicsEngine.device_name() or len(PhysicsEngine.device_name()) > 0

@@ -1,0 +1,99 @@
+"""Pins the oracle (oracle/alma_oracle.c, the FP64 C restatement) to the
+reference: every golden vector in tests/golden/ was produced by the
+reference engine compiled from its own sources (make_golden.py).
+
+Tolerances: neighbor lists bit-exact (order included); Born radii 1e-12
+relative; energies 1e-10 relative (the reference build uses -ffast-math,
+the oracle strict IEEE: only last-bit rounding differs); move ΔE 1e-8
+kcal/mol absolute.
+"""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def test_bridge_case(oracle):
+    """tests/bridge_test.py of the reference: 3 particles, no topology."""
+    with open(os.path.join(GOLDEN, "bridge.json")) as f:
+        g = json.load(f)
+    xyz = np.array(g["xyz"], float)
+    terms = oracle.calculate_potential(xyz, np.array(g["q"]), np.full(3, g["radius"]), np.full(3, g["epsilon"]))
+    assert terms[4] == pytest.approx(g["energy"], rel=1e-12)
+    assert g["energy"] == pytest.approx(43.20215093684962, rel=1e-14)
+
+
+def test_empty_and_single(oracle):
+    assert oracle.calculate_potential(np.zeros((0, 3)), [], [], [])[4] == 0.0
+    t = oracle.calculate_potential(np.zeros((1, 3)), [1.0], [1.9], [0.1])
+    # one atom: SASA of a free sphere only
+    assert t[3] == 0.0 and t[0] == pytest.approx(0.92 + 0.00542 * 4 * np.pi * 3.3 ** 2)
+
+
+def test_nl_bit_exact(golden, oracle):
+    ptr, cols = oracle.nl_build(golden["xyz"])
+    assert np.array_equal(np.diff(ptr).astype(np.int32), golden["nl_row_cnt"])
+    assert sha(cols.astype(np.int32)) == str(golden["nl_sha"])
+    if "nl_cols" in golden.d:
+        assert np.array_equal(cols, golden["nl_cols"])
+
+
+def test_born_radii(golden, oracle):
+    nl = oracle.nl_build(golden["xyz"])
+    a = oracle.born_radii(golden["xyz"], golden["r"], nl)
+    np.testing.assert_allclose(a, golden["born"], rtol=1e-12, atol=0)
+
+
+def _topo_arrays(golden):
+    from oracle import TopoArrays
+    from protein_physics_b200.topology import flatten
+    return TopoArrays(flatten(golden.topology()))
+
+
+def test_energy_terms(golden, oracle):
+    nl = oracle.nl_build(golden["xyz"])
+    a = oracle.born_radii(golden["xyz"], golden["r"], nl)
+    terms = oracle.energy(golden["xyz"], golden["q"], golden["r"], golden["eps"], nl, a, _topo_arrays(golden))
+    np.testing.assert_allclose(terms, golden["energy_topo"], rtol=1e-10, atol=1e-9)
+    t0 = oracle.energy(golden["xyz"], golden["q"], golden["r"], golden["eps"], nl, a, None)
+    np.testing.assert_allclose(t0, golden["energy_notopo"], rtol=1e-10, atol=1e-9)
+
+
+def _move_rotations(T, flat, kind, code, delta):
+    """Oracle rotation list + groups for a golden move record."""
+    n = flat.n
+    group = np.zeros(n, np.int8)
+    sides = T.rot_bond_sides
+    rbs = T.rot_bonds
+    if kind == 0:
+        k = int(code)
+        side = sides[k]
+        group[side] = 1
+        return [(rbs[k].i, rbs[k].j, delta, side)], group
+    phi_k, psi_k = divmod(int(code), 100000)
+    group[sides[phi_k]] = 1
+    return [(rbs[phi_k].i, rbs[phi_k].j, delta, sides[phi_k]), (rbs[psi_k].i, rbs[psi_k].j, -delta, sides[psi_k])], group
+
+
+def test_move_dE(golden, oracle):
+    from oracle import TopoArrays
+    from protein_physics_b200.topology import flatten
+    T = golden.topology()
+    flat = flatten(T)
+    TA = TopoArrays(flat)
+    x, q, r, e = golden["xyz"], golden["q"], golden["r"], golden["eps"]
+    nl = oracle.nl_build(x)
+    a = oracle.born_radii(x, r, nl)
+    for kind, code, delta, dE_ref, *terms_ref in golden["moves"]:
+        rots, group = _move_rotations(T, flat, int(kind), code, float(delta))
+        dE, terms, _, _ = oracle.move_dE(x, q, r, e, nl, a, TA, rots, group)
+        assert dE == pytest.approx(dE_ref, abs=1e-8 + 1e-11 * abs(dE_ref)), (kind, code)
+        np.testing.assert_allclose(terms, terms_ref, atol=1e-8, rtol=1e-11)
