@@ -134,6 +134,8 @@ typedef struct {
 /* ---- library ------------------------------------------------------------ */
 int alma_abi_version(void);
 const char *alma_last_error(void);
+/* Kernel launches the library has issued since load (all threads). */
+long long alma_launch_count(void);
 /* Reference preset (P1: 0.6 sigma smooth capped hard core, gamma 0.00542). */
 void alma_params_reference(AlmaParams *p);
 /* Bytes of device workspace alma_nl_build needs for a batch. */
@@ -165,25 +167,31 @@ int alma_nl_build(const AlmaBatch *b, const AlmaTopo *t, AlmaNL *nl, const uint8
 
 /* Effective Born radii over the full rows (replaces born_radii,
  * physics_engine.cpp:2024-2039, and born_sum/born_finalize kernels,
- * physics_engine_cuda.cu:537-578).  Writes b->born. */
+ * physics_engine_cuda.cu:537-578).  Writes b->born for the systems with a
+ * nonzero sys_mask entry (device uint8[nsys]; NULL: all). */
 int alma_born_radii(const AlmaBatch *b, const AlmaNL *nl, const AlmaParams *p, int prec,
-                    void *stream);
+                    const uint8_t *sys_mask, void *stream);
 
 /* Per-system energy terms (replaces total_e / calculate_potential,
  * physics_engine.cpp:2205-2248, and pair_energy_kernel,
  * physics_engine_cuda.cu:587-617).  terms: device double[nsys*5] =
  * {sasa, dihedral, disulfide, pair sum, total} per system.  t may be NULL
- * (no exclusions / dihedrals / disulfides).  atom_e: optional device
- * double[natoms] scratch (NULL: allocated internally per call is NOT done —
- * it must be given). */
+ * (no exclusions / dihedrals / disulfides).  sys_mask as above (terms of
+ * other systems are left untouched).  atom_e: device double[natoms*2]
+ * scratch (per-atom pair and SASA contributions). */
 int alma_energy(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *nl, const AlmaParams *p,
-                int prec, double *atom_e, double *terms, void *stream);
+                int prec, const uint8_t *sys_mask, double *atom_e, double *terms, void *stream);
 
 /* Device scratch for the move / MC kernels: alma_move_scratch_bytes(natoms)
  * bytes, zeroed once by alma_move_scratch_init; every call leaves it zeroed.
  * Calls that share a scratch buffer must not overlap on the GPU. */
 size_t alma_move_scratch_bytes(int32_t natoms);
 int alma_move_scratch_init(void *scratch, int32_t natoms, void *stream);
+/* Cumulative work of the move / MC kernels per system (host out[4*nsys]):
+ * {pair-term evaluations, hct evaluations, SASA neighbour visits, moved
+ * atoms}.  Synchronises the stream. */
+int alma_move_counters(const void *scratch, int32_t natoms, int32_t nsys, unsigned long long *out,
+                       void *stream);
 
 /* ΔE of one proposal per system, replayed for a given move (the ΔE core of
  * try_torsion / try_crankshaft / the concerted sidechain move,
@@ -199,6 +207,48 @@ int alma_move_scratch_init(void *scratch, int32_t natoms, void *stream);
 int alma_move_dE(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *nl, const AlmaParams *p,
                  int prec, void *scratch, const int32_t *move_kind, const int32_t *move_a,
                  const double *move_delta, int apply, double *dE, double *dterms, void *stream);
+
+/* ---- device Monte Carlo ------------------------------------------------- */
+/* Proposal policy (the MC loop of generate_ensemble / run_landscape_*,
+ * physics_engine.cpp:2273-2543, :2557-3270). */
+typedef struct {
+    uint64_t seed;            /* Philox key; every run reproducible from it  */
+    int32_t policy;           /* 0 generate_ensemble, 1 landscape, 2 torsion */
+    int32_t tune_freq;        /* 200; 0 disables the cur_max adaptation      */
+    double target_lo, target_hi;  /* 0.28, 0.52                              */
+    double scale_up, scale_down;  /* 1.06, 0.94                              */
+    double angle_max, angle_min;  /* 0.5, 0.004 rad                          */
+    double sidechain_mult;    /* 2.5                                         */
+    double crank_prob;        /* 0.25                                        */
+    double concerted_prob;    /* 0.15 (policy 1)                             */
+    double fixed_delta;       /* > 0: angles ~ U(-fixed_delta, fixed_delta)  */
+    const int32_t *moveset_off;   /* optional [nsys+1] device: torsion moves */
+    const int32_t *moveset;       /* drawn from these local rot-bond indices */
+} AlmaMCConfig;
+
+/* Per-system chain state, device memory, one per system (72 bytes). */
+typedef struct {
+    double cur_max;           /* adaptive max angle (rad)                    */
+    double energy;            /* running energy: last full evaluation + ΣΔE  */
+    double temperature;       /* kcal/mol                                    */
+    int64_t step;             /* proposals drawn (the RNG counter)           */
+    int64_t n_proposed, n_accepted, n_rebuild;
+    int32_t acc_win, tot_win; /* adaptation window                           */
+    int32_t need_rebuild;     /* set when an accepted move drifted > skin/2  */
+    int32_t pad;
+} AlmaChainState;
+
+/* Runs proposals on every system until its state.step reaches step_limit
+ * or it needs a neighbor-list rebuild (one CTA per system, no host sync).
+ * The caller then rebuilds flagged systems (alma_nl_build + alma_born_radii
+ * + alma_energy with their mask), calls alma_mc_after_rebuild, and calls
+ * again.  Scratch as for alma_move_dE. */
+int alma_mc_run(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *nl, const AlmaParams *p, int prec,
+                void *scratch, const AlmaMCConfig *cfg, AlmaChainState *states, int64_t step_limit,
+                void *stream);
+/* state.energy <- terms[5*s+4], need_rebuild <- 0 for masked systems. */
+int alma_mc_after_rebuild(AlmaChainState *states, const double *terms, const uint8_t *sys_mask,
+                          int32_t nsys, void *stream);
 
 #ifdef __cplusplus
 }

@@ -394,3 +394,186 @@ done:
     free(st); free(aa);
     return result;
 }
+
+
+/* ---- Monte Carlo driver (see alma_oracle.h) ----------------------------------- */
+/* Philox4x32-10: Salmon, Moraes, Dror, Shaw, SC'11. */
+void or_philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1, uint32_t *out) {
+    const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u, W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+    for (int r = 0; r < 10; ++r) {
+        uint64_t p0 = (uint64_t)M0 * c0, p1 = (uint64_t)M1 * c2;
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0, hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        uint32_t n0 = hi1 ^ c1 ^ k0, n1 = lo1, n2 = hi0 ^ c3 ^ k1, n3 = lo0;
+        c0 = n0; c1 = n1; c2 = n2; c3 = n3;
+        k0 += W0; k1 += W1;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+static double u01(uint32_t a, uint32_t b) {
+    return (double)(((uint64_t)(a >> 5) << 26) | (uint64_t)(b >> 6)) * (1.0 / 9007199254740992.0);
+}
+
+static int pick_index(double u, int n) {
+    int k = (int)(u * (double)n);
+    return k < n ? k : n - 1;
+}
+
+typedef struct {
+    int64_t *row_ptr;
+    int32_t *cols;
+    int64_t cap;
+    double *ref;
+} mc_nl;
+
+static void mc_rebuild(or_mc_sys *S, mc_nl *nl, or_mc_state *st) {
+    int64_t m = or_nl_build(S->n, S->xyz, nl->row_ptr, nl->cols, nl->cap);
+    if (m < 0) {
+        free(nl->cols);
+        nl->cap = -m + 1024;
+        nl->cols = malloc(sizeof(int32_t) * (size_t)nl->cap);
+        or_nl_build(S->n, S->xyz, nl->row_ptr, nl->cols, nl->cap);
+    }
+    memcpy(nl->ref, S->xyz, sizeof(double) * 3 * (size_t)S->n);
+    or_born_radii(S->n, S->xyz, S->radius, nl->row_ptr, nl->cols, S->born);
+    st->energy = or_energy(S->n, S->xyz, S->q, S->radius, S->eps, nl->row_ptr, nl->cols, S->born, S->topo, NULL);
+}
+
+void or_mc_run(or_mc_sys *S, const or_mc_cfg *cfg, or_mc_state *st, int64_t step_limit) {
+    const int n = S->n;
+    mc_nl nl;
+    nl.row_ptr = malloc(sizeof(int64_t) * (size_t)(n + 1));
+    nl.cap = 256 * (int64_t)n + 64;
+    nl.cols = malloc(sizeof(int32_t) * (size_t)nl.cap);
+    nl.ref = malloc(sizeof(double) * 3 * (size_t)n);
+    mc_rebuild(S, &nl, st); /* every call starts from a fresh list, as a chain does */
+    int8_t *group = calloc((size_t)n, 1);
+    double *new_xyz = malloc(sizeof(double) * 3 * (size_t)n);
+    double *new_born = malloc(sizeof(double) * (size_t)n);
+    int32_t axis[4];
+    double dl[2];
+    int64_t rptr[3];
+    int32_t *ridx = malloc(sizeof(int32_t) * 2 * (size_t)n + 8);
+    const uint32_t k0 = (uint32_t)cfg->seed ^ (0x9E3779B9u * (uint32_t)(S->sys_index + 1)),
+                   k1 = (uint32_t)(cfg->seed >> 32);
+    while (st->step < step_limit) {
+        if (st->need_rebuild) {
+            mc_rebuild(S, &nl, st);
+            st->need_rebuild = 0;
+            st->n_rebuild++;
+        }
+        const uint64_t sp = (uint64_t)st->step;
+        uint32_t w0[4], w1[4], w2[4];
+        or_philox((uint32_t)sp, (uint32_t)(sp >> 32), (uint32_t)S->sys_index, 0u, k0, k1, w0);
+        or_philox((uint32_t)sp, (uint32_t)(sp >> 32), (uint32_t)S->sys_index, 1u, k0, k1, w1);
+        or_philox((uint32_t)sp, (uint32_t)(sp >> 32), (uint32_t)S->sys_index, 2u, k0, k1, w2);
+        const double u[6] = {u01(w0[0], w0[1]), u01(w0[2], w0[3]), u01(w1[0], w1[1]),
+                             u01(w1[2], w1[3]), u01(w2[0], w2[1]), u01(w2[2], w2[3])};
+        int conc = 0, crank = 0, kind = -1, nrot = 0;
+        dl[0] = dl[1] = 0.0;
+        if (cfg->policy == 1) {
+            conc = S->ncsp > 0 && u[0] < cfg->concerted_prob;
+            crank = !conc && S->ncp > 0 && u[4] < cfg->crank_prob;
+        } else if (cfg->policy == 0) {
+            crank = S->ncp > 0 && u[0] < cfg->crank_prob;
+        }
+        int ka = -1, kb = -1;
+        if (conc) {
+            kind = 2;
+            const int p = pick_index(u[1], S->ncsp);
+            ka = S->csp[2 * p];
+            kb = S->csp[2 * p + 1];
+            const double da = st->cur_max * cfg->sidechain_mult * S->rb_scale[ka];
+            const double db = st->cur_max * cfg->sidechain_mult * S->rb_scale[kb];
+            dl[0] = -da + 2.0 * da * u[2];
+            dl[1] = -db + 2.0 * db * u[5];
+        } else if (crank) {
+            kind = 1;
+            const int p = pick_index(u[1], S->ncp);
+            ka = S->cp[2 * p];
+            kb = S->cp[2 * p + 1];
+            dl[0] = -st->cur_max + 2.0 * st->cur_max * u[2];
+        } else {
+            const int nset = cfg->nset > 0 ? cfg->nset : S->nrb;
+            if (nset > 0) {
+                kind = 0;
+                const int q = pick_index(u[1], nset);
+                ka = cfg->nset > 0 ? cfg->moveset[q] : q;
+                const int bk = S->rb_kind[ka];
+                double base = (bk == 0 || bk == 1) ? st->cur_max : st->cur_max * cfg->sidechain_mult;
+                base *= S->rb_scale[ka];
+                dl[0] = -base + 2.0 * base * u[2];
+            }
+        }
+        if (cfg->fixed_delta > 0.0) {
+            dl[0] = cfg->fixed_delta * (2.0 * u[2] - 1.0);
+            dl[1] = cfg->fixed_delta * (2.0 * u[5] - 1.0);
+        }
+        if (kind < 0) { st->step++; continue; }
+        /* rotations and groups */
+        int64_t pos = 0;
+        rptr[0] = 0;
+        const int32_t *sa = S->side_idx + S->side_ptr[ka];
+        const int64_t na = S->side_ptr[ka + 1] - S->side_ptr[ka];
+        double rdelta[2];
+        if (kind == 0) {
+            axis[0] = S->rb_ij[2 * ka]; axis[1] = S->rb_ij[2 * ka + 1];
+            rdelta[0] = dl[0];
+            for (int64_t k = 0; k < na; ++k) { ridx[pos++] = sa[k]; group[sa[k]] = 1; }
+            rptr[1] = pos;
+            nrot = 1;
+        } else {
+            const int32_t *sb = S->side_idx + S->side_ptr[kb];
+            const int64_t nb = S->side_ptr[kb + 1] - S->side_ptr[kb];
+            axis[0] = S->rb_ij[2 * ka]; axis[1] = S->rb_ij[2 * ka + 1];
+            axis[2] = S->rb_ij[2 * kb]; axis[3] = S->rb_ij[2 * kb + 1];
+            rdelta[0] = dl[0];
+            rdelta[1] = kind == 1 ? -dl[0] : dl[1];
+            for (int64_t k = 0; k < na; ++k) { ridx[pos++] = sa[k]; group[sa[k]] = 1; }
+            rptr[1] = pos;
+            for (int64_t k = 0; k < nb; ++k) { ridx[pos++] = sb[k]; if (kind == 2) group[sb[k]] = 2; }
+            rptr[2] = pos;
+            nrot = 2;
+            if (na == 0 || nb == 0) { memset(group, 0, (size_t)n); st->step++; continue; }
+        }
+        if (na == 0) { memset(group, 0, (size_t)n); st->step++; continue; }
+        double terms[4];
+        const double dE = or_move_dE(n, S->xyz, S->q, S->radius, S->eps, nl.row_ptr, nl.cols, S->born, S->topo, nrot,
+                                     axis, rdelta, rptr, ridx, group, terms, new_xyz, new_born);
+        if (dE != dE) { /* degenerate axis */
+            memset(group, 0, (size_t)n);
+            st->step++;
+            continue;
+        }
+        const int acc = (dE < 0.0) || (u[3] < exp(-dE / st->temperature));
+        int drift = 0;
+        if (acc) {
+            for (int i = 0; i < n; ++i)
+                if (group[i]) {
+                    S->xyz[3 * i] = new_xyz[3 * i];
+                    S->xyz[3 * i + 1] = new_xyz[3 * i + 1];
+                    S->xyz[3 * i + 2] = new_xyz[3 * i + 2];
+                    S->born[i] = new_born[i];
+                    double dx = S->xyz[3 * i] - nl.ref[3 * i], dy = S->xyz[3 * i + 1] - nl.ref[3 * i + 1],
+                           dz = S->xyz[3 * i + 2] - nl.ref[3 * i + 2];
+                    if (dx * dx + dy * dy + dz * dz > HALF_SKIN2) drift = 1;
+                }
+            st->energy += dE;
+            st->n_accepted++;
+            if (drift) st->need_rebuild = 1;
+        }
+        memset(group, 0, (size_t)n);
+        st->n_proposed++;
+        st->acc_win += acc;
+        if (cfg->tune_freq > 0 && ++st->tot_win == cfg->tune_freq) {
+            const double rate = (double)st->acc_win / (double)cfg->tune_freq;
+            if (rate > cfg->target_hi) st->cur_max = dmin(cfg->angle_max, st->cur_max * cfg->scale_up);
+            else if (rate < cfg->target_lo) st->cur_max = dmax(cfg->angle_min, st->cur_max * cfg->scale_down);
+            st->acc_win = 0;
+            st->tot_win = 0;
+        }
+        st->step++;
+    }
+    free(group); free(new_xyz); free(new_born); free(ridx);
+    free(nl.row_ptr); free(nl.cols); free(nl.ref);
+}

@@ -97,6 +97,53 @@ double or_move_dE(int n, const double *xyz, const double *q, const double *radiu
                   const double *rot_delta, const int64_t *rot_ptr, const int32_t *rot_idx,
                   const int8_t *group, double *terms, double *new_xyz, double *new_a);
 
+/* ---- Monte Carlo driver ------------------------------------------------------
+ * Restates the proposal loop of generate_ensemble / run_landscape_*
+ * (physics_engine.cpp:2273-2543, :2557-2921) with the move draws taken
+ * from Philox4x32-10 (counter = step, key = seed and system) instead of
+ * mt19937, so a run is reproducible and comparable draw for draw with the
+ * device engine's alma_mc_run.  Layout of the state matches AlmaChainState. */
+typedef struct {
+    double cur_max, energy, temperature;
+    int64_t step, n_proposed, n_accepted, n_rebuild;
+    int32_t acc_win, tot_win, need_rebuild, pad;
+} or_mc_state;
+
+typedef struct {
+    uint64_t seed;
+    int policy, tune_freq;
+    double target_lo, target_hi, scale_up, scale_down, angle_max, angle_min;
+    double sidechain_mult, crank_prob, concerted_prob, fixed_delta;
+    int nset;              /* > 0: torsion moves drawn from moveset[0..nset) */
+    const int32_t *moveset;
+} or_mc_cfg;
+
+typedef struct {
+    int n;
+    double *xyz;           /* [3n], updated in place */
+    const double *q, *radius, *eps;
+    double *born;          /* [n], updated in place */
+    const or_topo *topo;
+    int nrb;
+    const int32_t *rb_ij, *rb_kind;
+    const double *rb_scale;
+    const int64_t *side_ptr;   /* [nrb+1] full j-sides, sorted */
+    const int32_t *side_idx;
+    int ncp;
+    const int32_t *cp;         /* [2 ncp] (phi, psi) rot-bond indices */
+    int ncsp;
+    const int32_t *csp;        /* [2 ncsp] */
+    int sys_index;             /* the system number used in the RNG key */
+} or_mc_sys;
+
+/* Advances the chain to step_limit.  Builds the neighbor list, Born radii
+ * and energy on entry (as a chain starts, :2288-2292) and again whenever
+ * the drift flag is set at the start of a step (:2506-2510). */
+void or_mc_run(or_mc_sys *sys, const or_mc_cfg *cfg, or_mc_state *st, int64_t step_limit);
+
+/* Philox4x32-10 block (out[4]). */
+void or_philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1, uint32_t *out);
+
 /* Rodrigues rotation of one point (:1848-1862). */
 void or_rodrigues(double *p, const double *o, const double *u, double c, double s);
 

@@ -157,6 +157,66 @@ class Oracle:
         return dE, terms, new_xyz, new_born
 
 
+class OrMCState(C.Structure):
+    _fields_ = [("cur_max", C.c_double), ("energy", C.c_double), ("temperature", C.c_double),
+                ("step", C.c_int64), ("n_proposed", C.c_int64), ("n_accepted", C.c_int64), ("n_rebuild", C.c_int64),
+                ("acc_win", C.c_int32), ("tot_win", C.c_int32), ("need_rebuild", C.c_int32), ("pad", C.c_int32)]
+
+
+class OrMCCfg(C.Structure):
+    _fields_ = [("seed", C.c_uint64), ("policy", C.c_int), ("tune_freq", C.c_int)] + \
+               [(n, C.c_double) for n in ("target_lo", "target_hi", "scale_up", "scale_down", "angle_max",
+                                          "angle_min", "sidechain_mult", "crank_prob", "concerted_prob",
+                                          "fixed_delta")] + [("nset", C.c_int), ("moveset", _p)]
+
+
+class OrMCSys(C.Structure):
+    _fields_ = [("n", C.c_int), ("xyz", _p), ("q", _p), ("radius", _p), ("eps", _p), ("born", _p), ("topo", _p),
+                ("nrb", C.c_int), ("rb_ij", _p), ("rb_kind", _p), ("rb_scale", _p), ("side_ptr", _p),
+                ("side_idx", _p), ("ncp", C.c_int), ("cp", _p), ("ncsp", C.c_int), ("csp", _p),
+                ("sys_index", C.c_int)]
+
+
+def oracle_mc(orc, flat, xyz, q, radius, eps, seed, steps, temperature=0.6, cur_max=0.12, policy=0,
+              fixed_delta=0.0, moveset=None, sys_index=0, tune_freq=200):
+    """Runs the oracle's MC chain (alma_oracle.c or_mc_run); returns
+    (final xyz [n,3], state dict)."""
+    L = orc.L
+    L.or_mc_run.argtypes = [_p, _p, _p, C.c_int64]
+    n = flat.n
+    keep = []
+
+    def arr(a, dt):
+        a = np.ascontiguousarray(a, dtype=dt)
+        keep.append(a)
+        return a.ctypes.data
+
+    x = np.ascontiguousarray(np.asarray(xyz, np.float64).reshape(-1, 3).copy())
+    born = np.zeros(n)
+    TA = TopoArrays(flat)
+    # full sorted j-sides from the compact form
+    rows = []
+    for k in range(flat.nrb):
+        s = set(range(int(flat.side_lo[k]), int(flat.side_hi[k])))
+        s.update(flat.side_idx[flat.side_ptr[k]:flat.side_ptr[k + 1]].tolist())
+        rows.append(sorted(s))
+    sp = np.zeros(flat.nrb + 1, np.int64)
+    sp[1:] = np.cumsum([len(r) for r in rows])
+    si = np.array([j for r in rows for j in r], np.int32) if sp[-1] else np.zeros(1, np.int32)
+    S = OrMCSys(n, x.ctypes.data, arr(q, np.float64), arr(radius, np.float64), arr(eps, np.float64), born.ctypes.data,
+                C.cast(C.pointer(TA.s), _p), flat.nrb, arr(np.stack([flat.rb_i, flat.rb_j], 1).reshape(-1), np.int32),
+                arr(flat.rb_kind, np.int32), arr(flat.rb_scale, np.float64), arr(sp, np.int64), arr(si, np.int32),
+                int(flat.crank.shape[0]), arr(flat.crank.reshape(-1), np.int32) if flat.crank.size else None,
+                int(flat.conc_sc.shape[0]), arr(flat.conc_sc.reshape(-1), np.int32) if flat.conc_sc.size else None,
+                int(sys_index))
+    cfg = OrMCCfg(int(seed) & ((1 << 64) - 1), int(policy), int(tune_freq), 0.28, 0.52, 1.06, 0.94, 0.5, 0.004,
+                  2.5, 0.25, 0.15, float(fixed_delta), len(moveset) if moveset is not None else 0,
+                  arr(moveset, np.int32) if moveset is not None and len(moveset) else None)
+    st = OrMCState(cur_max, 0.0, temperature, 0, 0, 0, 0, 0, 0, 0, 0)
+    L.or_mc_run(C.byref(S), C.byref(cfg), C.byref(st), int(steps))
+    return x, {f[0]: getattr(st, f[0]) for f in OrMCState._fields_}, born
+
+
 def ref_so_path():
     hits = glob.glob(os.path.join(HERE, "_ref", "protein_physics*.so"))
     return hits[0] if hits else None

@@ -23,11 +23,17 @@ int alma_cuda_error(cudaError_t e, const char *what);
         if (_e != cudaSuccess) return alma_cuda_error(_e, #expr);  \
     } while (0)
 
-#define ALMA_LAUNCH_CHECK(what)                                        \
+// Kernel launches issued by the library (alma_launch_count); every launch
+// site is followed by ALMA_LAUNCH_CHECK(what, number of kernels launched).
+void alma_count_launches(int n);
+
+#define ALMA_LAUNCH_CHECK_N(what, n)                                   \
     do {                                                               \
         cudaError_t _e = cudaGetLastError();                           \
         if (_e != cudaSuccess) return alma_cuda_error(_e, what);       \
+        alma_count_launches(n);                                        \
     } while (0)
+#define ALMA_LAUNCH_CHECK(what) ALMA_LAUNCH_CHECK_N(what, 1)
 
 // ---------------------------------------------------------------------------
 // energy model (physics_engine.cpp:181-196, :2007-2011, :2148-2164)
@@ -99,6 +105,55 @@ __device__ __forceinline__ R pair_energy(const DevParams &P, R r2, R qp, R sig, 
         E += h < (R)P.hard_cap ? h : (R)P.hard_cap;
     }
     return E;
+}
+
+__device__ __forceinline__ float m_expm1(float x) { return expm1f(x); }
+__device__ __forceinline__ double m_expm1(double x) { return expm1(x); }
+__device__ __forceinline__ float m_log1p(float x) { return log1pf(x); }
+__device__ __forceinline__ double m_log1p(double x) { return log1p(x); }
+
+// LJ 12-6 + capped hard core of one pair (r2 in FP64).  Inside sigma the
+// terms grow steeply and are evaluated in FP64; outside, in precision R.
+template <typename R>
+__device__ __forceinline__ double lj_hard(const DevParams &P, double r2, R sig, R eps_prod) {
+    const double sig2 = (double)sig * (double)sig;
+    if (r2 < sig2) {
+        const double s2 = sig2 / r2, s6 = s2 * s2 * s2;
+        double E = 4.0 * sqrt((double)eps_prod) * (s6 * s6 - s6);
+        const double rc2 = sig2 * P.hard_frac * P.hard_frac;
+        if (r2 < rc2) {
+            const double t2 = rc2 / r2, t6 = t2 * t2 * t2, x = t6 * t6 - 1.0;
+            E += fmin(P.hard_scale * x * x, P.hard_cap);
+        }
+        return E;
+    }
+    const R s2 = (R)(sig2 / r2);
+    const R s6 = s2 * s2 * s2;
+    return (double)((R)4 * m_sqrt(eps_prod) * (s6 * s6 - s6));
+}
+
+// Change of one pair's energy between two geometries (old: r2o, Born
+// product aao; new: r2n, aan), both inside the pair cutoff.  Written as a
+// difference so the rounding error scales with the change, not with the
+// pair energy: r2n - r2o comes from FP64 coordinates,
+//   DH: K qq g(ro) expm1(-kappa dr - log1p(dr/ro)),  g(r) = exp(-kappa r)/r
+//   GB: C qq (fo^2 - fn^2) / (fo fn (fo + fn)),  f^2 = r^2 + aa exp(-r^2/4aa)
+// LJ and the hard core are differenced directly (FP64 inside sigma).
+template <typename R>
+__device__ __forceinline__ double pair_delta(const DevParams &P, double r2o, double r2n, R qp, R sig, R eps_prod,
+                                             R aao, R aan) {
+    const double d2 = r2n - r2o;
+    const R ro2 = (R)r2o, rn2 = (R)r2n;
+    const R ro = m_sqrt(ro2), rn = m_sqrt(rn2);
+    const R dr = (R)d2 / (ro + rn);
+    const R kap = (R)P.kappa;
+    const R gdo = (R)P.coulomb_over_epsw * qp / ro * m_exp(-kap * ro);
+    const R ddh = gdo * m_expm1(-kap * dr - m_log1p(dr / ro));
+    const R xo = aao * m_exp(-ro2 / ((R)4 * aao)), xn = aan * m_exp(-rn2 / ((R)4 * aan));
+    const R fo = m_sqrt(ro2 + xo), fn = m_sqrt(rn2 + xn);
+    const R num = (R)(-d2) + (xo - xn);
+    const R dgb = (R)P.gb_coef * qp * num / (fo * fn * (fo + fn));
+    return (double)ddh + (double)dgb + (lj_hard<R>(P, r2n, sig, eps_prod) - lj_hard<R>(P, r2o, sig, eps_prod));
 }
 
 // HCT descreening integral of atom j (radius rj) on atom i (radius ri).
@@ -192,6 +247,17 @@ __host__ __device__ __forceinline__ Philox4 philox4x32_10(uint32_t c0, uint32_t 
 // 53-bit uniform double in [0, 1) from two 32-bit words.
 __host__ __device__ __forceinline__ double u01_from(uint32_t a, uint32_t b) {
     return (double)(((uint64_t)(a >> 5) << 26) | (uint64_t)(b >> 6)) * (1.0 / 9007199254740992.0);
+}
+
+// System of global atom i: binary search in atom_off[nsys+1].
+__device__ __forceinline__ int sys_of_atom(const int32_t *atom_off, int nsys, int i) {
+    int lo = 0, hi = nsys - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (atom_off[mid] <= i) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
 }
 
 __device__ __forceinline__ void set_status(uint32_t *status, uint32_t bit) {

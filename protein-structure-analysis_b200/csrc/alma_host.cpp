@@ -6,13 +6,17 @@
 #include <cstdio>
 #include <cstring>
 #include <algorithm>
+#include <atomic>
 #include <vector>
 
 #include "alma_b200.h"
 
 namespace {
 thread_local char g_err[512] = "";
+std::atomic<long long> g_launches{0};
 }
+
+void alma_count_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 int alma_set_error(int code, const char *fmt, ...) {
     va_list ap;
@@ -31,6 +35,8 @@ extern "C" {
 int alma_abi_version(void) { return ALMA_ABI_VERSION; }
 
 const char *alma_last_error(void) { return g_err; }
+
+long long alma_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
 // Reference preset: physics_engine.cpp:181-196 (hard core 0.6 sigma, smooth
 // and capped at 5000, gamma_SA 0.00542, kappa 0.1257) and the disulfide

@@ -31,13 +31,15 @@ __device__ __forceinline__ void load_prm(const float *prm, const double *prm64, 
 }
 
 template <typename R>
-__global__ void born_kernel(int natoms, const double *__restrict__ xyz, const float *__restrict__ prm,
+__global__ void born_kernel(int natoms, const int32_t *__restrict__ atom_off, int nsys, const uint8_t *__restrict__ mask,
+                            const double *__restrict__ xyz, const float *__restrict__ prm,
                             const double *__restrict__ prm64, const int64_t *__restrict__ full_ptr,
                             const int32_t *__restrict__ full_len, const uint32_t *__restrict__ full_cols,
                             double *__restrict__ born) {
     const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     if (i >= natoms) return;
+    if (mask && !mask[sys_of_atom(atom_off, nsys, i)]) return;
     R qi, ri, ei;
     load_prm<R>(prm, prm64, i, qi, ri, ei);
     const double4 pi = ld_xyz(xyz, i);
@@ -61,13 +63,16 @@ __global__ void born_kernel(int natoms, const double *__restrict__ xyz, const fl
 // Warp per atom: pair energy and SASA of row i.  atom_e[2*i] = pair sum of
 // row i, atom_e[2*i+1] = gamma * max(0, sa_i).
 template <typename R>
-__global__ void pair_sasa_kernel(DevParams P, int natoms, const double *__restrict__ xyz, const float *__restrict__ prm,
+__global__ void pair_sasa_kernel(DevParams P, int natoms, const int32_t *__restrict__ atom_off, int nsys,
+                                 const uint8_t *__restrict__ mask, const double *__restrict__ xyz,
+                                 const float *__restrict__ prm,
                                  const double *__restrict__ prm64, const double *__restrict__ born,
                                  const int64_t *__restrict__ half_ptr, const int32_t *__restrict__ half_len,
                                  const uint32_t *__restrict__ half_cols, int use_excl, double *__restrict__ atom_e) {
     const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     if (i >= natoms) return;
+    if (mask && !mask[sys_of_atom(atom_off, nsys, i)]) return;
     R qi, ri, ei;
     load_prm<R>(prm, prm64, i, qi, ri, ei);
     const R ai = (R)born[i];
@@ -135,9 +140,10 @@ __device__ __forceinline__ double dih_record_energy(const double *xyz, const Alm
 // One CTA per system.
 __global__ void energy_reduce_kernel(DevParams P, const int32_t *__restrict__ atom_off, const double *__restrict__ xyz,
                                      const double *__restrict__ atom_e, AlmaTopo t, int has_topo,
-                                     double *__restrict__ terms) {
+                                     const uint8_t *__restrict__ mask, double *__restrict__ terms) {
     __shared__ double sm[32];
     const int s = blockIdx.x;
+    if (mask && !mask[s]) return;
     const int a0 = atom_off[s], a1 = atom_off[s + 1];
     double ep = 0.0, es = 0.0, ed = 0.0, ess = 0.0;
     for (int i = a0 + threadIdx.x; i < a1; i += blockDim.x) {
@@ -177,7 +183,8 @@ static int check_batch(const AlmaBatch *b, const char *who) {
     return ALMA_OK;
 }
 
-extern "C" int alma_born_radii(const AlmaBatch *b, const AlmaNL *nl, const AlmaParams *p, int prec, void *stream) {
+extern "C" int alma_born_radii(const AlmaBatch *b, const AlmaNL *nl, const AlmaParams *p, int prec,
+                               const uint8_t *sys_mask, void *stream) {
     int rc = check_batch(b, "alma_born_radii");
     if (rc) return rc;
     if (!nl || !nl->full_ptr || !nl->full_cols || !p) return alma_set_error(ALMA_EINVAL, "alma_born_radii: null");
@@ -185,15 +192,15 @@ extern "C" int alma_born_radii(const AlmaBatch *b, const AlmaNL *nl, const AlmaP
     cudaStream_t st = (cudaStream_t)stream;
     const int wpb = 8, nb = (b->natoms + wpb - 1) / wpb;
     if (prec == ALMA_PREC_FP64)
-        born_kernel<double><<<nb, wpb * 32, 0, st>>>(b->natoms, b->xyz, b->prm, b->prm64, nl->full_ptr, nl->full_len, nl->full_cols, b->born);
+        born_kernel<double><<<nb, wpb * 32, 0, st>>>(b->natoms, b->atom_off, b->nsys, sys_mask, b->xyz, b->prm, b->prm64, nl->full_ptr, nl->full_len, nl->full_cols, b->born);
     else
-        born_kernel<float><<<nb, wpb * 32, 0, st>>>(b->natoms, b->xyz, b->prm, b->prm64, nl->full_ptr, nl->full_len, nl->full_cols, b->born);
+        born_kernel<float><<<nb, wpb * 32, 0, st>>>(b->natoms, b->atom_off, b->nsys, sys_mask, b->xyz, b->prm, b->prm64, nl->full_ptr, nl->full_len, nl->full_cols, b->born);
     ALMA_LAUNCH_CHECK("alma_born_radii");
     return ALMA_OK;
 }
 
 extern "C" int alma_energy(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *nl, const AlmaParams *p, int prec,
-                           double *atom_e, double *terms, void *stream) {
+                           const uint8_t *sys_mask, double *atom_e, double *terms, void *stream) {
     int rc = check_batch(b, "alma_energy");
     if (rc) return rc;
     if (!nl || !nl->half_ptr || !nl->half_cols || !p || !atom_e || !terms)
@@ -204,16 +211,16 @@ extern "C" int alma_energy(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *
         const int wpb = 8, nb = (b->natoms + wpb - 1) / wpb;
         const int use_excl = t != nullptr;
         if (prec == ALMA_PREC_FP64)
-            pair_sasa_kernel<double><<<nb, wpb * 32, 0, st>>>(P, b->natoms, b->xyz, b->prm, b->prm64, b->born,
+            pair_sasa_kernel<double><<<nb, wpb * 32, 0, st>>>(P, b->natoms, b->atom_off, b->nsys, sys_mask, b->xyz, b->prm, b->prm64, b->born,
                                                               nl->half_ptr, nl->half_len, nl->half_cols, use_excl, atom_e);
         else
-            pair_sasa_kernel<float><<<nb, wpb * 32, 0, st>>>(P, b->natoms, b->xyz, b->prm, b->prm64, b->born,
+            pair_sasa_kernel<float><<<nb, wpb * 32, 0, st>>>(P, b->natoms, b->atom_off, b->nsys, sys_mask, b->xyz, b->prm, b->prm64, b->born,
                                                              nl->half_ptr, nl->half_len, nl->half_cols, use_excl, atom_e);
     }
     AlmaTopo tt;
     if (t) tt = *t;
     else memset(&tt, 0, sizeof(tt));
-    energy_reduce_kernel<<<b->nsys, 256, 0, st>>>(P, b->atom_off, b->xyz, atom_e, tt, t != nullptr, terms);
-    ALMA_LAUNCH_CHECK("alma_energy");
+    energy_reduce_kernel<<<b->nsys, 256, 0, st>>>(P, b->atom_off, b->xyz, atom_e, tt, t != nullptr, sys_mask, terms);
+    ALMA_LAUNCH_CHECK_N("alma_energy", b->natoms > 0 ? 2 : 1);
     return ALMA_OK;
 }

@@ -1,0 +1,238 @@
+// Device Monte Carlo: one CTA per system runs proposals back to back.
+//
+// Per proposal (the generate_ensemble / run_landscape_* step,
+// physics_engine.cpp:2504-2528, :2880-2921):
+//   draw   Philox4x32-10 keyed by (seed, system), counter = step: move type,
+//          move index, angle(s), Metropolis uniform — reproducible from the
+//          seed (the reference's mt19937 seeded from random_device is not);
+//   move   policy 0 = generate_ensemble: crankshaft with p 0.25 when pairs
+//          exist, else torsion; policy 1 = landscape: concerted sidechain
+//          pair with p 0.15, else crankshaft with p 0.25, else torsion;
+//          policy 2 = torsion only.  Torsion step = cur_max (backbone) or
+//          sidechain_mult * cur_max, times the lever scale
+//          (:2340-2346); crankshaft step cur_max (:2441); concerted steps
+//          2.5 cur_max * scale (:2818-2821); fixed_delta > 0 replaces all
+//          of that by U(-fixed_delta, fixed_delta);
+//   ΔE     move_eval (move.cuh);
+//   test   accept when dE < 0 or u < exp(-dE / T), FP64 (:2387);
+//   commit moved coordinates + half-list Born radii, else discard;
+//   tune   every tune_freq proposals that moved: rate > target_hi ->
+//          cur_max *= scale_up (<= angle_max); rate < target_lo -> *=
+//          scale_down (>= angle_min) (:2515-2526);
+//   drift  an accepted move that takes any moved atom more than the half
+//          skin from its position at the last list build flags the system
+//          for a rebuild (NeighborList::needs_rebuild, :345-351); the CTA
+//          stops at the start of its next step, the host rebuilds the
+//          list, the Born radii and the energy for flagged systems only
+//          (alma_mc_after_rebuild) and relaunches.
+#include "move.cuh"
+
+namespace alma {
+
+struct MCConfigDev {
+    uint64_t seed;
+    int policy, tune_freq;
+    double target_lo, target_hi, scale_up, scale_down, angle_max, angle_min;
+    double sidechain_mult, crank_prob, concerted_prob, fixed_delta;
+    const int32_t *moveset_off, *moveset;
+};
+
+__device__ __forceinline__ int pick(double u, int n) {
+    int k = (int)(u * (double)n);
+    return k < n ? k : n - 1;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(MOVE_THREADS) mc_kernel(MoveCtx C, MCConfigDev cfg, AlmaChainState *__restrict__ states,
+                                                          int64_t step_limit) {
+    __shared__ MoveDesc M;
+    __shared__ double sm[32];
+    __shared__ int naff;
+    __shared__ AlmaChainState S;
+    __shared__ double u[6];
+    __shared__ int did_move, accept;
+    const int s = blockIdx.x;
+    if (threadIdx.x == 0) S = states[s];
+    __syncthreads();
+    const int a0 = C.b.atom_off[s];
+    const int nrb = C.t.rb_off[s + 1] - C.t.rb_off[s];
+    const int ncp = C.t.cp_off[s + 1] - C.t.cp_off[s];
+    const int ncsp = C.t.csp_off[s + 1] - C.t.csp_off[s];
+    const int nset = cfg.moveset_off ? cfg.moveset_off[s + 1] - cfg.moveset_off[s] : nrb;
+    (void)a0;
+    while (S.step < step_limit && !S.need_rebuild) {
+        if (threadIdx.x == 0) {
+            const uint64_t st = (uint64_t)S.step;
+            const uint32_t k0 = (uint32_t)cfg.seed ^ (0x9E3779B9u * (uint32_t)(s + 1)), k1 = (uint32_t)(cfg.seed >> 32);
+            const Philox4 r0 = philox4x32_10((uint32_t)st, (uint32_t)(st >> 32), (uint32_t)s, 0u, k0, k1);
+            const Philox4 r1 = philox4x32_10((uint32_t)st, (uint32_t)(st >> 32), (uint32_t)s, 1u, k0, k1);
+            const Philox4 r2 = philox4x32_10((uint32_t)st, (uint32_t)(st >> 32), (uint32_t)s, 2u, k0, k1);
+            u[0] = u01_from(r0.v[0], r0.v[1]);
+            u[1] = u01_from(r0.v[2], r0.v[3]);
+            u[2] = u01_from(r1.v[0], r1.v[1]);
+            u[3] = u01_from(r1.v[2], r1.v[3]);
+            u[4] = u01_from(r2.v[0], r2.v[1]);
+            u[5] = u01_from(r2.v[2], r2.v[3]);
+            int kind = 0, idx = 0;
+            double delta[2] = {0.0, 0.0};
+            bool conc = false, crank = false;
+            if (cfg.policy == 1) {
+                conc = ncsp > 0 && u[0] < cfg.concerted_prob;
+                crank = !conc && ncp > 0 && u[4] < cfg.crank_prob;
+            } else if (cfg.policy == 0) {
+                crank = ncp > 0 && u[0] < cfg.crank_prob;
+            }
+            if (conc) {
+                kind = 2;
+                idx = pick(u[1], ncsp);
+                const int pi = C.t.csp_off[s] + idx;
+                const double sa = C.t.rb_scale[C.t.rb_off[s] + C.t.csp[2 * pi]];
+                const double sb = C.t.rb_scale[C.t.rb_off[s] + C.t.csp[2 * pi + 1]];
+                const double da = S.cur_max * cfg.sidechain_mult * sa, db = S.cur_max * cfg.sidechain_mult * sb;
+                delta[0] = -da + 2.0 * da * u[2];
+                delta[1] = -db + 2.0 * db * u[5];
+            } else if (crank) {
+                kind = 1;
+                idx = pick(u[1], ncp);
+                delta[0] = -S.cur_max + 2.0 * S.cur_max * u[2];
+            } else if (nset > 0) {
+                kind = 0;
+                const int q = pick(u[1], nset);
+                idx = cfg.moveset_off ? cfg.moveset[cfg.moveset_off[s] + q] : q;
+                const int k = C.t.rb_off[s] + idx;
+                const int bk = C.t.rb_kind[k];
+                double base = (bk == 0 || bk == 1) ? S.cur_max : S.cur_max * cfg.sidechain_mult;
+                base *= C.t.rb_scale[k];
+                delta[0] = -base + 2.0 * base * u[2];
+            } else {
+                kind = -1;
+            }
+            if (cfg.fixed_delta > 0.0) {
+                delta[0] = cfg.fixed_delta * (2.0 * u[2] - 1.0);
+                delta[1] = cfg.fixed_delta * (2.0 * u[5] - 1.0);
+            }
+            if (kind >= 0) decode_move(M, C.t, C.b.xyz, s, kind, idx, delta);
+            else M.degenerate = 1;
+            did_move = !M.degenerate;
+        }
+        __syncthreads();
+        if (!did_move) {
+            if (threadIdx.x == 0) S.step++;
+            __syncthreads();
+            continue;
+        }
+        const MoveResult r = move_eval<R>(C, M, s, sm, &naff);
+        if (threadIdx.x == 0) {
+            const double T = S.temperature;
+            accept = (r.dE < 0.0) || (u[3] < exp(-r.dE / T));
+        }
+        __syncthreads();
+        const int acc = accept;
+        // commit / discard, then the drift test on the committed atoms
+        int drift = 0;
+        {
+            const MoveScratch &w = C.w;
+            const int64_t nm = n_members(M);
+            for (int64_t k = threadIdx.x; k < nm; k += blockDim.x) {
+                int g;
+                const int m = member(M, C.t.side_idx, k, g);
+                if (acc) {
+                    const double4 p = ld_xyz(w.xyz_new, m);
+                    *reinterpret_cast<double4 *>(C.b.xyz + 4 * (size_t)m) = p;
+                    C.b.born[m] = w.born_new[m];
+                    if (d2_of(p, ld_xyz(C.nl.ref_xyz, m)) > C.P.half_skin2) drift = 1;
+                }
+                w.group[m] = 0;
+                w.dE_atom[2 * (size_t)m] = 0.0;
+                w.dE_atom[2 * (size_t)m + 1] = 0.0;
+            }
+            const int na = naff;
+            for (int k = threadIdx.x; k < na; k += blockDim.x) {
+                const int i = w.affected[C.b.atom_off[s] + k];
+                w.mark[i] = 0;
+                w.dE_atom[2 * (size_t)i + 1] = 0.0;
+            }
+        }
+        drift = __syncthreads_or(drift);
+        if (threadIdx.x == 0) {
+            S.n_proposed++;
+            if (acc) {
+                S.n_accepted++;
+                S.energy += r.dE;
+                if (drift) S.need_rebuild = 1;
+            }
+            S.acc_win += acc;
+            if (cfg.tune_freq > 0 && ++S.tot_win == cfg.tune_freq) {
+                const double rate = (double)S.acc_win / (double)cfg.tune_freq;
+                if (rate > cfg.target_hi) S.cur_max = fmin(cfg.angle_max, S.cur_max * cfg.scale_up);
+                else if (rate < cfg.target_lo) S.cur_max = fmax(cfg.angle_min, S.cur_max * cfg.scale_down);
+                S.acc_win = 0;
+                S.tot_win = 0;
+            }
+            S.step++;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) states[s] = S;
+}
+
+// After a rebuild of the flagged systems: energy <- fresh total, flag
+// cleared, rebuild counted.
+__global__ void mc_after_rebuild_kernel(AlmaChainState *__restrict__ states, const double *__restrict__ terms,
+                                        const uint8_t *__restrict__ mask, int nsys) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nsys || (mask && !mask[s])) return;
+    states[s].energy = terms[5 * (size_t)s + 4];
+    if (states[s].need_rebuild) states[s].n_rebuild++;
+    states[s].need_rebuild = 0;
+}
+
+}  // namespace alma
+
+using namespace alma;
+
+int alma_check_move_args(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *nl, const AlmaParams *p,
+                         void *scratch, const char *who);
+MoveCtx alma_make_move_ctx(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *nl, const AlmaParams *p,
+                           void *scratch);
+
+extern "C" int alma_mc_run(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *nl, const AlmaParams *p, int prec,
+                           void *scratch, const AlmaMCConfig *cfg, AlmaChainState *states, int64_t step_limit,
+                           void *stream) {
+    int rc = alma_check_move_args(b, t, nl, p, scratch, "alma_mc_run");
+    if (rc) return rc;
+    if (!cfg || !states) return alma_set_error(ALMA_EINVAL, "alma_mc_run: null config/states");
+    if (cfg->policy < 0 || cfg->policy > 2) return alma_set_error(ALMA_EINVAL, "alma_mc_run: bad policy");
+    const MoveCtx C = alma_make_move_ctx(b, t, nl, p, scratch);
+    MCConfigDev d;
+    d.seed = cfg->seed;
+    d.policy = cfg->policy;
+    d.tune_freq = cfg->tune_freq;
+    d.target_lo = cfg->target_lo;
+    d.target_hi = cfg->target_hi;
+    d.scale_up = cfg->scale_up;
+    d.scale_down = cfg->scale_down;
+    d.angle_max = cfg->angle_max;
+    d.angle_min = cfg->angle_min;
+    d.sidechain_mult = cfg->sidechain_mult;
+    d.crank_prob = cfg->crank_prob;
+    d.concerted_prob = cfg->concerted_prob;
+    d.fixed_delta = cfg->fixed_delta;
+    d.moveset_off = cfg->moveset_off;
+    d.moveset = cfg->moveset;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (prec == ALMA_PREC_FP64)
+        mc_kernel<double><<<b->nsys, MOVE_THREADS, 0, st>>>(C, d, states, step_limit);
+    else
+        mc_kernel<float><<<b->nsys, MOVE_THREADS, 0, st>>>(C, d, states, step_limit);
+    ALMA_LAUNCH_CHECK("alma_mc_run");
+    return ALMA_OK;
+}
+
+extern "C" int alma_mc_after_rebuild(AlmaChainState *states, const double *terms, const uint8_t *sys_mask,
+                                     int32_t nsys, void *stream) {
+    if (!states || !terms || nsys <= 0) return alma_set_error(ALMA_EINVAL, "alma_mc_after_rebuild: bad arguments");
+    mc_after_rebuild_kernel<<<(nsys + 127) / 128, 128, 0, (cudaStream_t)stream>>>(states, terms, sys_mask, nsys);
+    ALMA_LAUNCH_CHECK("alma_mc_after_rebuild");
+    return ALMA_OK;
+}

@@ -19,6 +19,7 @@ static size_t carve_scratch(MoveScratch *w, char *base, int32_t natoms) {
     t.born_new = (double *)take(sizeof(double) * (size_t)natoms);
     t.dE_atom = (double *)take(sizeof(double) * 2 * (size_t)natoms);
     t.affected = (int32_t *)take(sizeof(int32_t) * (size_t)natoms);
+    t.ctr = (unsigned long long *)take(sizeof(unsigned long long) * 4 * (size_t)(natoms + 1));
     if (w) *w = t;
     return off;
 }
@@ -62,6 +63,20 @@ __global__ void __launch_bounds__(MOVE_THREADS) move_dE_kernel(MoveCtx C, const 
 using namespace alma;
 
 extern "C" size_t alma_move_scratch_bytes(int32_t natoms) { return carve_scratch(nullptr, nullptr, natoms); }
+
+// Cumulative work counters of the move kernels, per system: {pair-term
+// evaluations, hct evaluations, SASA neighbour visits, moved atoms}.
+extern "C" int alma_move_counters(const void *scratch, int32_t natoms, int32_t nsys, unsigned long long *out,
+                                  void *stream) {
+    if (!scratch || !out || nsys <= 0 || nsys > natoms + 1)
+        return alma_set_error(ALMA_EINVAL, "alma_move_counters: bad arguments");
+    MoveScratch w;
+    carve_scratch(&w, (char *)scratch, natoms);
+    ALMA_CUDA_TRY(cudaMemcpyAsync(out, w.ctr, sizeof(unsigned long long) * 4 * (size_t)nsys, cudaMemcpyDeviceToHost,
+                                  (cudaStream_t)stream));
+    ALMA_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+    return ALMA_OK;
+}
 
 extern "C" int alma_move_scratch_init(void *scratch, int32_t natoms, void *stream) {
     if (!scratch || natoms < 0) return alma_set_error(ALMA_EINVAL, "alma_move_scratch_init: bad arguments");

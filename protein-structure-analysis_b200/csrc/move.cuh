@@ -37,6 +37,8 @@ struct MoveScratch {
     double *born_new;   // [natoms]
     double *dE_atom;    // [natoms*2]
     int32_t *affected;  // [natoms] compaction list (per-system region)
+    unsigned long long *ctr;  // [4*nsys] cumulative work counters: pair terms,
+                              // hct terms, SASA neighbour visits, moved atoms
 };
 
 // A j-side: sorted explicit atoms side_idx[eb, ee) plus the range [lo, hi).
@@ -280,7 +282,10 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
             sum += (double)hct_term<R>(m_sqrt(r2), r2, rm, rj);
         }
         sum = warp_sum(sum);
-        if (lane == 0) w.born_new[m] = 1.0 / fmax(1.0 / b.prm64[4 * (size_t)m + 1] - 0.5 * sum, 2.0);
+        if (lane == 0) {
+            w.born_new[m] = 1.0 / fmax(1.0 / b.prm64[4 * (size_t)m + 1] - 0.5 * sum, 2.0);
+            atomicAdd(&w.ctr[4 * s + 1], (unsigned long long)C.nl.half_len[m]);
+        }
         for (int64_t e = C.nl.full_ptr[m] + lane; e < C.nl.full_ptr[m] + C.nl.full_len[m]; e += 32) {
             const int j = (int)(C.nl.full_cols[e] & ALMA_IDX_MASK);
             if (j < m && w.group[j] == 0) w.mark[j] = 1;
@@ -297,6 +302,7 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
         prm_of<R>(b.prm, b.prm64, m, qm, rm, em);
         const R amo = (R)b.born[m], amn = (R)w.born_new[m];
         double acc = 0.0;
+        int npair = 0;
         for (int64_t e = C.nl.full_ptr[m] + lane; e < C.nl.full_ptr[m] + C.nl.full_len[m]; e += 32) {
             const uint32_t ent = C.nl.full_cols[e];
             if (ent & ALMA_EXCL_BIT) continue;
@@ -309,14 +315,25 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
             const double4 pjo = ld_xyz(b.xyz, j);
             const double r2o = d2_of(pmo, pjo);
             const R ajo = (R)b.born[j];
-            if (r2o <= C.P.pair_cut2) acc -= (double)pair_energy<R>(C.P, (R)r2o, qp, sig, ep, amo, ajo);
             const double4 pjn = gj ? ld_xyz(w.xyz_new, j) : pjo;
             const double r2n = d2_of(pmn, pjn);
             const R ajn = gj ? (R)w.born_new[j] : ajo;
-            if (r2n <= C.P.pair_cut2) acc += (double)pair_energy<R>(C.P, (R)r2n, qp, sig, ep, amn, ajn);
+            const bool ino = r2o <= C.P.pair_cut2, inn = r2n <= C.P.pair_cut2;
+            npair += (int)ino + (int)inn;
+            if (ino && inn) {
+                acc += pair_delta<R>(C.P, r2o, r2n, qp, sig, ep, amo * ajo, amn * ajn);
+            } else if (ino) {
+                acc -= (double)pair_energy<R>(C.P, (R)r2o, qp, sig, ep, amo, ajo);
+            } else if (inn) {
+                acc += (double)pair_energy<R>(C.P, (R)r2n, qp, sig, ep, amn, ajn);
+            }
         }
         acc = warp_sum(acc);
-        if (lane == 0) w.dE_atom[2 * (size_t)m] = acc;
+        npair = __reduce_add_sync(0xffffffffu, npair);
+        if (lane == 0) {
+            w.dE_atom[2 * (size_t)m] = acc;
+            atomicAdd(&w.ctr[4 * s + 0], (unsigned long long)npair);
+        }
     }
     // Affected fixed atoms -> compaction list (order irrelevant: results go
     // to per-atom slots and are summed in atom order).
@@ -372,7 +389,10 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
                 san -= fmin(san * 0.85, __shfl_sync(0xffffffffu, cn, l));
             }
         }
-        if (lane == 0) w.dE_atom[2 * (size_t)i + 1] = C.P.gamma_sa * (fmax(0.0, san) - fmax(0.0, sao));
+        if (lane == 0) {
+            w.dE_atom[2 * (size_t)i + 1] = C.P.gamma_sa * (fmax(0.0, san) - fmax(0.0, sao));
+            atomicAdd(&w.ctr[4 * s + 2], 2ull * (unsigned long long)(end - beg));
+        }
     }
     // P6: boundary dihedral records and disulfides of system s.
     double ddih = 0.0, dss = 0.0;
@@ -399,6 +419,7 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
         dss += C.P.k_ss * drn * drn - C.P.k_ss * dro * dro;
     }
     __syncthreads();
+    if (tid == 0) atomicAdd(&w.ctr[4 * s + 3], (unsigned long long)nm);
     // P7: deterministic sums.
     double c = 0.0, sa = 0.0;
     for (int i = a0 + tid; i < a1; i += nthr) {

@@ -77,16 +77,6 @@ static size_t carve(NLWork *w, char *base, int32_t nsys, int32_t natoms, int64_t
     return off;
 }
 
-__device__ __forceinline__ int sys_of_atom(const int32_t *atom_off, int nsys, int i) {
-    int lo = 0, hi = nsys - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (atom_off[mid] <= i) lo = mid;
-        else hi = mid - 1;
-    }
-    return lo;
-}
-
 // One CTA per system: bounding box and grid shape (physics_engine.cpp:299-316).
 // A system outside the mask gets a 1x1x1 grid that no atom uses.
 __global__ void nl_grid_kernel(const int32_t *__restrict__ atom_off, const uint8_t *__restrict__ mask,
@@ -386,6 +376,6 @@ extern "C" int alma_nl_build(const AlmaBatch *b, const AlmaTopo *t, AlmaNL *nl, 
     nl_rows_kernel<1><<<rb, wpb * 32, 0, st>>>(b->atom_off, nsys, natoms, sys_mask, b->xyz, rcut2, w.grid, w.ok,
                                                w.cell_of, w.cell_start, w.cell_atoms, w.full_cnt, w.half_cnt, ep, ec,
                                                *nl, w.sys_ok);
-    ALMA_LAUNCH_CHECK("alma_nl_build");
+    ALMA_LAUNCH_CHECK_N("alma_nl_build", 11);
     return ALMA_OK;
 }

@@ -78,6 +78,12 @@ class AlmaChainState(C.Structure):
                 ("acc_win", _i32), ("tot_win", _i32), ("need_rebuild", _i32), ("pad", _i32)]
 
 
+# numpy view of AlmaChainState (72 bytes)
+STATE_DTYPE = np.dtype([("cur_max", "f8"), ("energy", "f8"), ("temperature", "f8"), ("step", "i8"),
+                        ("n_proposed", "i8"), ("n_accepted", "i8"), ("n_rebuild", "i8"), ("acc_win", "i4"),
+                        ("tot_win", "i4"), ("need_rebuild", "i4"), ("pad", "i4")])
+assert STATE_DTYPE.itemsize == C.sizeof(AlmaChainState) == 72
+
 _lib = None
 
 
@@ -92,6 +98,7 @@ def lib():
             "`python protein-structure-analysis_b200/build.py` (nvcc, sm_100a)")
     L = C.CDLL(LIB_PATH)
     L.alma_abi_version.restype = C.c_int
+    L.alma_launch_count.restype = C.c_longlong
     L.alma_last_error.restype = C.c_char_p
     L.alma_params_reference.argtypes = [C.POINTER(AlmaParams)]
     L.alma_nl_workspace_bytes.restype = C.c_size_t
@@ -101,14 +108,13 @@ def lib():
     L.alma_topo_sides.argtypes = [_i32, _p, _p, _i32, _p, _p, _p, _i64]
     L.alma_topo_sides_compact.argtypes = [_i32, _p, _p, _i32, _p, _p, _p, _p, _p, _p, _i64]
     L.alma_nl_build.argtypes = [_p, _p, _p, _p, _p, _i64, _p]
-    L.alma_born_radii.argtypes = [_p, _p, _p, C.c_int, _p]
-    L.alma_energy.argtypes = [_p, _p, _p, _p, C.c_int, _p, _p, _p]
+    L.alma_born_radii.argtypes = [_p, _p, _p, C.c_int, _p, _p]
+    L.alma_energy.argtypes = [_p, _p, _p, _p, C.c_int, _p, _p, _p, _p]
+    L.alma_mc_run.argtypes = [_p, _p, _p, _p, C.c_int, _p, _p, _p, _i64, _p]
+    L.alma_mc_after_rebuild.argtypes = [_p, _p, _p, _i32, _p]
     L.alma_move_scratch_init.argtypes = [_p, _i32, _p]
+    L.alma_move_counters.argtypes = [_p, _i32, _i32, _p, _p]
     L.alma_move_dE.argtypes = [_p, _p, _p, _p, C.c_int, _p, _p, _p, _p, C.c_int, _p, _p, _p]
-    for name, args in (("alma_mc_run", [_p, _p, _p, _p, C.c_int, _p, _p, _p, _i32, _p]),
-                       ("alma_forces", [_p, _p, _p, _p, C.c_int, _p, _p, _p])):
-        if hasattr(L, name):
-            getattr(L, name).argtypes = args
     if L.alma_abi_version() != 1:
         raise RuntimeError("protein_physics_b200: ABI version mismatch")
     _lib = L

@@ -274,25 +274,29 @@ class DeviceBatch:
         self.build_nl()
 
     # ---- energies -------------------------------------------------------------
-    def born_radii(self):
+    def born_radii(self, sys_mask=None):
         if not self.nl_ready:
             self.build_nl()
         b, nl = self.batch_s, self.nl_s
-        _lib.check(self.L.alma_born_radii(C.byref(b), C.byref(nl), C.byref(self.params), self.prec, self._sp()),
+        _lib.check(self.L.alma_born_radii(C.byref(b), C.byref(nl), C.byref(self.params), self.prec,
+                                          _ptr(sys_mask) if sys_mask is not None else None, self._sp()),
                    "alma_born_radii")
 
-    def energy_terms(self, recompute_born=True):
-        """[nsys, 5] float64 tensor {sasa, dihedral, disulfide, pairs, total}."""
+    def energy_terms(self, recompute_born=True, sys_mask=None, out=None):
+        """[nsys, 5] float64 tensor {sasa, dihedral, disulfide, pairs, total}
+        (rows of systems outside sys_mask are left as in `out`)."""
         if not self.nl_ready:
             self.build_nl()
         if recompute_born:
-            self.born_radii()
-        terms = torch.zeros((self.nsys, 5), dtype=torch.float64, device=_DEV)
-        atom_e = torch.zeros((max(self.natoms, 1), 2), dtype=torch.float64, device=_DEV)
+            self.born_radii(sys_mask)
+        terms = out if out is not None else torch.zeros((self.nsys, 5), dtype=torch.float64, device=_DEV)
+        if getattr(self, "_atom_e", None) is None:
+            self._atom_e = torch.zeros((max(self.natoms, 1), 2), dtype=torch.float64, device=_DEV)
         b, t, nl = self.batch_s, self.topo_s, self.nl_s
         _lib.check(self.L.alma_energy(C.byref(b), C.byref(t) if self.use_topo else None, C.byref(nl),
-                                      C.byref(self.params), self.prec, _ptr(atom_e), _ptr(terms), self._sp()),
-                   "alma_energy")
+                                      C.byref(self.params), self.prec,
+                                      _ptr(sys_mask) if sys_mask is not None else None, _ptr(self._atom_e),
+                                      _ptr(terms), self._sp()), "alma_energy")
         return terms
 
     # ---- one proposal per system ---------------------------------------------
@@ -319,6 +323,13 @@ class DeviceBatch:
                                        _ptr(self.scratch), _ptr(kind_t), _ptr(a_t), _ptr(d_t), int(bool(apply)),
                                        _ptr(dE), _ptr(dterms), self._sp()), "alma_move_dE")
         return dE, dterms
+
+    def move_counters(self):
+        """[nsys, 4] uint64: pair terms, hct terms, SASA visits, moved atoms."""
+        out = np.zeros((self.nsys, 4), np.uint64)
+        _lib.check(self.L.alma_move_counters(_ptr(self.scratch), self.natoms, self.nsys, out.ctypes.data,
+                                             self._sp()), "alma_move_counters")
+        return out
 
     # ---- host views -------------------------------------------------------------
     def coords(self, s=None):

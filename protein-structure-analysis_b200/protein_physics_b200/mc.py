@@ -1,0 +1,167 @@
+"""Host driver of the device Monte Carlo (alma_mc_run) and the reference's
+MC entry points on top of it.
+
+``MCRunner`` advances every system of a DeviceBatch by a number of
+proposals: it launches the persistent per-system kernel, and when a chain
+has drifted more than half the skin since its last list build it rebuilds
+that chain's neighbor list, Born radii and energy (the reference does the
+same at the start of the next step, physics_engine.cpp:2506-2510) and
+relaunches.  All other chains keep their lists.
+
+``generate_ensemble`` / ``run_landscape`` reproduce the reference
+semantics (physics_engine.cpp:2273-2543 and :2557-2951): value in, value
+out; each candidate chain or the landscape chain starts from the initial
+state; cur_max starts at max_angle; the landscape energies are full
+calculate_potential evaluations of each snapshot.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib
+from .device import DeviceBatch, _ptr, _t
+from .engine import particle_arrays, particles_from
+from .topology import flatten
+
+K_BOLTZMANN = 0.0019872  # kcal mol^-1 K^-1 (temperatures in K -> kcal/mol)
+
+
+def mc_config(seed, policy=0, tune_freq=200, max_angle_bounds=(0.004, 0.5), fixed_delta=0.0, moveset=None,
+              nsys=1, device_keep=None):
+    """AlmaMCConfig with the reference constants (physics_engine.cpp:2304-2307)."""
+    cfg = _lib.AlmaMCConfig()
+    cfg.seed = int(seed) & ((1 << 64) - 1)
+    cfg.policy = int(policy)
+    cfg.tune_freq = int(tune_freq)
+    cfg.target_lo, cfg.target_hi = 0.28, 0.52
+    cfg.scale_up, cfg.scale_down = 1.06, 0.94
+    cfg.angle_min, cfg.angle_max = max_angle_bounds
+    cfg.sidechain_mult = 2.5
+    cfg.crank_prob = 0.25
+    cfg.concerted_prob = 0.15
+    cfg.fixed_delta = float(fixed_delta)
+    cfg.moveset_off = cfg.moveset = None
+    if moveset is not None:
+        off = np.zeros(nsys + 1, np.int32)
+        off[1:] = np.cumsum([len(m) for m in moveset])
+        flat = np.concatenate([np.asarray(m, np.int32) for m in moveset]) if off[-1] else np.zeros(1, np.int32)
+        keep = (_t(off, torch.int32), _t(flat, torch.int32))
+        cfg.moveset_off, cfg.moveset = _ptr(keep[0]), _ptr(keep[1])
+        if device_keep is not None:
+            device_keep.extend(keep)
+    return cfg
+
+
+class MCRunner:
+    """Device MC over every system of `batch`.
+
+    temperatures: kcal/mol, one per system (scalar broadcast).  cur_max0:
+    initial max angle (the reference's max_angle)."""
+
+    def __init__(self, batch: DeviceBatch, temperatures, seed, policy=0, cur_max0=0.12, tune_freq=200,
+                 fixed_delta=0.0, moveset=None):
+        self.b = batch
+        self.L = batch.L
+        self._keep = []
+        self.cfg = mc_config(seed, policy, tune_freq, fixed_delta=fixed_delta, moveset=moveset, nsys=batch.nsys,
+                             device_keep=self._keep)
+        T = np.broadcast_to(np.asarray(temperatures, np.float64), (batch.nsys,)).copy()
+        if np.any(T <= 0):
+            raise ValueError("temperature must be positive")
+        st = np.zeros(batch.nsys, dtype=_lib.STATE_DTYPE)
+        st["cur_max"] = cur_max0
+        st["temperature"] = T
+        self.states = torch.from_numpy(st.view(np.uint8).copy()).to("cuda")
+        self.terms = torch.zeros((batch.nsys, 5), dtype=torch.float64, device="cuda")
+        self.rebuilds = 0
+        batch.build_nl()
+        self.reset_energy()
+
+    def reset_energy(self, sys_mask=None):
+        """Full Born radii + energy of the (masked) systems -> state.energy."""
+        self.b.energy_terms(recompute_born=True, sys_mask=sys_mask, out=self.terms)
+        _lib.check(self.L.alma_mc_after_rebuild(_ptr(self.states), _ptr(self.terms),
+                                                _ptr(sys_mask) if sys_mask is not None else None,
+                                                self.b.nsys, self.b._sp()), "alma_mc_after_rebuild")
+
+    def state(self):
+        return self.states.cpu().numpy().view(_lib.STATE_DTYPE).copy()
+
+    def launch(self, step_limit):
+        b = self.b
+        _lib.check(self.L.alma_mc_run(C.byref(b.batch_s), C.byref(b.topo_s), C.byref(b.nl_s), C.byref(b.params),
+                                      b.prec, _ptr(b.scratch), C.byref(self.cfg), _ptr(self.states),
+                                      int(step_limit), b._sp()), "alma_mc_run")
+
+    def run(self, nsteps):
+        """Advances every system by nsteps proposals (host loop over rebuilds)."""
+        target = int(self.state()["step"].max()) + int(nsteps) if nsteps > 0 else 0
+        return self.run_to(target)
+
+    def run_to(self, step_limit):
+        while True:
+            self.launch(step_limit)
+            st = self.state()
+            need = st["need_rebuild"] != 0
+            if need.any():
+                mask = torch.from_numpy(need.astype(np.uint8)).to("cuda")
+                self.b.build_nl(sys_mask=mask)
+                self.reset_energy(sys_mask=mask)
+                self.rebuilds += int(need.sum())
+                continue
+            if np.all(st["step"] >= step_limit):
+                return st
+
+
+def _check_inputs(state, topology):
+    if len(state) == 0:
+        raise ValueError("initial_state empty")
+    if topology is None:
+        raise ValueError("topology is required")
+    flat = flatten(topology)
+    if flat.n != len(state):
+        raise ValueError(f"topology has {flat.n} atoms, initial_state {len(state)}")
+    if flat.nrb == 0:
+        raise ValueError("topology has no rotatable bonds")
+    return flat
+
+
+def generate_ensemble(engine, initial_state, topology, n_candidates, steps_per_cand, temperature=0.6,
+                      max_angle=0.12):
+    """n_candidates independent chains of steps_per_cand proposals from the
+    initial state, run as one batch (one CTA per chain)."""
+    flat = _check_inputs(initial_state, topology)
+    if n_candidates <= 0 or steps_per_cand <= 0:
+        raise ValueError("ncand/steps must be positive")
+    xyz, q, r, e = particle_arrays(initial_state)
+    batch = DeviceBatch([(xyz, q, r, e, flat)] * int(n_candidates), precision=engine.precision)
+    runner = MCRunner(batch, temperature, engine._next_seed(), policy=0, cur_max0=max_angle)
+    runner.run(steps_per_cand)
+    X = batch.coords()
+    return [particles_from(X[batch.atom_off_h[c]:batch.atom_off_h[c + 1]], initial_state)
+            for c in range(int(n_candidates))]
+
+
+def run_landscape(engine, initial_state, topology, n_snapshots, steps_per_snapshot, temperature=0.6,
+                  max_angle=0.12):
+    """One landscape chain (policy 1: concerted sidechain pairs, crankshaft,
+    torsion); a snapshot and its full energy every steps_per_snapshot
+    proposals.  Returns (snapshots, energies, final cur_max)."""
+    flat = _check_inputs(initial_state, topology)
+    if n_snapshots <= 0 or steps_per_snapshot <= 0:
+        raise ValueError("n_snapshots/steps_per_snapshot must be positive")
+    xyz, q, r, e = particle_arrays(initial_state)
+    batch = DeviceBatch([(xyz, q, r, e, flat)], precision=engine.precision)
+    runner = MCRunner(batch, temperature, engine._next_seed(), policy=1, cur_max0=max_angle)
+    snaps, energies = [], []
+    for _ in range(int(n_snapshots)):
+        runner.run(steps_per_snapshot)
+        X = batch.coords(0)
+        snaps.append(particles_from(X, initial_state))
+        shot = DeviceBatch([(X, q, r, e, flat)], precision=engine.precision)
+        energies.append(float(shot.energy_terms()[0, 4].item()))
+    cur_max = float(runner.state()["cur_max"][0])
+    return snaps, energies, cur_max

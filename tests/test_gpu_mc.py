@@ -1,0 +1,109 @@
+"""Device Monte Carlo vs the oracle's MC driver, draw for draw.
+
+Both sides take the same Philox draws (seed, system, step), so with FP64
+pair arithmetic on the device the two trajectories must coincide: the same
+accepted / rebuilt counts, the same adaptive cur_max and final coordinates
+to 1e-9 Å.  The mixed-precision engine may flip a Metropolis decision only
+when u is within its ~1e-5 kcal/mol ΔE error of the threshold; over the
+short runs here it does not.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def _setup(name):
+    from conftest import Golden
+    from protein_physics_b200.topology import flatten
+    g = Golden(name)
+    return g, flatten(g.topology())
+
+
+def _gpu_run(g, F, nsys, seed, steps, precision="fp64", policy=0, fixed_delta=0.0, moveset=None, T=0.6):
+    from protein_physics_b200.device import DeviceBatch
+    from protein_physics_b200.mc import MCRunner
+    b = DeviceBatch([(g["xyz"], g["q"], g["r"], g["eps"], F)] * nsys, precision=precision)
+    R = MCRunner(b, T, seed, policy=policy, fixed_delta=fixed_delta,
+                 moveset=[moveset] * nsys if moveset is not None else None)
+    st = R.run_to(steps)
+    return b, st
+
+
+def _oracle_run(g, F, seed, steps, sys_index=0, policy=0, fixed_delta=0.0, moveset=None, T=0.6):
+    from oracle import Oracle, oracle_mc
+    return oracle_mc(Oracle(), F, g["xyz"], g["q"], g["r"], g["eps"], seed, steps, temperature=T, policy=policy,
+                     fixed_delta=fixed_delta, moveset=moveset, sys_index=sys_index)
+
+
+@pytest.mark.parametrize("name,policy,steps", [("insulin", 0, 300), ("xq8", 0, 150), ("xq8", 1, 150)])
+def test_fp64_trajectory_matches_oracle(name, policy, steps):
+    g, F = _setup(name)
+    b, st = _gpu_run(g, F, 1, 11, steps, policy=policy)
+    x_o, st_o, _ = _oracle_run(g, F, 11, steps, policy=policy)
+    assert st["n_accepted"][0] == st_o["n_accepted"]
+    assert st["n_proposed"][0] == st_o["n_proposed"]
+    assert st["n_rebuild"][0] == st_o["n_rebuild"]
+    assert st["cur_max"][0] == pytest.approx(st_o["cur_max"], rel=1e-15)
+    np.testing.assert_allclose(b.coords(0), x_o, rtol=0, atol=1e-9)
+    assert st["energy"][0] == pytest.approx(st_o["energy"], rel=1e-9, abs=1e-6)
+
+
+def test_rebuild_path_matches_oracle():
+    """Large fixed angles force drift > skin/2 and neighbor-list rebuilds."""
+    g, F = _setup("insulin")
+    b, st = _gpu_run(g, F, 1, 5, 120, fixed_delta=0.6, T=50.0)
+    x_o, st_o, _ = _oracle_run(g, F, 5, 120, fixed_delta=0.6, T=50.0)
+    assert st_o["n_rebuild"] > 0
+    assert st["n_rebuild"][0] == st_o["n_rebuild"]
+    assert st["n_accepted"][0] == st_o["n_accepted"]
+    np.testing.assert_allclose(b.coords(0), x_o, rtol=0, atol=1e-8)
+
+
+def test_batched_chains_are_independent_streams():
+    g, F = _setup("insulin")
+    b, st = _gpu_run(g, F, 3, 21, 80)
+    for s in range(3):
+        x_o, st_o, _ = _oracle_run(g, F, 21, 80, sys_index=s)
+        assert st["n_accepted"][s] == st_o["n_accepted"]
+        np.testing.assert_allclose(b.coords(s), x_o, rtol=0, atol=1e-9)
+
+
+def test_moveset_restriction():
+    g, F = _setup("xq8")
+    small = [k for k in range(F.nrb) if F.side_count[k] <= 0.25 * F.n]
+    b, st = _gpu_run(g, F, 1, 3, 100, policy=2, moveset=small)
+    x_o, st_o, _ = _oracle_run(g, F, 3, 100, policy=2, moveset=small)
+    assert st["n_accepted"][0] == st_o["n_accepted"]
+    np.testing.assert_allclose(b.coords(0), x_o, rtol=0, atol=1e-9)
+
+
+def test_mixed_precision_chain_is_sane():
+    g, F = _setup("insulin")
+    b, st = _gpu_run(g, F, 2, 9, 200, precision="mixed")
+    _, st_o, _ = _oracle_run(g, F, 9, 200)
+    assert abs(int(st["n_accepted"][0]) - st_o["n_accepted"]) <= 2
+    assert np.all(np.isfinite(st["energy"]))
+
+
+def test_dropin_mc_entry_points():
+    from protein_physics_b200 import Particle, PhysicsEngine
+    g, F = _setup("insulin")
+    T = g.topology()
+    P = [Particle(*x, q, r, e) for x, q, r, e in zip(g["xyz"], g["q"], g["r"], g["eps"])]
+    eng = PhysicsEngine(seed=1)
+    ens = eng.generate_ensemble(P, T, 3, 50)
+    assert len(ens) == 3 and all(len(m) == len(P) for m in ens)
+    snaps, energies = eng.run_landscape_trajectory(P, T, 2, 20)
+    assert len(snaps) == 2 and len(energies) == 2 and all(np.isfinite(energies))
+    snaps, energies, cur_max = eng.run_landscape_segment(P, T, 1, 10, 0.6, 0.1)
+    assert 0.004 <= cur_max <= 0.5
+    best = eng.lowest_energy_structure(ens)
+    assert len(best) == len(P)
+    with pytest.raises(ValueError):
+        eng.generate_ensemble([], T, 1, 1)
+    with pytest.raises(ValueError):
+        eng.generate_ensemble(P, T, 0, 1)
+    with pytest.raises(ValueError):
+        eng.run_landscape_trajectory(P, T, 1, 0)
