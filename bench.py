@@ -84,6 +84,12 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
+def _coil_chain(n_res, seed):
+    sys.path.insert(0, os.path.join(ROOT, "protein-structure-analysis_b200"))
+    from protein_physics_b200 import synth
+    return synth.coil_chain(n_res, seed)
+
+
 def make_workload(kind, rank):
     from protein_physics_b200 import synth
     from protein_physics_b200.topology import BondTopology, flatten
@@ -91,10 +97,14 @@ def make_workload(kind, rank):
         chains = [synth.compact_chain(300, seed=2 + 1000 * rank)]
         temps = [300.0 * KB]
     else:
+        import multiprocessing as mp
         import numpy as np
         rng = np.random.default_rng(3 + 1000 * rank)
         sizes = rng.integers(50, 601, size=256)
-        chains = [synth.coil_chain(int(n), seed=int(1000 * rank + k)) for k, n in enumerate(sizes)]
+        jobs = [(int(n), int(1000 * rank + k)) for k, n in enumerate(sizes)]
+        # chain generation is host Python: spread it over the host cores
+        with mp.get_context("spawn").Pool(min(32, os.cpu_count() or 1)) as pool:
+            chains = pool.starmap(_coil_chain, jobs, chunksize=1)
         temps = list(280.0 * (400.0 / 280.0) ** (np.arange(256) / 255.0) * KB)
     systems, movesets, topos = [], [], []
     for ch in chains:

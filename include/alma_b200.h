@@ -224,6 +224,8 @@ typedef struct {
     double fixed_delta;       /* > 0: angles ~ U(-fixed_delta, fixed_delta)  */
     const int32_t *moveset_off;   /* optional [nsys+1] device: torsion moves */
     const int32_t *moveset;       /* drawn from these local rot-bond indices */
+    int32_t threads_per_system;   /* CTA size 256 or 512; 0 = by batch size  */
+    int32_t pad;
 } AlmaMCConfig;
 
 /* Per-system chain state, device memory, one per system (72 bytes). */

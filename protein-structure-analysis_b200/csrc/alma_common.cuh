@@ -113,14 +113,17 @@ __device__ __forceinline__ float m_log1p(float x) { return log1pf(x); }
 __device__ __forceinline__ double m_log1p(double x) { return log1p(x); }
 
 // LJ 12-6 + capped hard core of one pair (r2 in FP64).  Inside sigma the
-// terms grow steeply and are evaluated in FP64; outside, in precision R.
+// terms grow steeply and are evaluated in FP64 with FP64 sigma and
+// epsilon (sig64 = R*_i + R*_j, eps64 = eps_i eps_j); outside, in
+// precision R.
 template <typename R>
-__device__ __forceinline__ double lj_hard(const DevParams &P, double r2, R sig, R eps_prod) {
-    const double sig2 = (double)sig * (double)sig;
+__device__ __forceinline__ double lj_hard(const DevParams &P, double r2, R sig, R eps_prod, double sig64,
+                                          double eps64) {
+    const double sig2 = sig64 * sig64;
     if (r2 < sig2) {
         const double s2 = sig2 / r2, s6 = s2 * s2 * s2;
-        double E = 4.0 * sqrt((double)eps_prod) * (s6 * s6 - s6);
-        const double rc2 = sig2 * P.hard_frac * P.hard_frac;
+        double E = 4.0 * sqrt(eps64) * (s6 * s6 - s6);
+        const double rc = sig64 * P.hard_frac, rc2 = rc * rc;
         if (r2 < rc2) {
             const double t2 = rc2 / r2, t6 = t2 * t2 * t2, x = t6 * t6 - 1.0;
             E += fmin(P.hard_scale * x * x, P.hard_cap);
@@ -141,7 +144,7 @@ __device__ __forceinline__ double lj_hard(const DevParams &P, double r2, R sig, 
 // LJ and the hard core are differenced directly (FP64 inside sigma).
 template <typename R>
 __device__ __forceinline__ double pair_delta(const DevParams &P, double r2o, double r2n, R qp, R sig, R eps_prod,
-                                             R aao, R aan) {
+                                             R aao, R aan, double sig64, double eps64) {
     const double d2 = r2n - r2o;
     const R ro2 = (R)r2o, rn2 = (R)r2n;
     const R ro = m_sqrt(ro2), rn = m_sqrt(rn2);
@@ -153,7 +156,8 @@ __device__ __forceinline__ double pair_delta(const DevParams &P, double r2o, dou
     const R fo = m_sqrt(ro2 + xo), fn = m_sqrt(rn2 + xn);
     const R num = (R)(-d2) + (xo - xn);
     const R dgb = (R)P.gb_coef * qp * num / (fo * fn * (fo + fn));
-    return (double)ddh + (double)dgb + (lj_hard<R>(P, r2n, sig, eps_prod) - lj_hard<R>(P, r2o, sig, eps_prod));
+    return (double)ddh + (double)dgb +
+           (lj_hard<R>(P, r2n, sig, eps_prod, sig64, eps64) - lj_hard<R>(P, r2o, sig, eps_prod, sig64, eps64));
 }
 
 // HCT descreening integral of atom j (radius rj) on atom i (radius ri).

@@ -42,9 +42,9 @@ __device__ __forceinline__ int pick(double u, int n) {
     return k < n ? k : n - 1;
 }
 
-template <typename R>
-__global__ void __launch_bounds__(MOVE_THREADS) mc_kernel(MoveCtx C, MCConfigDev cfg, AlmaChainState *__restrict__ states,
-                                                          int64_t step_limit) {
+template <typename R, int NT>
+__global__ void __launch_bounds__(NT, 512 / NT) mc_kernel(MoveCtx C, MCConfigDev cfg,
+                                                          AlmaChainState *__restrict__ states, int64_t step_limit) {
     __shared__ MoveDesc M;
     __shared__ double sm[32];
     __shared__ int naff;
@@ -221,10 +221,23 @@ extern "C" int alma_mc_run(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *
     d.moveset_off = cfg->moveset_off;
     d.moveset = cfg->moveset;
     cudaStream_t st = (cudaStream_t)stream;
-    if (prec == ALMA_PREC_FP64)
-        mc_kernel<double><<<b->nsys, MOVE_THREADS, 0, st>>>(C, d, states, step_limit);
-    else
-        mc_kernel<float><<<b->nsys, MOVE_THREADS, 0, st>>>(C, d, states, step_limit);
+    // Threads per system: 512 when the batch fits one CTA per SM, else 256
+    // (two CTAs per SM), so every chain of a persistent launch is resident.
+    int nt = cfg->threads_per_system;
+    if (nt == 0) {
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        nt = b->nsys <= sms ? 512 : 256;
+    }
+    if (nt != 256 && nt != 512) return alma_set_error(ALMA_EINVAL, "alma_mc_run: threads_per_system must be 0, 256 or 512");
+    if (prec == ALMA_PREC_FP64) {
+        if (nt == 512) mc_kernel<double, 512><<<b->nsys, 512, 0, st>>>(C, d, states, step_limit);
+        else mc_kernel<double, 256><<<b->nsys, 256, 0, st>>>(C, d, states, step_limit);
+    } else {
+        if (nt == 512) mc_kernel<float, 512><<<b->nsys, 512, 0, st>>>(C, d, states, step_limit);
+        else mc_kernel<float, 256><<<b->nsys, 256, 0, st>>>(C, d, states, step_limit);
+    }
     ALMA_LAUNCH_CHECK("alma_mc_run");
     return ALMA_OK;
 }

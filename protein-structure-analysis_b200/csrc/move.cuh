@@ -286,9 +286,20 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
             w.born_new[m] = 1.0 / fmax(1.0 / b.prm64[4 * (size_t)m + 1] - 0.5 * sum, 2.0);
             atomicAdd(&w.ctr[4 * s + 1], (unsigned long long)C.nl.half_len[m]);
         }
+        // SASA reach: atoms i < j interact when j is in i's half row and
+        // r < R*_i + R*_j + 2 probe.  A pair whose distance changes (groups
+        // differ) and is within reach before or after the move changes the
+        // SASA of its lower atom only; mark that atom.
+        const double4 pmo_s = ld_xyz(b.xyz, m);
+        const double rsm = b.prm64[4 * (size_t)m + 1] + C.P.probe_r;
+        const int gm_s = w.group[m];
         for (int64_t e = C.nl.full_ptr[m] + lane; e < C.nl.full_ptr[m] + C.nl.full_len[m]; e += 32) {
             const int j = (int)(C.nl.full_cols[e] & ALMA_IDX_MASK);
-            if (j < m && w.group[j] == 0) w.mark[j] = 1;
+            const int gj = w.group[j];
+            if (gj == gm_s) continue;
+            const double dc = rsm + b.prm64[4 * (size_t)j + 1] + C.P.probe_r, dc2 = dc * dc;
+            const double4 pjo = ld_xyz(b.xyz, j), pjn = gj ? ld_xyz(w.xyz_new, j) : pjo;
+            if (d2_of(pmo_s, pjo) < dc2 || d2_of(pm, pjn) < dc2) w.mark[j < m ? j : m] = 1;
         }
     }
     __syncthreads();
@@ -301,6 +312,7 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
         R qm, rm, em;
         prm_of<R>(b.prm, b.prm64, m, qm, rm, em);
         const R amo = (R)b.born[m], amn = (R)w.born_new[m];
+        const double rm64 = b.prm64[4 * (size_t)m + 1], em64 = b.prm64[4 * (size_t)m + 2];
         double acc = 0.0;
         int npair = 0;
         for (int64_t e = C.nl.full_ptr[m] + lane; e < C.nl.full_ptr[m] + C.nl.full_len[m]; e += 32) {
@@ -321,7 +333,14 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
             const bool ino = r2o <= C.P.pair_cut2, inn = r2n <= C.P.pair_cut2;
             npair += (int)ino + (int)inn;
             if (ino && inn) {
-                acc += pair_delta<R>(C.P, r2o, r2n, qp, sig, ep, amo * ajo, amn * ajn);
+                // FP64 sigma/epsilon only for contacts inside sigma (steep LJ)
+                double sig64 = (double)sig, eps64 = (double)ep;
+                if (fmin(r2o, r2n) < 1.0001 * sig64 * sig64) {
+                    const double4 pj64 = *reinterpret_cast<const double4 *>(b.prm64 + 4 * (size_t)j);
+                    sig64 = rm64 + pj64.y;
+                    eps64 = em64 * pj64.z;
+                }
+                acc += pair_delta<R>(C.P, r2o, r2n, qp, sig, ep, amo * ajo, amn * ajn, sig64, eps64);
             } else if (ino) {
                 acc -= (double)pair_energy<R>(C.P, (R)r2o, qp, sig, ep, amo, ajo);
             } else if (inn) {
@@ -335,8 +354,8 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
             atomicAdd(&w.ctr[4 * s + 0], (unsigned long long)npair);
         }
     }
-    // Affected fixed atoms -> compaction list (order irrelevant: results go
-    // to per-atom slots and are summed in atom order).
+    // Atoms whose SASA can change -> compaction list (order irrelevant:
+    // results go to per-atom slots and are summed in atom order).
     for (int i = a0 + tid; i < a1; i += nthr) {
         if (w.mark[i]) {
             const int slot = atomicAdd(s_naff, 1);
@@ -344,18 +363,13 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
         }
     }
     __syncthreads();
-    // P5: SASA of every affected atom (members + marked), old and new, in
-    // row order.
-    const int64_t naff = nm + *s_naff;
+    // P5: SASA of every affected atom, old and new, in row order; every
+    // other atom's SASA is unchanged bit for bit (its half row holds no pair
+    // whose distance changed within reach).
+    const int64_t naff = *s_naff;
     const double pi4 = 4.0 * 3.14159265358979323846, pi2 = 2.0 * 3.14159265358979323846;
     for (int64_t k = wid; k < naff; k += nw) {
-        int i;
-        if (k < nm) {
-            int g;
-            i = member(M, t.side_idx, k, g);
-        } else {
-            i = w.affected[a0 + (k - nm)];
-        }
+        const int i = w.affected[a0 + k];
         const bool moved = w.group[i] != 0;
         const double4 pio = ld_xyz(b.xyz, i), pin = moved ? ld_xyz(w.xyz_new, i) : pio;
         const double rsi = b.prm64[4 * (size_t)i + 1] + C.P.probe_r;

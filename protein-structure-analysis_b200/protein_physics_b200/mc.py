@@ -44,6 +44,7 @@ def mc_config(seed, policy=0, tune_freq=200, max_angle_bounds=(0.004, 0.5), fixe
     cfg.concerted_prob = 0.15
     cfg.fixed_delta = float(fixed_delta)
     cfg.moveset_off = cfg.moveset = None
+    cfg.threads_per_system = 0
     if moveset is not None:
         off = np.zeros(nsys + 1, np.int32)
         off[1:] = np.cumsum([len(m) for m in moveset])
