@@ -225,7 +225,8 @@ typedef struct {
     const int32_t *moveset_off;   /* optional [nsys+1] device: torsion moves */
     const int32_t *moveset;       /* drawn from these local rot-bond indices */
     int32_t threads_per_system;   /* CTA size 256 or 512; 0 = by batch size  */
-    int32_t pad;
+    int32_t cluster_size;         /* CTAs per system (1,2,4,8,16; 0 = 1): a  */
+                                  /* thread-block cluster shares a proposal  */
 } AlmaMCConfig;
 
 /* Per-system chain state, device memory, one per system (72 bytes). */

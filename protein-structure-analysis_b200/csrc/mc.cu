@@ -42,24 +42,28 @@ __device__ __forceinline__ int pick(double u, int n) {
     return k < n ? k : n - 1;
 }
 
-template <typename R, int NT>
+// One system per CTA (CL = 1) or per cluster of CL CTAs.  Every CTA of a
+// cluster keeps its own copy of the chain state and makes the same draws
+// and decisions (the ΔE totals are bit-identical in every CTA); rank 0
+// writes the state back.
+template <typename R, int NT, int CL>
 __global__ void __launch_bounds__(NT, 512 / NT) mc_kernel(MoveCtx C, MCConfigDev cfg,
                                                           AlmaChainState *__restrict__ states, int64_t step_limit) {
     __shared__ MoveDesc M;
     __shared__ double sm[32];
-    __shared__ int naff;
+    __shared__ double part[4];
+    __shared__ int flag;
     __shared__ AlmaChainState S;
     __shared__ double u[6];
     __shared__ int did_move, accept;
-    const int s = blockIdx.x;
+    const Team<CL> T;
+    const int s = blockIdx.x / CL;
     if (threadIdx.x == 0) S = states[s];
     __syncthreads();
-    const int a0 = C.b.atom_off[s];
     const int nrb = C.t.rb_off[s + 1] - C.t.rb_off[s];
     const int ncp = C.t.cp_off[s + 1] - C.t.cp_off[s];
     const int ncsp = C.t.csp_off[s + 1] - C.t.csp_off[s];
     const int nset = cfg.moveset_off ? cfg.moveset_off[s + 1] - cfg.moveset_off[s] : nrb;
-    (void)a0;
     while (S.step < step_limit && !S.need_rebuild) {
         if (threadIdx.x == 0) {
             const uint64_t st = (uint64_t)S.step;
@@ -121,39 +125,14 @@ __global__ void __launch_bounds__(NT, 512 / NT) mc_kernel(MoveCtx C, MCConfigDev
             __syncthreads();
             continue;
         }
-        const MoveResult r = move_eval<R>(C, M, s, sm, &naff);
-        if (threadIdx.x == 0) {
-            const double T = S.temperature;
-            accept = (r.dE < 0.0) || (u[3] < exp(-r.dE / T));
-        }
+        // every CTA must have read the current coordinates before any
+        // commits of this proposal: move_eval starts with a team barrier
+        // only after P1, which writes scratch, not coordinates.
+        const MoveResult r = move_eval<R, CL>(C, M, s, sm, part, T);
+        if (threadIdx.x == 0) accept = (r.dE < 0.0) || (u[3] < exp(-r.dE / S.temperature));
         __syncthreads();
         const int acc = accept;
-        // commit / discard, then the drift test on the committed atoms
-        int drift = 0;
-        {
-            const MoveScratch &w = C.w;
-            const int64_t nm = n_members(M);
-            for (int64_t k = threadIdx.x; k < nm; k += blockDim.x) {
-                int g;
-                const int m = member(M, C.t.side_idx, k, g);
-                if (acc) {
-                    const double4 p = ld_xyz(w.xyz_new, m);
-                    *reinterpret_cast<double4 *>(C.b.xyz + 4 * (size_t)m) = p;
-                    C.b.born[m] = w.born_new[m];
-                    if (d2_of(p, ld_xyz(C.nl.ref_xyz, m)) > C.P.half_skin2) drift = 1;
-                }
-                w.group[m] = 0;
-                w.dE_atom[2 * (size_t)m] = 0.0;
-                w.dE_atom[2 * (size_t)m + 1] = 0.0;
-            }
-            const int na = naff;
-            for (int k = threadIdx.x; k < na; k += blockDim.x) {
-                const int i = w.affected[C.b.atom_off[s] + k];
-                w.mark[i] = 0;
-                w.dE_atom[2 * (size_t)i + 1] = 0.0;
-            }
-        }
-        drift = __syncthreads_or(drift);
+        const int drift = move_finish<CL>(C, M, s, acc, &flag, T);
         if (threadIdx.x == 0) {
             S.n_proposed++;
             if (acc) {
@@ -171,9 +150,43 @@ __global__ void __launch_bounds__(NT, 512 / NT) mc_kernel(MoveCtx C, MCConfigDev
             }
             S.step++;
         }
-        __syncthreads();
+        // commits of this proposal visible to every CTA before the next
+        // proposal reads coordinates
+        T.sync();
     }
-    if (threadIdx.x == 0) states[s] = S;
+    if (threadIdx.x == 0 && T.rank == 0) states[s] = S;
+}
+
+template <typename R, int NT, int CL>
+static cudaError_t launch_mc(const MoveCtx &C, const MCConfigDev &d, AlmaChainState *states, int64_t step_limit,
+                             int nsys, cudaStream_t st) {
+    if constexpr (CL == 1) {
+        mc_kernel<R, NT, 1><<<nsys, NT, 0, st>>>(C, d, states, step_limit);
+        return cudaGetLastError();
+    } else {
+        auto kfn = mc_kernel<R, NT, CL>;
+        if (CL > 8) {
+            cudaError_t e = cudaFuncSetAttribute(kfn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+            if (e != cudaSuccess) return e;
+        }
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)(nsys * CL), 1, 1);
+        cfg.blockDim = dim3(NT, 1, 1);
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = CL;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int max_clusters = 0;
+        cudaError_t e = cudaOccupancyMaxActiveClusters(&max_clusters, kfn, &cfg);
+        if (e != cudaSuccess) return e;
+        if (max_clusters < 1) return cudaErrorInvalidConfiguration;  // cluster does not fit a GPC
+        return cudaLaunchKernelEx(&cfg, kfn, C, d, states, step_limit);
+    }
 }
 
 // After a rebuild of the flagged systems: energy <- fresh total, flag
@@ -223,6 +236,7 @@ extern "C" int alma_mc_run(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *
     cudaStream_t st = (cudaStream_t)stream;
     // Threads per system: 512 when the batch fits one CTA per SM, else 256
     // (two CTAs per SM), so every chain of a persistent launch is resident.
+    // cluster_size CTAs cooperate on each system (1, 2, 4, 8 or 16).
     int nt = cfg->threads_per_system;
     if (nt == 0) {
         int dev = 0, sms = 148;
@@ -230,14 +244,26 @@ extern "C" int alma_mc_run(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         nt = b->nsys <= sms ? 512 : 256;
     }
+    const int cl = cfg->cluster_size <= 0 ? 1 : cfg->cluster_size;
     if (nt != 256 && nt != 512) return alma_set_error(ALMA_EINVAL, "alma_mc_run: threads_per_system must be 0, 256 or 512");
-    if (prec == ALMA_PREC_FP64) {
-        if (nt == 512) mc_kernel<double, 512><<<b->nsys, 512, 0, st>>>(C, d, states, step_limit);
-        else mc_kernel<double, 256><<<b->nsys, 256, 0, st>>>(C, d, states, step_limit);
-    } else {
-        if (nt == 512) mc_kernel<float, 512><<<b->nsys, 512, 0, st>>>(C, d, states, step_limit);
-        else mc_kernel<float, 256><<<b->nsys, 256, 0, st>>>(C, d, states, step_limit);
+    if (cl != 1 && cl != 2 && cl != 4 && cl != 8 && cl != 16)
+        return alma_set_error(ALMA_EINVAL, "alma_mc_run: cluster_size must be 1, 2, 4, 8 or 16");
+    cudaError_t e = cudaSuccess;
+#define ALMA_MC_CASE(R, NT)                                                              \
+    switch (cl) {                                                                        \
+        case 1: e = launch_mc<R, NT, 1>(C, d, states, step_limit, b->nsys, st); break;   \
+        case 2: e = launch_mc<R, NT, 2>(C, d, states, step_limit, b->nsys, st); break;   \
+        case 4: e = launch_mc<R, NT, 4>(C, d, states, step_limit, b->nsys, st); break;   \
+        case 8: e = launch_mc<R, NT, 8>(C, d, states, step_limit, b->nsys, st); break;   \
+        default: e = launch_mc<R, NT, 16>(C, d, states, step_limit, b->nsys, st); break; \
     }
+    if (prec == ALMA_PREC_FP64) {
+        if (nt == 512) { ALMA_MC_CASE(double, 512) } else { ALMA_MC_CASE(double, 256) }
+    } else {
+        if (nt == 512) { ALMA_MC_CASE(float, 512) } else { ALMA_MC_CASE(float, 256) }
+    }
+#undef ALMA_MC_CASE
+    if (e != cudaSuccess) return alma_cuda_error(e, "alma_mc_run launch");
     ALMA_LAUNCH_CHECK("alma_mc_run");
     return ALMA_OK;
 }

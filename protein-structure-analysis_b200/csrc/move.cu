@@ -14,12 +14,14 @@ static size_t carve_scratch(MoveScratch *w, char *base, int32_t natoms) {
     };
     MoveScratch t;
     t.group = (int8_t *)take((size_t)natoms);
+    t.body = (int8_t *)take((size_t)natoms);
     t.mark = (uint8_t *)take((size_t)natoms);
     t.xyz_new = (double *)take(sizeof(double) * 4 * (size_t)natoms);
     t.born_new = (double *)take(sizeof(double) * (size_t)natoms);
     t.dE_atom = (double *)take(sizeof(double) * 2 * (size_t)natoms);
     t.affected = (int32_t *)take(sizeof(int32_t) * (size_t)natoms);
     t.ctr = (unsigned long long *)take(sizeof(unsigned long long) * 4 * (size_t)(natoms + 1));
+    t.naff = (int *)take(sizeof(int) * (size_t)(natoms + 1));
     if (w) *w = t;
     return off;
 }
@@ -31,7 +33,9 @@ __global__ void __launch_bounds__(MOVE_THREADS) move_dE_kernel(MoveCtx C, const 
                                                                double *__restrict__ dE, double *__restrict__ dterms) {
     __shared__ MoveDesc M;
     __shared__ double sm[32];
-    __shared__ int naff;
+    __shared__ double part[4];
+    __shared__ int flag;
+    const Team<1> T;
     const int s = blockIdx.x;
     const int k = kind[s];
     if (threadIdx.x == 0) {
@@ -47,7 +51,7 @@ __global__ void __launch_bounds__(MOVE_THREADS) move_dE_kernel(MoveCtx C, const 
         }
         return;
     }
-    const MoveResult r = move_eval<R>(C, M, s, sm, &naff);
+    const MoveResult r = move_eval<R, 1>(C, M, s, sm, part, T);
     if (threadIdx.x == 0) {
         dE[s] = r.dE;
         dterms[4 * (size_t)s + 0] = r.dcross;
@@ -55,7 +59,7 @@ __global__ void __launch_bounds__(MOVE_THREADS) move_dE_kernel(MoveCtx C, const 
         dterms[4 * (size_t)s + 2] = r.ddih;
         dterms[4 * (size_t)s + 3] = r.dss;
     }
-    move_finish(C, M, s, &naff, apply);
+    move_finish<1>(C, M, s, apply, &flag, T);
 }
 
 }  // namespace alma

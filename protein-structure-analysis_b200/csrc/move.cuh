@@ -21,9 +21,67 @@
 // Per-atom contributions land in dE_atom[2*i] (cross) / dE_atom[2*i+1]
 // (SASA) and are summed in atom order, so the result is deterministic.
 #pragma once
+#include <cooperative_groups.h>
+
 #include "alma_common.cuh"
 
 namespace alma {
+
+namespace cg = cooperative_groups;
+
+// The threads that evaluate one system's proposal: one CTA (CL = 1) or a
+// thread-block cluster of CL CTAs on CL SMs.  Work is strided over all the
+// team's threads / warps; phase barriers are CTA or cluster barriers (the
+// latter order global-memory writes across the cluster's CTAs).
+template <int CL>
+struct Team {
+    int rank;
+    __device__ Team() { rank = CL > 1 ? (int)cg::this_cluster().block_rank() : 0; }
+    __device__ __forceinline__ int gtid() const { return rank * (int)blockDim.x + (int)threadIdx.x; }
+    __device__ __forceinline__ int gthreads() const { return CL * (int)blockDim.x; }
+    __device__ __forceinline__ int gwarp() const { return rank * ((int)blockDim.x >> 5) + ((int)threadIdx.x >> 5); }
+    __device__ __forceinline__ int gwarps() const { return CL * ((int)blockDim.x >> 5); }
+    __device__ __forceinline__ void sync() const {
+        if constexpr (CL > 1) cg::this_cluster().sync();
+        else __syncthreads();
+    }
+};
+
+// Team-wide sums of K doubles; every thread of every CTA gets the same
+// totals (CTA partials combined in rank order through distributed shared
+// memory).  smem: >= 32 doubles; part: __shared__ double[K] per CTA.
+template <int CL, int K>
+__device__ __forceinline__ void team_sum(const Team<CL> &T, double (&v)[K], double *smem, double *part) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = block_sum(v[k], smem);
+    if constexpr (CL > 1) {
+        if (threadIdx.x == 0)
+            for (int k = 0; k < K; ++k) part[k] = v[k];
+        T.sync();
+        cg::cluster_group cl = cg::this_cluster();
+        for (int k = 0; k < K; ++k) v[k] = 0.0;
+        for (int r = 0; r < CL; ++r) {
+            const double *pr = cl.map_shared_rank(part, r);
+            for (int k = 0; k < K; ++k) v[k] += pr[k];
+        }
+        T.sync();
+    }
+}
+
+// Team-wide OR of one flag per thread.
+template <int CL>
+__device__ __forceinline__ int team_or(const Team<CL> &T, int f, int *part) {
+    f = __syncthreads_or(f);
+    if constexpr (CL > 1) {
+        if (threadIdx.x == 0) *part = f;
+        T.sync();
+        cg::cluster_group cl = cg::this_cluster();
+        f = 0;
+        for (int r = 0; r < CL; ++r) f |= *cl.map_shared_rank(part, r);
+        T.sync();
+    }
+    return f;
+}
 
 constexpr int MOVE_THREADS = 512;
 constexpr int MAX_ROT = 2;
@@ -31,7 +89,11 @@ constexpr int MAX_ROT = 2;
 // Global scratch for the move kernels; every array is all-zero between
 // proposals (each proposal clears what it set).
 struct MoveScratch {
-    int8_t *group;      // [natoms]
+    int8_t *group;      // [natoms] move group for the cross-pair sum (0 fixed)
+    int8_t *body;       // [natoms] rigid body for the SASA reach test: equals
+                        // group, except the psi side of a crankshaft (2),
+                        // which turns twice and so moves against the rest of
+                        // its group
     uint8_t *mark;      // [natoms]
     double *xyz_new;    // [natoms*4]
     double *born_new;   // [natoms]
@@ -39,6 +101,7 @@ struct MoveScratch {
     int32_t *affected;  // [natoms] compaction list (per-system region)
     unsigned long long *ctr;  // [4*nsys] cumulative work counters: pair terms,
                               // hct terms, SASA neighbour visits, moved atoms
+    int *naff;                // [nsys] atoms in the affected list
 };
 
 // A j-side: sorted explicit atoms side_idx[eb, ee) plus the range [lo, hi).
@@ -233,13 +296,14 @@ __device__ __forceinline__ int member(const MoveDesc &M, const int32_t *side_idx
 // smem_d: >= 32 doubles; s_nAff: shared counter.  Leaves group/xyz_new/
 // born_new set for the members (the caller commits or discards, then calls
 // move_clear).
-template <typename R>
-__device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, double *smem_d, int *s_naff) {
+template <typename R, int CL>
+__device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, double *smem_d, double *part,
+                                const Team<CL> &T) {
     const AlmaBatch &b = C.b;
     const AlmaTopo &t = C.t;
     const MoveScratch &w = C.w;
-    const int tid = threadIdx.x, nthr = blockDim.x;
-    const int lane = tid & 31, wid = tid >> 5, nw = nthr >> 5;
+    const int tid = T.gtid(), nthr = T.gthreads();
+    const int lane = threadIdx.x & 31, wid = T.gwarp(), nw = T.gwarps();
     const int a0 = b.atom_off[s], a1 = b.atom_off[s + 1];
     const int64_t nm = n_members(M);
 
@@ -248,10 +312,11 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
         int g;
         const int m = member(M, t.side_idx, k, g);
         w.group[m] = (int8_t)(g + 1);
+        w.body[m] = (int8_t)(g + 1);
         *reinterpret_cast<double4 *>(w.xyz_new + 4 * (size_t)m) = ld_xyz(b.xyz, m);
     }
-    if (tid == 0) *s_naff = 0;
-    __syncthreads();
+    if (tid == 0) w.naff[s] = 0;
+    T.sync();
     // P2: the rotations, in order, on the proposal copy.
     for (int r = 0; r < M.nrot; ++r) {
         const Rot &Ro = M.rot[r];
@@ -261,8 +326,9 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
             double4 p = ld_xyz(w.xyz_new, m);
             rodrigues(p.x, p.y, p.z, Ro);
             *reinterpret_cast<double4 *>(w.xyz_new + 4 * (size_t)m) = p;
+            if (M.kind == 1 && r == 1) w.body[m] = 2;
         }
-        __syncthreads();
+        T.sync();
     }
     // P3: half-list Born radii of the members at the new geometry, and
     // marks on fixed atoms whose half row holds a member (SASA changes).
@@ -287,22 +353,22 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
             atomicAdd(&w.ctr[4 * s + 1], (unsigned long long)C.nl.half_len[m]);
         }
         // SASA reach: atoms i < j interact when j is in i's half row and
-        // r < R*_i + R*_j + 2 probe.  A pair whose distance changes (groups
-        // differ) and is within reach before or after the move changes the
-        // SASA of its lower atom only; mark that atom.
+        // r < R*_i + R*_j + 2 probe.  A pair whose distance changes (rigid
+        // bodies differ) and is within reach before or after the move
+        // changes the SASA of its lower atom only; mark that atom.
         const double4 pmo_s = ld_xyz(b.xyz, m);
         const double rsm = b.prm64[4 * (size_t)m + 1] + C.P.probe_r;
-        const int gm_s = w.group[m];
+        const int bm = w.body[m];
         for (int64_t e = C.nl.full_ptr[m] + lane; e < C.nl.full_ptr[m] + C.nl.full_len[m]; e += 32) {
             const int j = (int)(C.nl.full_cols[e] & ALMA_IDX_MASK);
+            if (w.body[j] == bm) continue;
             const int gj = w.group[j];
-            if (gj == gm_s) continue;
             const double dc = rsm + b.prm64[4 * (size_t)j + 1] + C.P.probe_r, dc2 = dc * dc;
             const double4 pjo = ld_xyz(b.xyz, j), pjn = gj ? ld_xyz(w.xyz_new, j) : pjo;
             if (d2_of(pmo_s, pjo) < dc2 || d2_of(pm, pjn) < dc2) w.mark[j < m ? j : m] = 1;
         }
     }
-    __syncthreads();
+    T.sync();
     // P4: cross pairs from the members' full rows, before and after.
     for (int64_t k = wid; k < nm; k += nw) {
         int g;
@@ -358,15 +424,15 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
     // results go to per-atom slots and are summed in atom order).
     for (int i = a0 + tid; i < a1; i += nthr) {
         if (w.mark[i]) {
-            const int slot = atomicAdd(s_naff, 1);
+            const int slot = atomicAdd(&w.naff[s], 1);
             w.affected[a0 + slot] = i;
         }
     }
-    __syncthreads();
+    T.sync();
     // P5: SASA of every affected atom, old and new, in row order; every
     // other atom's SASA is unchanged bit for bit (its half row holds no pair
     // whose distance changed within reach).
-    const int64_t naff = *s_naff;
+    const int64_t naff = w.naff[s];
     const double pi4 = 4.0 * 3.14159265358979323846, pi2 = 2.0 * 3.14159265358979323846;
     for (int64_t k = wid; k < naff; k += nw) {
         const int i = w.affected[a0 + k];
@@ -432,47 +498,58 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
         const double drn = sqrt(d2_of(pos_new(b.xyz, w.xyz_new, w.group, i), pos_new(b.xyz, w.xyz_new, w.group, j))) - C.P.r0_ss;
         dss += C.P.k_ss * drn * drn - C.P.k_ss * dro * dro;
     }
-    __syncthreads();
+    T.sync();
     if (tid == 0) atomicAdd(&w.ctr[4 * s + 3], (unsigned long long)nm);
-    // P7: deterministic sums.
+    // P7: deterministic sums (per-atom slots in atom order, then CTA
+    // partials in rank order).
     double c = 0.0, sa = 0.0;
     for (int i = a0 + tid; i < a1; i += nthr) {
         c += w.dE_atom[2 * (size_t)i];
         sa += w.dE_atom[2 * (size_t)i + 1];
     }
+    double v[4] = {c, sa, ddih, dss};
+    team_sum<CL, 4>(T, v, smem_d, part);
     MoveResult res;
-    res.dcross = block_sum(c, smem_d);
-    res.dsasa = block_sum(sa, smem_d);
-    res.ddih = block_sum(ddih, smem_d);
-    res.dss = block_sum(dss, smem_d);
+    res.dcross = v[0];
+    res.dsasa = v[1];
+    res.ddih = v[2];
+    res.dss = v[3];
     res.dE = res.dcross + res.dsasa + res.ddih + res.dss;
     return res;
 }
 
-// Commit (accept != 0) the members' proposal and clear all scratch.
-__device__ inline void move_finish(const MoveCtx &C, const MoveDesc &M, int s, const int *s_naff, int accept) {
+// Commit (accept != 0) the members' proposal, clear all scratch, and
+// return whether a committed atom drifted more than half the skin from its
+// position at the last list build (team-wide).
+template <int CL>
+__device__ inline int move_finish(const MoveCtx &C, const MoveDesc &M, int s, int accept, int *part_flag,
+                                  const Team<CL> &T) {
     const MoveScratch &w = C.w;
-    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int tid = T.gtid(), nthr = T.gthreads();
     const int a0 = C.b.atom_off[s];
     const int64_t nm = n_members(M);
+    int drift = 0;
     for (int64_t k = tid; k < nm; k += nthr) {
         int g;
         const int m = member(M, C.t.side_idx, k, g);
         if (accept) {
-            *reinterpret_cast<double4 *>(C.b.xyz + 4 * (size_t)m) = ld_xyz(w.xyz_new, m);
+            const double4 p = ld_xyz(w.xyz_new, m);
+            *reinterpret_cast<double4 *>(C.b.xyz + 4 * (size_t)m) = p;
             C.b.born[m] = w.born_new[m];
+            if (C.nl.ref_xyz && d2_of(p, ld_xyz(C.nl.ref_xyz, m)) > C.P.half_skin2) drift = 1;
         }
         w.group[m] = 0;
+        w.body[m] = 0;
         w.dE_atom[2 * (size_t)m] = 0.0;
         w.dE_atom[2 * (size_t)m + 1] = 0.0;
     }
-    const int naff = *s_naff;
+    const int naff = w.naff[s];
     for (int k = tid; k < naff; k += nthr) {
         const int i = w.affected[a0 + k];
         w.mark[i] = 0;
         w.dE_atom[2 * (size_t)i + 1] = 0.0;
     }
-    __syncthreads();
+    return team_or<CL>(T, drift, part_flag);
 }
 
 }  // namespace alma

@@ -69,7 +69,7 @@ class AlmaMCConfig(C.Structure):
                 ("angle_max", C.c_double), ("angle_min", C.c_double),
                 ("sidechain_mult", C.c_double), ("crank_prob", C.c_double),
                 ("concerted_prob", C.c_double), ("fixed_delta", C.c_double),
-                ("moveset_off", _p), ("moveset", _p), ("threads_per_system", _i32), ("pad", _i32)]
+                ("moveset_off", _p), ("moveset", _p), ("threads_per_system", _i32), ("cluster_size", _i32)]
 
 
 class AlmaChainState(C.Structure):

@@ -45,6 +45,7 @@ def mc_config(seed, policy=0, tune_freq=200, max_angle_bounds=(0.004, 0.5), fixe
     cfg.fixed_delta = float(fixed_delta)
     cfg.moveset_off = cfg.moveset = None
     cfg.threads_per_system = 0
+    cfg.cluster_size = 1
     if moveset is not None:
         off = np.zeros(nsys + 1, np.int32)
         off[1:] = np.cumsum([len(m) for m in moveset])
@@ -63,12 +64,21 @@ class MCRunner:
     initial max angle (the reference's max_angle)."""
 
     def __init__(self, batch: DeviceBatch, temperatures, seed, policy=0, cur_max0=0.12, tune_freq=200,
-                 fixed_delta=0.0, moveset=None):
+                 fixed_delta=0.0, moveset=None, cluster_size=None, threads=0):
         self.b = batch
         self.L = batch.L
         self._keep = []
         self.cfg = mc_config(seed, policy, tune_freq, fixed_delta=fixed_delta, moveset=moveset, nsys=batch.nsys,
                              device_keep=self._keep)
+        if cluster_size is None:  # small batches: spread each chain over a cluster of SMs
+            sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+            cluster_size = 1
+            for cl in (16, 8, 4, 2):
+                if batch.nsys * cl <= sms:
+                    cluster_size = cl
+                    break
+        self.cfg.cluster_size = int(cluster_size)
+        self.cfg.threads_per_system = int(threads)
         T = np.broadcast_to(np.asarray(temperatures, np.float64), (batch.nsys,)).copy()
         if np.any(T <= 0):
             raise ValueError("temperature must be positive")
