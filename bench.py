@@ -130,7 +130,11 @@ def run_ours(args, rank, world, local):
     chains, systems, movesets, temps, topos = make_workload(args.workload, rank)
     per_step = 1000 if args.workload == "single" else 100
     batch = DeviceBatch(systems, precision="mixed")
-    runner = MCRunner(batch, temps, seed=12345 + rank, policy=2, cur_max0=0.12, moveset=movesets)
+    from protein_physics_b200.mc import autotune
+    tuned = autotune(batch, temps, seed=777, policy=2, moveset=movesets,
+                     proposals=300 if args.workload == "single" else 30)
+    runner = MCRunner(batch, temps, seed=12345 + rank, policy=2, cur_max0=0.12, moveset=movesets,
+                      cluster_size=tuned[0], threads=tuned[1])
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     stream = torch.cuda.current_stream()
 
@@ -211,6 +215,7 @@ def run_ours(args, rank, world, local):
         h2d = ch.n * 8 * 6
         d2h = ch.n * 8 * 3
     clocks = sampler.summary()
+    de_err = de_error_vs_fp64(systems[0], movesets[0], runner.state()["cur_max"][0]) if rank == 0 else None
     out = None
     if rank == 0:
         value = prop_total / (ms_max * 1e-3)
@@ -232,6 +237,8 @@ def run_ours(args, rank, world, local):
                        "l2": "flushed between steps (256 MiB write)", "parallelism": "replicas" if world > 1 else "1 GPU"},
             "clocks": clocks,
             "gpu_launches": int(launches),
+            "dE_error_vs_fp64": de_err,
+            "tuned": {"cluster_size": tuned[0], "threads_per_system": tuned[1]},
             "wall_s": t_wall,
             "e2e": {"value": e2e_val, "unit": "proposals/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "api": "PhysicsEngine.generate_ensemble(host particles, topology, 1, 1000)"},
@@ -250,6 +257,34 @@ def run_ours(args, rank, world, local):
         dist.barrier()
         dist.destroy_process_group()
     return out
+
+
+def de_error_vs_fp64(system, moveset, cur_max, n=256):
+    """|ΔE(mixed) - ΔE(fp64)| over n seeded torsion proposals on the bench
+    chain (same state, same moves; the device FP64 path matches the
+    reference to 1e-7 kcal/mol)."""
+    import numpy as np
+    from protein_physics_b200.device import DeviceBatch
+    rng = np.random.default_rng(4242)
+    bm = DeviceBatch([system], precision="mixed")
+    bf = DeviceBatch([system], precision="fp64")
+    for b in (bm, bf):
+        b.build_nl()
+        b.born_radii()
+    errs, mags = [], []
+    F = system[4]
+    for _ in range(n):
+        k = int(moveset[rng.integers(0, len(moveset))])
+        base = cur_max * (1.0 if F.rb_kind[k] in (0, 1) else 2.5) * F.rb_scale[k]
+        d = float(rng.uniform(-base, base))
+        em, _ = bm.move_dE([0], [k], [[d, 0.0]])
+        ef, _ = bf.move_dE([0], [k], [[d, 0.0]])
+        em, ef = float(em[0]), float(ef[0])
+        errs.append(abs(em - ef))
+        mags.append(abs(ef))
+    errs = np.array(errs)
+    return {"max": float(errs.max()), "p99": float(np.percentile(errs, 99)), "median": float(np.median(errs)),
+            "n_moves": n, "median_abs_dE": float(np.median(mags)), "unit": "kcal/mol"}
 
 
 def cpu_baseline(ch, topo, T, args, budget_s=12.0):
@@ -319,8 +354,31 @@ def run_reference(args, rank, world):
             "e2e": {"value": value, "unit": "proposals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def run_profile_case(args):
+    """Small case for ncu: the single-chain workload, 100 warm-up proposals,
+    then exactly one mc_kernel launch of 200 proposals (no rebuild inside:
+    the launch stops at the first drift flag)."""
+    import torch
+    from protein_physics_b200.device import DeviceBatch
+    from protein_physics_b200.mc import MCRunner
+    chains, systems, movesets, temps, topos = make_workload("single", 0)
+    batch = DeviceBatch(systems, precision="mixed")
+    runner = MCRunner(batch, temps, seed=12345, policy=2, moveset=movesets, cluster_size=args.cluster,
+                      threads=args.threads)
+    runner.run(100)
+    lim = int(runner.state()["step"].max()) + 200
+    runner.launch(lim)
+    torch.cuda.synchronize()
+    st = runner.state()
+    print(json.dumps({"profile_case": "single chain", "atoms": chains[0].n, "steps_done": int(st["step"][0]),
+                      "cluster": args.cluster, "threads": args.threads}))
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--profile", action="store_true", help="one mc_kernel launch on the single chain (for ncu)")
+    ap.add_argument("--cluster", type=int, default=16)
+    ap.add_argument("--threads", type=int, default=512)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
@@ -328,6 +386,9 @@ def main():
     ap.add_argument("--workload", default="single", choices=["single", "batched"])
     args = ap.parse_args()
     rank, world, local = rank_info()
+    if args.profile:
+        run_profile_case(args)
+        return
     if args.impl == "reference":
         out = run_reference(args, rank, world)
     else:

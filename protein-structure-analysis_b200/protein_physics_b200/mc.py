@@ -127,6 +127,44 @@ class MCRunner:
                 return st
 
 
+_TUNED = {}
+
+
+def autotune(batch, temperatures, seed, policy=0, moveset=None, proposals=200, candidates=None):
+    """Picks (cluster_size, threads_per_system) for this batch shape by
+    timing `proposals` proposals per candidate on a scratch copy of the
+    batch state; cached per (systems, atom-count bucket, policy)."""
+    import time
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    key = (batch.nsys, int(np.log2(max(1, batch.natoms // max(1, batch.nsys)))), policy, moveset is not None)
+    if key in _TUNED:
+        return _TUNED[key]
+    if candidates is None:
+        candidates = [(cl, nt) for cl in (1, 2, 4, 8, 16) for nt in (256, 512) if batch.nsys * cl <= 2 * sms]
+    xyz0, born0 = batch.xyz.clone(), batch.born.clone()
+    best, best_rate = None, -1.0
+    for cl, nt in candidates:
+        try:
+            R = MCRunner(batch, temperatures, seed, policy=policy, moveset=moveset, cluster_size=cl, threads=nt)
+            R.run(max(10, proposals // 10))
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            R.run(proposals)
+            torch.cuda.synchronize()
+            rate = proposals * batch.nsys / (time.perf_counter() - t0)
+        except RuntimeError:
+            continue
+        finally:
+            batch.xyz.copy_(xyz0)
+            batch.born.copy_(born0)
+            batch.nl_ready = False
+        if rate > best_rate:
+            best, best_rate = (cl, nt), rate
+    batch.build_nl()
+    _TUNED[key] = best
+    return best
+
+
 def _check_inputs(state, topology):
     if len(state) == 0:
         raise ValueError("initial_state empty")
