@@ -238,7 +238,7 @@ typedef struct {
     int64_t n_proposed, n_accepted, n_rebuild;
     int32_t acc_win, tot_win; /* adaptation window                           */
     int32_t need_rebuild;     /* set when an accepted move drifted > skin/2  */
-    int32_t pad;
+    int32_t parity;           /* scratch double-buffer selector (internal)   */
 } AlmaChainState;
 
 /* Runs proposals on every system until its state.step reaches step_limit

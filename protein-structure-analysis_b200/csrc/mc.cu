@@ -51,8 +51,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) mc_kernel(MoveCtx C, MCConfigDev
                                                           AlmaChainState *__restrict__ states, int64_t step_limit) {
     __shared__ MoveDesc M;
     __shared__ double sm[32];
-    __shared__ double part[4];
-    __shared__ int flag;
+    __shared__ double part[8];
     __shared__ AlmaChainState S;
     __shared__ double u[6];
     __shared__ int did_move, accept;
@@ -125,15 +124,18 @@ __global__ void __launch_bounds__(NT, 512 / NT) mc_kernel(MoveCtx C, MCConfigDev
             __syncthreads();
             continue;
         }
-        // every CTA must have read the current coordinates before any
-        // commits of this proposal: move_eval starts with a team barrier
-        // only after P1, which writes scratch, not coordinates.
-        const MoveResult r = move_eval<R, CL>(C, M, s, sm, part, T);
+        const int parity = S.parity & 1;
+        const MoveResult r = move_eval<R, CL>(C, M, s, sm, part, parity, T);
         if (threadIdx.x == 0) accept = (r.dE < 0.0) || (u[3] < exp(-r.dE / S.temperature));
         __syncthreads();
         const int acc = accept;
-        const int drift = move_finish<CL>(C, M, s, acc, &flag, T);
+        move_finish<CL>(C, M, s, acc, parity, T);
+        // commits and the drift flag visible to every CTA before the state
+        // update and the next proposal's coordinate reads
+        T.sync();
+        const int drift = C.w.drift[2 * s + parity];
         if (threadIdx.x == 0) {
+            S.parity ^= 1;
             S.n_proposed++;
             if (acc) {
                 S.n_accepted++;
@@ -150,9 +152,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) mc_kernel(MoveCtx C, MCConfigDev
             }
             S.step++;
         }
-        // commits of this proposal visible to every CTA before the next
-        // proposal reads coordinates
-        T.sync();
+        __syncthreads();
     }
     if (threadIdx.x == 0 && T.rank == 0) states[s] = S;
 }

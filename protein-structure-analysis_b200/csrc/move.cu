@@ -19,9 +19,9 @@ static size_t carve_scratch(MoveScratch *w, char *base, int32_t natoms) {
     t.xyz_new = (double *)take(sizeof(double) * 4 * (size_t)natoms);
     t.born_new = (double *)take(sizeof(double) * (size_t)natoms);
     t.dE_atom = (double *)take(sizeof(double) * 2 * (size_t)natoms);
-    t.affected = (int32_t *)take(sizeof(int32_t) * (size_t)natoms);
     t.ctr = (unsigned long long *)take(sizeof(unsigned long long) * 4 * (size_t)(natoms + 1));
-    t.naff = (int *)take(sizeof(int) * (size_t)(natoms + 1));
+    t.queue = (int *)take(sizeof(int) * 8 * (size_t)(natoms + 1));
+    t.drift = (int *)take(sizeof(int) * 2 * (size_t)(natoms + 1));
     if (w) *w = t;
     return off;
 }
@@ -33,12 +33,13 @@ __global__ void __launch_bounds__(MOVE_THREADS) move_dE_kernel(MoveCtx C, const 
                                                                double *__restrict__ dE, double *__restrict__ dterms) {
     __shared__ MoveDesc M;
     __shared__ double sm[32];
-    __shared__ double part[4];
-    __shared__ int flag;
+    __shared__ double part[8];
     const Team<1> T;
     const int s = blockIdx.x;
     const int k = kind[s];
     if (threadIdx.x == 0) {
+        for (int q = 0; q < 8; ++q) C.w.queue[8 * s + q] = 0;  // fresh queues: parity 0
+        C.w.drift[2 * s] = C.w.drift[2 * s + 1] = 0;
         if (k >= 0) decode_move(M, C.t, C.b.xyz, s, k, a[s], delta + 2 * (size_t)s);
         else M.degenerate = 1;
     }
@@ -51,7 +52,7 @@ __global__ void __launch_bounds__(MOVE_THREADS) move_dE_kernel(MoveCtx C, const 
         }
         return;
     }
-    const MoveResult r = move_eval<R, 1>(C, M, s, sm, part, T);
+    const MoveResult r = move_eval<R, 1>(C, M, s, sm, part, 0, T);
     if (threadIdx.x == 0) {
         dE[s] = r.dE;
         dterms[4 * (size_t)s + 0] = r.dcross;
@@ -59,7 +60,7 @@ __global__ void __launch_bounds__(MOVE_THREADS) move_dE_kernel(MoveCtx C, const 
         dterms[4 * (size_t)s + 2] = r.ddih;
         dterms[4 * (size_t)s + 3] = r.dss;
     }
-    move_finish<1>(C, M, s, apply, &flag, T);
+    move_finish<1>(C, M, s, apply, 0, T);
 }
 
 }  // namespace alma

@@ -68,21 +68,6 @@ __device__ __forceinline__ void team_sum(const Team<CL> &T, double (&v)[K], doub
     }
 }
 
-// Team-wide OR of one flag per thread.
-template <int CL>
-__device__ __forceinline__ int team_or(const Team<CL> &T, int f, int *part) {
-    f = __syncthreads_or(f);
-    if constexpr (CL > 1) {
-        if (threadIdx.x == 0) *part = f;
-        T.sync();
-        cg::cluster_group cl = cg::this_cluster();
-        f = 0;
-        for (int r = 0; r < CL; ++r) f |= *cl.map_shared_rank(part, r);
-        T.sync();
-    }
-    return f;
-}
-
 constexpr int MOVE_THREADS = 512;
 constexpr int MAX_ROT = 2;
 
@@ -98,10 +83,10 @@ struct MoveScratch {
     double *xyz_new;    // [natoms*4]
     double *born_new;   // [natoms]
     double *dE_atom;    // [natoms*2]
-    int32_t *affected;  // [natoms] compaction list (per-system region)
     unsigned long long *ctr;  // [4*nsys] cumulative work counters: pair terms,
                               // hct terms, SASA neighbour visits, moved atoms
-    int *naff;                // [nsys] atoms in the affected list
+    int *queue;               // [8*nsys] work-queue counters, two proposals
+    int *drift;               // [2*nsys] drift flags, two proposals
 };
 
 // A j-side: sorted explicit atoms side_idx[eb, ee) plus the range [lo, hi).
@@ -296,43 +281,71 @@ __device__ __forceinline__ int member(const MoveDesc &M, const int32_t *side_idx
 // smem_d: >= 32 doubles; s_nAff: shared counter.  Leaves group/xyz_new/
 // born_new set for the members (the caller commits or discards, then calls
 // move_clear).
+// Per-warp dynamic work distribution: lane 0 takes the next item of a
+// queue counter, the warp gets it by shuffle.
+__device__ __forceinline__ int warp_take(int *q) {
+    int v = 0;
+    if ((threadIdx.x & 31) == 0) v = atomicAdd(q, 1);
+    return __shfl_sync(0xffffffffu, v, 0);
+}
+
+// Whole-team evaluation of a decoded, non-degenerate proposal of system s.
+// parity alternates between consecutive proposals (double-buffered queue
+// counters, CTA partials and drift flag).  Leaves group/body/xyz_new/
+// born_new set for the members; move_finish commits or discards.
+//
+// Team barriers: (1) after the proposal copy, (2) after the member Born
+// radii and SASA marks, (3) after the cross-pair and SASA slots, (4) the
+// CTA-partials exchange of team_sum.
 template <typename R, int CL>
 __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, double *smem_d, double *part,
-                                const Team<CL> &T) {
+                                int parity, const Team<CL> &T) {
     const AlmaBatch &b = C.b;
     const AlmaTopo &t = C.t;
     const MoveScratch &w = C.w;
     const int tid = T.gtid(), nthr = T.gthreads();
-    const int lane = threadIdx.x & 31, wid = T.gwarp(), nw = T.gwarps();
+    const int lane = threadIdx.x & 31;
     const int a0 = b.atom_off[s], a1 = b.atom_off[s + 1];
     const int64_t nm = n_members(M);
+    int *q = w.queue + 8 * s + 4 * parity;  // this proposal's queue counters
 
-    // P1: group flags and starting copies of the member coordinates.
+    // P1: move groups, rigid bodies and the proposed coordinates — every
+    // rotation applied in order (the crankshaft's second rotation turns its
+    // psi side again, taking the axis from the post-phi positions).
     for (int64_t k = tid; k < nm; k += nthr) {
         int g;
         const int m = member(M, t.side_idx, k, g);
-        w.group[m] = (int8_t)(g + 1);
-        w.body[m] = (int8_t)(g + 1);
-        *reinterpret_cast<double4 *>(w.xyz_new + 4 * (size_t)m) = ld_xyz(b.xyz, m);
-    }
-    if (tid == 0) w.naff[s] = 0;
-    T.sync();
-    // P2: the rotations, in order, on the proposal copy.
-    for (int r = 0; r < M.nrot; ++r) {
-        const Rot &Ro = M.rot[r];
-        const int64_t nr = side_count(Ro.side);
-        for (int64_t k = tid; k < nr; k += nthr) {
-            const int m = side_atom(Ro.side, t.side_idx, k);
-            double4 p = ld_xyz(w.xyz_new, m);
-            rodrigues(p.x, p.y, p.z, Ro);
-            *reinterpret_cast<double4 *>(w.xyz_new + 4 * (size_t)m) = p;
-            if (M.kind == 1 && r == 1) w.body[m] = 2;
+        double4 p = ld_xyz(b.xyz, m);
+        int body = g + 1;
+        if (M.kind == 2) {
+            rodrigues(p.x, p.y, p.z, M.rot[g]);
+        } else {
+            rodrigues(p.x, p.y, p.z, M.rot[0]);
+            if (M.kind == 1 && side_has(M.rot[1].side, t.side_idx, m)) {
+                rodrigues(p.x, p.y, p.z, M.rot[1]);
+                body = 2;
+            }
         }
-        T.sync();
+        w.group[m] = (int8_t)(g + 1);
+        w.body[m] = (int8_t)body;
+        *reinterpret_cast<double4 *>(w.xyz_new + 4 * (size_t)m) = p;
     }
-    // P3: half-list Born radii of the members at the new geometry, and
-    // marks on fixed atoms whose half row holds a member (SASA changes).
-    for (int64_t k = wid; k < nm; k += nw) {
+    T.sync();
+    // The other parity's counters and drift flag belong to the previous
+    // proposal, whose last readers finished before the barrier above: clear
+    // them for the next proposal.
+    if (tid == 0) {
+        int *qn = w.queue + 8 * s + 4 * (parity ^ 1);
+        qn[0] = qn[1] = qn[2] = qn[3] = 0;
+        w.drift[2 * s + (parity ^ 1)] = 0;
+    }
+
+    // P2: half-list Born radii of the members at the new geometry (P4
+    // semantics) and SASA marks.  SASA reach: atoms i < j interact when j is
+    // in i's half row and r < R*_i + R*_j + 2 probe; a pair whose distance
+    // changes (rigid bodies differ) and is within reach before or after the
+    // move changes the SASA of its lower atom only: mark that atom.
+    for (int k = warp_take(&q[0]); k < nm; k = warp_take(&q[0])) {
         int g;
         const int m = member(M, t.side_idx, k, g);
         const double4 pm = ld_xyz(w.xyz_new, m);
@@ -352,25 +365,23 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
             w.born_new[m] = 1.0 / fmax(1.0 / b.prm64[4 * (size_t)m + 1] - 0.5 * sum, 2.0);
             atomicAdd(&w.ctr[4 * s + 1], (unsigned long long)C.nl.half_len[m]);
         }
-        // SASA reach: atoms i < j interact when j is in i's half row and
-        // r < R*_i + R*_j + 2 probe.  A pair whose distance changes (rigid
-        // bodies differ) and is within reach before or after the move
-        // changes the SASA of its lower atom only; mark that atom.
-        const double4 pmo_s = ld_xyz(b.xyz, m);
+        const double4 pmo = ld_xyz(b.xyz, m);
         const double rsm = b.prm64[4 * (size_t)m + 1] + C.P.probe_r;
         const int bm = w.body[m];
         for (int64_t e = C.nl.full_ptr[m] + lane; e < C.nl.full_ptr[m] + C.nl.full_len[m]; e += 32) {
             const int j = (int)(C.nl.full_cols[e] & ALMA_IDX_MASK);
             if (w.body[j] == bm) continue;
-            const int gj = w.group[j];
             const double dc = rsm + b.prm64[4 * (size_t)j + 1] + C.P.probe_r, dc2 = dc * dc;
-            const double4 pjo = ld_xyz(b.xyz, j), pjn = gj ? ld_xyz(w.xyz_new, j) : pjo;
-            if (d2_of(pmo_s, pjo) < dc2 || d2_of(pm, pjn) < dc2) w.mark[j < m ? j : m] = 1;
+            const double4 pjo = ld_xyz(b.xyz, j), pjn = w.group[j] ? ld_xyz(w.xyz_new, j) : pjo;
+            if (d2_of(pmo, pjo) < dc2 || d2_of(pm, pjn) < dc2) w.mark[j < m ? j : m] = 1;
         }
     }
     T.sync();
-    // P4: cross pairs from the members' full rows, before and after.
-    for (int64_t k = wid; k < nm; k += nw) {
+
+    // P3: cross pairs from the members' full rows (old and new geometry in
+    // one pass), then SASA of the marked atoms (old and new, in row order),
+    // both pulled from queues; boundary dihedrals and disulfides strided.
+    for (int k = warp_take(&q[1]); k < nm; k = warp_take(&q[1])) {
         int g;
         const int m = member(M, t.side_idx, k, g);
         const int gm = g + 1;
@@ -387,17 +398,17 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
             const int j = (int)(ent & ALMA_IDX_MASK);
             const int gj = w.group[j];
             if (gj == gm || (gj != 0 && j < m)) continue;
+            const double4 pjo = ld_xyz(b.xyz, j);
+            const double4 pjn = gj ? ld_xyz(w.xyz_new, j) : pjo;
+            const double r2o = d2_of(pmo, pjo), r2n = d2_of(pmn, pjn);
+            const bool ino = r2o <= C.P.pair_cut2, inn = r2n <= C.P.pair_cut2;
+            if (!ino && !inn) continue;
+            npair += (int)ino + (int)inn;
             R qj, rj, ej;
             prm_of<R>(b.prm, b.prm64, j, qj, rj, ej);
             const R qp = qm * qj, sig = rm + rj, ep = em * ej;
-            const double4 pjo = ld_xyz(b.xyz, j);
-            const double r2o = d2_of(pmo, pjo);
             const R ajo = (R)b.born[j];
-            const double4 pjn = gj ? ld_xyz(w.xyz_new, j) : pjo;
-            const double r2n = d2_of(pmn, pjn);
             const R ajn = gj ? (R)w.born_new[j] : ajo;
-            const bool ino = r2o <= C.P.pair_cut2, inn = r2n <= C.P.pair_cut2;
-            npair += (int)ino + (int)inn;
             if (ino && inn) {
                 // FP64 sigma/epsilon only for contacts inside sigma (steep LJ)
                 double sig64 = (double)sig, eps64 = (double)ep;
@@ -409,7 +420,7 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
                 acc += pair_delta<R>(C.P, r2o, r2n, qp, sig, ep, amo * ajo, amn * ajn, sig64, eps64);
             } else if (ino) {
                 acc -= (double)pair_energy<R>(C.P, (R)r2o, qp, sig, ep, amo, ajo);
-            } else if (inn) {
+            } else {
                 acc += (double)pair_energy<R>(C.P, (R)r2n, qp, sig, ep, amn, ajn);
             }
         }
@@ -420,69 +431,62 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
             atomicAdd(&w.ctr[4 * s + 0], (unsigned long long)npair);
         }
     }
-    // Atoms whose SASA can change -> compaction list (order irrelevant:
-    // results go to per-atom slots and are summed in atom order).
-    for (int i = a0 + tid; i < a1; i += nthr) {
-        if (w.mark[i]) {
-            const int slot = atomicAdd(&w.naff[s], 1);
-            w.affected[a0 + slot] = i;
-        }
-    }
-    T.sync();
-    // P5: SASA of every affected atom, old and new, in row order; every
-    // other atom's SASA is unchanged bit for bit (its half row holds no pair
-    // whose distance changed within reach).
-    const int64_t naff = w.naff[s];
     const double pi4 = 4.0 * 3.14159265358979323846, pi2 = 2.0 * 3.14159265358979323846;
-    for (int64_t k = wid; k < naff; k += nw) {
-        const int i = w.affected[a0 + k];
-        const bool moved = w.group[i] != 0;
-        const double4 pio = ld_xyz(b.xyz, i), pin = moved ? ld_xyz(w.xyz_new, i) : pio;
-        const double rsi = b.prm64[4 * (size_t)i + 1] + C.P.probe_r;
-        const double cs = pi2 * rsi * rsi;
-        double sao = pi4 * rsi * rsi, san = sao;
-        const int64_t beg = C.nl.half_ptr[i], end = C.nl.half_ptr[i] + C.nl.half_len[i];
-        for (int64_t e0 = beg; e0 < end; e0 += 32) {
-            const int64_t e = e0 + lane;
-            double co = 0.0, cn = 0.0;
-            bool ho = false, hn = false;
-            if (e < end) {
-                const int j = (int)(C.nl.half_cols[e] & ALMA_IDX_MASK);
-                const double rsj = b.prm64[4 * (size_t)j + 1] + C.P.probe_r;
-                const double dc = rsi + rsj;
-                const double4 pjo = ld_xyz(b.xyz, j);
-                const double ro = sqrt(d2_of(pio, pjo));
-                if (ro < dc) { ho = true; co = cs * ((dc - ro) / (2.0 * rsi)); }
-                const double4 pjn = w.group[j] ? ld_xyz(w.xyz_new, j) : pjo;
-                const double rn = sqrt(d2_of(pin, pjn));
-                if (rn < dc) { hn = true; cn = cs * ((dc - rn) / (2.0 * rsi)); }
+    const int nchunk = (a1 - a0 + 31) >> 5;
+    unsigned long long nsasa = 0;
+    for (int c = warp_take(&q[2]); c < nchunk; c = warp_take(&q[2])) {
+        const int ia = a0 + 32 * c + lane;
+        unsigned todo = __ballot_sync(0xffffffffu, ia < a1 && w.mark[ia]);
+        while (todo) {
+            const int l = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const int i = a0 + 32 * c + l;
+            const bool moved = w.group[i] != 0;
+            const double4 pio = ld_xyz(b.xyz, i), pin = moved ? ld_xyz(w.xyz_new, i) : pio;
+            const double rsi = b.prm64[4 * (size_t)i + 1] + C.P.probe_r;
+            const double cs = pi2 * rsi * rsi;
+            double sao = pi4 * rsi * rsi, san = sao;
+            const int64_t beg = C.nl.half_ptr[i], end = C.nl.half_ptr[i] + C.nl.half_len[i];
+            for (int64_t e0 = beg; e0 < end; e0 += 32) {
+                const int64_t e = e0 + lane;
+                double co = 0.0, cn = 0.0;
+                bool ho = false, hn = false;
+                if (e < end) {
+                    const int j = (int)(C.nl.half_cols[e] & ALMA_IDX_MASK);
+                    const double rsj = b.prm64[4 * (size_t)j + 1] + C.P.probe_r;
+                    const double dc = rsi + rsj;
+                    const double4 pjo = ld_xyz(b.xyz, j);
+                    const double ro = sqrt(d2_of(pio, pjo));
+                    if (ro < dc) { ho = true; co = cs * ((dc - ro) / (2.0 * rsi)); }
+                    const double4 pjn = w.group[j] ? ld_xyz(w.xyz_new, j) : pjo;
+                    const double rn = sqrt(d2_of(pin, pjn));
+                    if (rn < dc) { hn = true; cn = cs * ((dc - rn) / (2.0 * rsi)); }
+                }
+                unsigned mo = __ballot_sync(0xffffffffu, ho), mn = __ballot_sync(0xffffffffu, hn);
+                while (mo) {
+                    const int l2 = __ffs(mo) - 1;
+                    mo &= mo - 1;
+                    sao -= fmin(sao * 0.85, __shfl_sync(0xffffffffu, co, l2));
+                }
+                while (mn) {
+                    const int l2 = __ffs(mn) - 1;
+                    mn &= mn - 1;
+                    san -= fmin(san * 0.85, __shfl_sync(0xffffffffu, cn, l2));
+                }
             }
-            unsigned mo = __ballot_sync(0xffffffffu, ho), mn = __ballot_sync(0xffffffffu, hn);
-            while (mo) {
-                const int l = __ffs(mo) - 1;
-                mo &= mo - 1;
-                sao -= fmin(sao * 0.85, __shfl_sync(0xffffffffu, co, l));
-            }
-            while (mn) {
-                const int l = __ffs(mn) - 1;
-                mn &= mn - 1;
-                san -= fmin(san * 0.85, __shfl_sync(0xffffffffu, cn, l));
-            }
-        }
-        if (lane == 0) {
-            w.dE_atom[2 * (size_t)i + 1] = C.P.gamma_sa * (fmax(0.0, san) - fmax(0.0, sao));
-            atomicAdd(&w.ctr[4 * s + 2], 2ull * (unsigned long long)(end - beg));
+            if (lane == 0) w.dE_atom[2 * (size_t)i + 1] = C.P.gamma_sa * (fmax(0.0, san) - fmax(0.0, sao));
+            nsasa += 2ull * (unsigned long long)(end - beg);
         }
     }
-    // P6: boundary dihedral records and disulfides of system s.
+    if (lane == 0 && nsasa) atomicAdd(&w.ctr[4 * s + 2], nsasa);
     double ddih = 0.0, dss = 0.0;
     for (int r = t.dih_off[s] + tid; r < t.dih_off[s + 1]; r += nthr) {
-        const int4 q = *reinterpret_cast<const int4 *>(t.dih_abcd + 4 * (size_t)r);
-        const int sa = w.group[q.x] != 0, sb = w.group[q.y] != 0, sc = w.group[q.z] != 0, sd = w.group[q.w] != 0;
+        const int4 qd = *reinterpret_cast<const int4 *>(t.dih_abcd + 4 * (size_t)r);
+        const int sa = w.group[qd.x] != 0, sb = w.group[qd.y] != 0, sc = w.group[qd.z] != 0, sd = w.group[qd.w] != 0;
         if (!(sa || sb || sc || sd) || (sa && sb && sc && sd)) continue;
-        const double po = dih_angle4(ld_xyz(b.xyz, q.x), ld_xyz(b.xyz, q.y), ld_xyz(b.xyz, q.z), ld_xyz(b.xyz, q.w));
-        const double pn = dih_angle4(pos_new(b.xyz, w.xyz_new, w.group, q.x), pos_new(b.xyz, w.xyz_new, w.group, q.y),
-                                     pos_new(b.xyz, w.xyz_new, w.group, q.z), pos_new(b.xyz, w.xyz_new, w.group, q.w));
+        const double po = dih_angle4(ld_xyz(b.xyz, qd.x), ld_xyz(b.xyz, qd.y), ld_xyz(b.xyz, qd.z), ld_xyz(b.xyz, qd.w));
+        const double pn = dih_angle4(pos_new(b.xyz, w.xyz_new, w.group, qd.x), pos_new(b.xyz, w.xyz_new, w.group, qd.y),
+                                     pos_new(b.xyz, w.xyz_new, w.group, qd.z), pos_new(b.xyz, w.xyz_new, w.group, qd.w));
         double eo = 0.0, en = 0.0;
         for (int k = t.term_off[r]; k < t.term_off[r + 1]; ++k) {
             const double n = (double)t.term_n[k];
@@ -498,17 +502,18 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
         const double drn = sqrt(d2_of(pos_new(b.xyz, w.xyz_new, w.group, i), pos_new(b.xyz, w.xyz_new, w.group, j))) - C.P.r0_ss;
         dss += C.P.k_ss * drn * drn - C.P.k_ss * dro * dro;
     }
-    T.sync();
     if (tid == 0) atomicAdd(&w.ctr[4 * s + 3], (unsigned long long)nm);
-    // P7: deterministic sums (per-atom slots in atom order, then CTA
-    // partials in rank order).
+    T.sync();
+
+    // P4: deterministic sums — per-atom slots in atom order, then the CTA
+    // partials in rank order.
     double c = 0.0, sa = 0.0;
     for (int i = a0 + tid; i < a1; i += nthr) {
         c += w.dE_atom[2 * (size_t)i];
         sa += w.dE_atom[2 * (size_t)i + 1];
     }
     double v[4] = {c, sa, ddih, dss};
-    team_sum<CL, 4>(T, v, smem_d, part);
+    team_sum<CL, 4>(T, v, smem_d, part + 4 * parity);
     MoveResult res;
     res.dcross = v[0];
     res.dsasa = v[1];
@@ -518,15 +523,16 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
     return res;
 }
 
-// Commit (accept != 0) the members' proposal, clear all scratch, and
-// return whether a committed atom drifted more than half the skin from its
-// position at the last list build (team-wide).
+// Commit (accept != 0) the members' proposal and clear all scratch; flags a
+// committed atom that drifted more than half the skin from its position at
+// the last list build in w.drift[2s + parity] (read after the caller's
+// next team barrier).
 template <int CL>
-__device__ inline int move_finish(const MoveCtx &C, const MoveDesc &M, int s, int accept, int *part_flag,
-                                  const Team<CL> &T) {
+__device__ inline void move_finish(const MoveCtx &C, const MoveDesc &M, int s, int accept, int parity,
+                                   const Team<CL> &T) {
     const MoveScratch &w = C.w;
     const int tid = T.gtid(), nthr = T.gthreads();
-    const int a0 = C.b.atom_off[s];
+    const int a0 = C.b.atom_off[s], a1 = C.b.atom_off[s + 1];
     const int64_t nm = n_members(M);
     int drift = 0;
     for (int64_t k = tid; k < nm; k += nthr) {
@@ -541,15 +547,14 @@ __device__ inline int move_finish(const MoveCtx &C, const MoveDesc &M, int s, in
         w.group[m] = 0;
         w.body[m] = 0;
         w.dE_atom[2 * (size_t)m] = 0.0;
-        w.dE_atom[2 * (size_t)m + 1] = 0.0;
     }
-    const int naff = w.naff[s];
-    for (int k = tid; k < naff; k += nthr) {
-        const int i = w.affected[a0 + k];
-        w.mark[i] = 0;
-        w.dE_atom[2 * (size_t)i + 1] = 0.0;
+    for (int i = a0 + tid; i < a1; i += nthr) {
+        if (w.mark[i]) {
+            w.mark[i] = 0;
+            w.dE_atom[2 * (size_t)i + 1] = 0.0;
+        }
     }
-    return team_or<CL>(T, drift, part_flag);
+    if (__any_sync(0xffffffffu, drift) && (threadIdx.x & 31) == 0) atomicOr(&w.drift[2 * s + parity], 1);
 }
 
 }  // namespace alma

@@ -75,13 +75,13 @@ class AlmaMCConfig(C.Structure):
 class AlmaChainState(C.Structure):
     _fields_ = [("cur_max", C.c_double), ("energy", C.c_double), ("temperature", C.c_double),
                 ("step", _i64), ("n_proposed", _i64), ("n_accepted", _i64), ("n_rebuild", _i64),
-                ("acc_win", _i32), ("tot_win", _i32), ("need_rebuild", _i32), ("pad", _i32)]
+                ("acc_win", _i32), ("tot_win", _i32), ("need_rebuild", _i32), ("parity", _i32)]
 
 
 # numpy view of AlmaChainState (72 bytes)
 STATE_DTYPE = np.dtype([("cur_max", "f8"), ("energy", "f8"), ("temperature", "f8"), ("step", "i8"),
                         ("n_proposed", "i8"), ("n_accepted", "i8"), ("n_rebuild", "i8"), ("acc_win", "i4"),
-                        ("tot_win", "i4"), ("need_rebuild", "i4"), ("pad", "i4")])
+                        ("tot_win", "i4"), ("need_rebuild", "i4"), ("parity", "i4")])
 assert STATE_DTYPE.itemsize == C.sizeof(AlmaChainState) == 72
 
 _lib = None
