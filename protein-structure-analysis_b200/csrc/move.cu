@@ -15,10 +15,11 @@ static size_t carve_scratch(MoveScratch *w, char *base, int32_t natoms) {
     MoveScratch t;
     t.group = (int8_t *)take((size_t)natoms);
     t.body = (int8_t *)take((size_t)natoms);
-    t.mark = (uint8_t *)take((size_t)natoms);
+    t.mark = (int *)take(sizeof(int) * (size_t)natoms);
     t.xyz_new = (double *)take(sizeof(double) * 4 * (size_t)natoms);
     t.born_new = (double *)take(sizeof(double) * (size_t)natoms);
     t.dE_atom = (double *)take(sizeof(double) * 2 * (size_t)natoms);
+    t.affected = (int32_t *)take(sizeof(int32_t) * (size_t)natoms);
     t.ctr = (unsigned long long *)take(sizeof(unsigned long long) * 4 * (size_t)(natoms + 1));
     t.queue = (int *)take(sizeof(int) * 8 * (size_t)(natoms + 1));
     t.drift = (int *)take(sizeof(int) * 2 * (size_t)(natoms + 1));

@@ -79,13 +79,17 @@ struct MoveScratch {
                         // group, except the psi side of a crankshaft (2),
                         // which turns twice and so moves against the rest of
                         // its group
-    uint8_t *mark;      // [natoms]
+    int *mark;          // [natoms] SASA recompute flags (first marker appends
+                        // the atom to `affected`)
     double *xyz_new;    // [natoms*4]
     double *born_new;   // [natoms]
     double *dE_atom;    // [natoms*2]
+    int32_t *affected;  // [natoms] atoms whose SASA is recomputed (per-system
+                        // region), appended during the marking pass
     unsigned long long *ctr;  // [4*nsys] cumulative work counters: pair terms,
                               // hct terms, SASA neighbour visits, moved atoms
-    int *queue;               // [8*nsys] work-queue counters, two proposals
+    int *queue;               // [8*nsys] per proposal parity: [3] = affected
+                              // atoms (other slots reserved), two parities
     int *drift;               // [2*nsys] drift flags, two proposals
 };
 
@@ -281,22 +285,15 @@ __device__ __forceinline__ int member(const MoveDesc &M, const int32_t *side_idx
 // smem_d: >= 32 doubles; s_nAff: shared counter.  Leaves group/xyz_new/
 // born_new set for the members (the caller commits or discards, then calls
 // move_clear).
-// Per-warp dynamic work distribution: lane 0 takes the next item of a
-// queue counter, the warp gets it by shuffle.
-__device__ __forceinline__ int warp_take(int *q) {
-    int v = 0;
-    if ((threadIdx.x & 31) == 0) v = atomicAdd(q, 1);
-    return __shfl_sync(0xffffffffu, v, 0);
-}
-
 // Whole-team evaluation of a decoded, non-degenerate proposal of system s.
 // parity alternates between consecutive proposals (double-buffered queue
 // counters, CTA partials and drift flag).  Leaves group/body/xyz_new/
 // born_new set for the members; move_finish commits or discards.
 //
-// Team barriers: (1) after the proposal copy, (2) after the member Born
-// radii and SASA marks, (3) after the cross-pair and SASA slots, (4) the
-// CTA-partials exchange of team_sum.
+// Rows are strided over the team's warps.  Team barriers: (1) after the
+// proposal copy, (2) after the member Born radii and SASA marks (the marking
+// pass also builds the affected-atom list), (3) after the cross-pair and
+// SASA slots, (4) the CTA-partials exchange of team_sum.
 template <typename R, int CL>
 __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, double *smem_d, double *part,
                                 int parity, const Team<CL> &T) {
@@ -345,7 +342,8 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
     // in i's half row and r < R*_i + R*_j + 2 probe; a pair whose distance
     // changes (rigid bodies differ) and is within reach before or after the
     // move changes the SASA of its lower atom only: mark that atom.
-    for (int k = warp_take(&q[0]); k < nm; k = warp_take(&q[0])) {
+    const int wid = T.gwarp(), nw = T.gwarps();
+    for (int64_t k = wid; k < nm; k += nw) {
         int g;
         const int m = member(M, t.side_idx, k, g);
         const double4 pm = ld_xyz(w.xyz_new, m);
@@ -373,15 +371,18 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
             if (w.body[j] == bm) continue;
             const double dc = rsm + b.prm64[4 * (size_t)j + 1] + C.P.probe_r, dc2 = dc * dc;
             const double4 pjo = ld_xyz(b.xyz, j), pjn = w.group[j] ? ld_xyz(w.xyz_new, j) : pjo;
-            if (d2_of(pmo, pjo) < dc2 || d2_of(pm, pjn) < dc2) w.mark[j < m ? j : m] = 1;
+            if (d2_of(pmo, pjo) < dc2 || d2_of(pm, pjn) < dc2) {
+                const int a = j < m ? j : m;
+                if (atomicExch(&w.mark[a], 1) == 0) w.affected[a0 + atomicAdd(&q[3], 1)] = a;
+            }
         }
     }
     T.sync();
 
     // P3: cross pairs from the members' full rows (old and new geometry in
-    // one pass), then SASA of the marked atoms (old and new, in row order),
-    // both pulled from queues; boundary dihedrals and disulfides strided.
-    for (int k = warp_take(&q[1]); k < nm; k = warp_take(&q[1])) {
+    // one pass), then SASA of the affected atoms (old and new, in row
+    // order); boundary dihedrals and disulfides strided over threads.
+    for (int64_t k = wid; k < nm; k += nw) {
         int g;
         const int m = member(M, t.side_idx, k, g);
         const int gm = g + 1;
@@ -432,15 +433,11 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
         }
     }
     const double pi4 = 4.0 * 3.14159265358979323846, pi2 = 2.0 * 3.14159265358979323846;
-    const int nchunk = (a1 - a0 + 31) >> 5;
+    const int naff = q[3];
     unsigned long long nsasa = 0;
-    for (int c = warp_take(&q[2]); c < nchunk; c = warp_take(&q[2])) {
-        const int ia = a0 + 32 * c + lane;
-        unsigned todo = __ballot_sync(0xffffffffu, ia < a1 && w.mark[ia]);
-        while (todo) {
-            const int l = __ffs(todo) - 1;
-            todo &= todo - 1;
-            const int i = a0 + 32 * c + l;
+    for (int k = wid; k < naff; k += nw) {
+        {
+            const int i = w.affected[a0 + k];
             const bool moved = w.group[i] != 0;
             const double4 pio = ld_xyz(b.xyz, i), pin = moved ? ld_xyz(w.xyz_new, i) : pio;
             const double rsi = b.prm64[4 * (size_t)i + 1] + C.P.probe_r;
@@ -532,7 +529,7 @@ __device__ inline void move_finish(const MoveCtx &C, const MoveDesc &M, int s, i
                                    const Team<CL> &T) {
     const MoveScratch &w = C.w;
     const int tid = T.gtid(), nthr = T.gthreads();
-    const int a0 = C.b.atom_off[s], a1 = C.b.atom_off[s + 1];
+    const int a0 = C.b.atom_off[s];
     const int64_t nm = n_members(M);
     int drift = 0;
     for (int64_t k = tid; k < nm; k += nthr) {
@@ -548,11 +545,11 @@ __device__ inline void move_finish(const MoveCtx &C, const MoveDesc &M, int s, i
         w.body[m] = 0;
         w.dE_atom[2 * (size_t)m] = 0.0;
     }
-    for (int i = a0 + tid; i < a1; i += nthr) {
-        if (w.mark[i]) {
-            w.mark[i] = 0;
-            w.dE_atom[2 * (size_t)i + 1] = 0.0;
-        }
+    const int naff = w.queue[8 * s + 4 * parity + 3];
+    for (int k = tid; k < naff; k += nthr) {
+        const int i = w.affected[a0 + k];
+        w.mark[i] = 0;
+        w.dE_atom[2 * (size_t)i + 1] = 0.0;
     }
     if (__any_sync(0xffffffffu, drift) && (threadIdx.x & 31) == 0) atomicOr(&w.drift[2 * s + parity], 1);
 }
