@@ -208,6 +208,7 @@ int alma_move_dE(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *nl, const 
                  int prec, void *scratch, const int32_t *move_kind, const int32_t *move_a,
                  const double *move_delta, int apply, double *dE, double *dterms, void *stream);
 
+
 /* ---- device Monte Carlo ------------------------------------------------- */
 /* Proposal policy (the MC loop of generate_ensemble / run_landscape_*,
  * physics_engine.cpp:2273-2543, :2557-3270). */

@@ -1,4 +1,4 @@
-// Move ΔE entry point: one given proposal per system, one CTA per system.
+// Move ΔE entry points: one given proposal per system, one CTA per system.
 #include "move.cuh"
 
 namespace alma {
@@ -95,6 +95,7 @@ int alma_check_move_args(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *nl
     if (!b || !t || !nl || !p || !scratch || b->nsys <= 0 || !b->atom_off || !b->xyz || !b->prm || !b->prm64 ||
         !b->born)
         return alma_set_error(ALMA_EINVAL, "%s: null argument", who);
+    if (b->nsys > b->natoms + 1) return alma_set_error(ALMA_EINVAL, "%s: more systems than atoms", who);
     if (!nl->full_ptr || !nl->full_len || !nl->full_cols || !nl->half_ptr || !nl->half_len || !nl->half_cols)
         return alma_set_error(ALMA_EINVAL, "%s: neighbor list not set", who);
     if (!t->rb_off || !t->side_ptr || !t->dih_off || !t->ss_off || !t->cp_off || !t->csp_off)
@@ -129,3 +130,4 @@ extern "C" int alma_move_dE(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL 
     ALMA_LAUNCH_CHECK("alma_move_dE");
     return ALMA_OK;
 }
+
