@@ -208,6 +208,33 @@ int alma_move_dE(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *nl, const 
                  int prec, void *scratch, const int32_t *move_kind, const int32_t *move_a,
                  const double *move_delta, int apply, double *dE, double *dterms, void *stream);
 
+/* alma_move_dE without caller scratch — no counterpart in the reference.
+ *
+ * For callers that cannot allocate device memory themselves: hosts whose
+ * own allocator already owns the GPU's memory and forbids other
+ * allocations, and latency-critical sampling loops that cannot pay for
+ * cudaMalloc's implicit device-wide synchronisation.  Such callers still
+ * pass their own input and output buffers; only the scratch moves into the
+ * library.
+ *
+ * Same arguments and results as alma_move_dE, minus `scratch`.  The
+ * scratch is a static area built into the library of
+ * ALMA_NOALLOC_SCRATCH_BYTES (4 MiB), which every GPU that loads the
+ * library holds until the process exits; batches up to
+ * ALMA_NOALLOC_MAX_ATOMS atoms fit, larger ones are rejected with
+ * ALMA_EINVAL and a message.  No call allocates or frees device memory.
+ * The first call on each device looks up the area's device address (with
+ * that device current); make that first call before any stream capture.
+ * All calls on a device share the one area: calls whose kernels overlap on
+ * the GPU (two streams, two host threads) race and corrupt each other's
+ * results — serialise them.  Each call clears the part it uses before
+ * running. */
+#define ALMA_NOALLOC_SCRATCH_BYTES (4u << 20)
+#define ALMA_NOALLOC_MAX_ATOMS 16384
+size_t alma_move_noalloc_capacity_bytes(void);
+int alma_move_dE_noalloc(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *nl, const AlmaParams *p,
+                         int prec, const int32_t *move_kind, const int32_t *move_a,
+                         const double *move_delta, int apply, double *dE, double *dterms, void *stream);
 
 /* ---- device Monte Carlo ------------------------------------------------- */
 /* Proposal policy (the MC loop of generate_ensemble / run_landscape_*,

@@ -1,4 +1,6 @@
 // Move ΔE entry points: one given proposal per system, one CTA per system.
+#include <mutex>
+
 #include "move.cuh"
 
 namespace alma {
@@ -131,3 +133,53 @@ extern "C" int alma_move_dE(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL 
     return ALMA_OK;
 }
 
+// ---------------------------------------------------------------------------
+// alma_move_dE_noalloc: the same ΔE evaluation for callers that cannot
+// allocate device memory.  Its scratch is this file-scope array, which every
+// GPU that loads the library holds until the process exits.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) unsigned char g_move_scratch[ALMA_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mu;
+void *g_scratch_ptr[kMaxDevices] = {};
+}  // namespace
+
+// Device address of g_move_scratch on the current device.  In host code the
+// array's name is only a host-side handle, so the address is looked up once
+// per device (with that device current) and cached.
+static int noalloc_scratch(void **out) {
+    int dev = 0;
+    ALMA_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return alma_set_error(ALMA_EINVAL, "alma_move_dE_noalloc: device %d", dev);
+    std::lock_guard<std::mutex> lock(g_scratch_mu);
+    if (!g_scratch_ptr[dev]) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_move_scratch);
+        if (e != cudaSuccess) return alma_cuda_error(e, "alma_move_dE_noalloc: cudaGetSymbolAddress");
+        g_scratch_ptr[dev] = p;
+    }
+    *out = g_scratch_ptr[dev];
+    return ALMA_OK;
+}
+
+extern "C" size_t alma_move_noalloc_capacity_bytes(void) { return (size_t)ALMA_NOALLOC_SCRATCH_BYTES; }
+
+extern "C" int alma_move_dE_noalloc(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *nl, const AlmaParams *p,
+                                    int prec, const int32_t *move_kind, const int32_t *move_a,
+                                    const double *move_delta, int apply, double *dE, double *dterms, void *stream) {
+    if (!b || b->natoms < 0) return alma_set_error(ALMA_EINVAL, "alma_move_dE_noalloc: null batch");
+    const size_t need = carve_scratch(nullptr, nullptr, b->natoms);
+    if (b->natoms > ALMA_NOALLOC_MAX_ATOMS || need > (size_t)ALMA_NOALLOC_SCRATCH_BYTES)
+        return alma_set_error(ALMA_EINVAL,
+                              "alma_move_dE_noalloc: batch of %d atoms exceeds the built-in scratch area "
+                              "(%d atoms, %zu bytes); use alma_move_dE with caller scratch",
+                              b->natoms, ALMA_NOALLOC_MAX_ATOMS, (size_t)ALMA_NOALLOC_SCRATCH_BYTES);
+    void *scratch = nullptr;
+    int rc = noalloc_scratch(&scratch);
+    if (rc) return rc;
+    // The area keeps whatever the previous call left: start from zero.
+    ALMA_CUDA_TRY(cudaMemsetAsync(scratch, 0, need, (cudaStream_t)stream));
+    return alma_move_dE(b, t, nl, p, prec, scratch, move_kind, move_a, move_delta, apply, dE, dterms, stream);
+}
