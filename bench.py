@@ -131,8 +131,11 @@ def run_ours(args, rank, world, local):
     per_step = 1000 if args.workload == "single" else 100
     batch = DeviceBatch(systems, precision="mixed")
     from protein_physics_b200.mc import autotune
-    tuned = autotune(batch, temps, seed=777, policy=2, moveset=movesets,
-                     proposals=300 if args.workload == "single" else 30)
+    if args.config:
+        tuned = tuple(int(v) for v in args.config.split(","))
+    else:
+        tuned = autotune(batch, temps, seed=777, policy=2, moveset=movesets,
+                         proposals=300 if args.workload == "single" else 30)
     runner = MCRunner(batch, temps, seed=12345 + rank, policy=2, cur_max0=0.12, moveset=movesets,
                       cluster_size=tuned[0], threads=tuned[1])
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
@@ -377,6 +380,7 @@ def run_profile_case(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--profile", action="store_true", help="one mc_kernel launch on the single chain (for ncu)")
+    ap.add_argument("--config", default="", help="CL,NT: cluster size and CTA size instead of the autotuner")
     ap.add_argument("--cluster", type=int, default=16)
     ap.add_argument("--threads", type=int, default=512)
     ap.add_argument("--gpus", type=int, default=1)

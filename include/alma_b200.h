@@ -187,9 +187,11 @@ int alma_energy(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *nl, const A
  * Calls that share a scratch buffer must not overlap on the GPU. */
 size_t alma_move_scratch_bytes(int32_t natoms);
 int alma_move_scratch_init(void *scratch, int32_t natoms, void *stream);
-/* Cumulative work of the move / MC kernels per system (host out[4*nsys]):
- * {pair-term evaluations, hct evaluations, SASA neighbour visits, moved
- * atoms}.  Synchronises the stream. */
+/* Cumulative work of the move / MC kernels per system (host out[8*nsys]):
+ * out[4s..4s+3] = {pair-term evaluations, hct evaluations, SASA neighbour
+ * visits, moved atoms}; out[4*nsys + 4s ..] = SM cycles spent in the four
+ * ΔE phases (copy+rotate, Born+marks, pairs+SASA, reduction).
+ * Synchronises the stream. */
 int alma_move_counters(const void *scratch, int32_t natoms, int32_t nsys, unsigned long long *out,
                        void *stream);
 

@@ -23,6 +23,7 @@ static size_t carve_scratch(MoveScratch *w, char *base, int32_t natoms) {
     t.dE_atom = (double *)take(sizeof(double) * 2 * (size_t)natoms);
     t.affected = (int32_t *)take(sizeof(int32_t) * (size_t)natoms);
     t.ctr = (unsigned long long *)take(sizeof(unsigned long long) * 4 * (size_t)(natoms + 1));
+    t.phase = (unsigned long long *)take(sizeof(unsigned long long) * 4 * (size_t)(natoms + 1));
     t.queue = (int *)take(sizeof(int) * 8 * (size_t)(natoms + 1));
     t.drift = (int *)take(sizeof(int) * 2 * (size_t)(natoms + 1));
     if (w) *w = t;
@@ -73,7 +74,8 @@ using namespace alma;
 extern "C" size_t alma_move_scratch_bytes(int32_t natoms) { return carve_scratch(nullptr, nullptr, natoms); }
 
 // Cumulative work counters of the move kernels, per system: {pair-term
-// evaluations, hct evaluations, SASA neighbour visits, moved atoms}.
+// evaluations, hct evaluations, SASA neighbour visits, moved atoms}, then
+// (out[4*nsys ..]) the SM cycles rank 0 spent in the four ΔE phases.
 extern "C" int alma_move_counters(const void *scratch, int32_t natoms, int32_t nsys, unsigned long long *out,
                                   void *stream) {
     if (!scratch || !out || nsys <= 0 || nsys > natoms + 1)
@@ -82,6 +84,8 @@ extern "C" int alma_move_counters(const void *scratch, int32_t natoms, int32_t n
     carve_scratch(&w, (char *)scratch, natoms);
     ALMA_CUDA_TRY(cudaMemcpyAsync(out, w.ctr, sizeof(unsigned long long) * 4 * (size_t)nsys, cudaMemcpyDeviceToHost,
                                   (cudaStream_t)stream));
+    ALMA_CUDA_TRY(cudaMemcpyAsync(out + 4 * (size_t)nsys, w.phase, sizeof(unsigned long long) * 4 * (size_t)nsys,
+                                  cudaMemcpyDeviceToHost, (cudaStream_t)stream));
     ALMA_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
     return ALMA_OK;
 }

@@ -88,6 +88,8 @@ struct MoveScratch {
                         // region), appended during the marking pass
     unsigned long long *ctr;  // [4*nsys] cumulative work counters: pair terms,
                               // hct terms, SASA neighbour visits, moved atoms
+    unsigned long long *phase;  // [4*nsys] cumulative SM cycles of rank 0 in
+                                // the four phases of move_eval (+ finish)
     int *queue;               // [8*nsys] per proposal parity: [3] = affected
                               // atoms (other slots reserved), two parities
     int *drift;               // [2*nsys] drift flags, two proposals
@@ -305,6 +307,8 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
     const int a0 = b.atom_off[s], a1 = b.atom_off[s + 1];
     const int64_t nm = n_members(M);
     int *q = w.queue + 8 * s + 4 * parity;  // this proposal's queue counters
+    const bool timer = tid == 0;
+    long long t0 = timer ? clock64() : 0;
 
     // P1: move groups, rigid bodies and the proposed coordinates — every
     // rotation applied in order (the crankshaft's second rotation turns its
@@ -328,6 +332,11 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
         *reinterpret_cast<double4 *>(w.xyz_new + 4 * (size_t)m) = p;
     }
     T.sync();
+    if (timer) {
+        const long long t1 = clock64();
+        atomicAdd(&w.phase[4 * s + 0], (unsigned long long)(t1 - t0));
+        t0 = t1;
+    }
     // The other parity's counters and drift flag belong to the previous
     // proposal, whose last readers finished before the barrier above: clear
     // them for the next proposal.
@@ -378,6 +387,11 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
         }
     }
     T.sync();
+    if (timer) {
+        const long long t1 = clock64();
+        atomicAdd(&w.phase[4 * s + 1], (unsigned long long)(t1 - t0));
+        t0 = t1;
+    }
 
     // P3: cross pairs from the members' full rows (old and new geometry in
     // one pass), then SASA of the affected atoms (old and new, in row
@@ -501,6 +515,11 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
     }
     if (tid == 0) atomicAdd(&w.ctr[4 * s + 3], (unsigned long long)nm);
     T.sync();
+    if (timer) {
+        const long long t1 = clock64();
+        atomicAdd(&w.phase[4 * s + 2], (unsigned long long)(t1 - t0));
+        t0 = t1;
+    }
 
     // P4: deterministic sums — per-atom slots in atom order, then the CTA
     // partials in rank order.
@@ -511,6 +530,7 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
     }
     double v[4] = {c, sa, ddih, dss};
     team_sum<CL, 4>(T, v, smem_d, part + 4 * parity);
+    if (timer) atomicAdd(&w.phase[4 * s + 3], (unsigned long long)(clock64() - t0));
     MoveResult res;
     res.dcross = v[0];
     res.dsasa = v[1];

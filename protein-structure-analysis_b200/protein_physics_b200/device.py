@@ -324,12 +324,13 @@ class DeviceBatch:
                                        _ptr(dE), _ptr(dterms), self._sp()), "alma_move_dE")
         return dE, dterms
 
-    def move_counters(self):
-        """[nsys, 4] uint64: pair terms, hct terms, SASA visits, moved atoms."""
-        out = np.zeros((self.nsys, 4), np.uint64)
+    def move_counters(self, phases=False):
+        """[nsys, 4] uint64: pair terms, hct terms, SASA visits, moved atoms
+        (phases=True: also [nsys, 4] SM cycles of the four ΔE phases)."""
+        out = np.zeros((2, self.nsys, 4), np.uint64)
         _lib.check(self.L.alma_move_counters(_ptr(self.scratch), self.natoms, self.nsys, out.ctypes.data,
                                              self._sp()), "alma_move_counters")
-        return out
+        return (out[0], out[1]) if phases else out[0]
 
     # ---- host views -------------------------------------------------------------
     def coords(self, s=None):
