@@ -22,6 +22,8 @@ static size_t carve_scratch(MoveScratch *w, char *base, int32_t natoms) {
     t.born_new = (double *)take(sizeof(double) * (size_t)natoms);
     t.dE_atom = (double *)take(sizeof(double) * 2 * (size_t)natoms);
     t.affected = (int32_t *)take(sizeof(int32_t) * (size_t)natoms);
+    t.hct_part = (double *)take(sizeof(double) * MAX_WPR * (size_t)natoms);
+    t.cross_part = (double *)take(sizeof(double) * MAX_WPR * (size_t)natoms);
     t.ctr = (unsigned long long *)take(sizeof(unsigned long long) * 4 * (size_t)(natoms + 1));
     t.phase = (unsigned long long *)take(sizeof(unsigned long long) * 4 * (size_t)(natoms + 1));
     t.queue = (int *)take(sizeof(int) * 8 * (size_t)(natoms + 1));

@@ -70,6 +70,15 @@ __device__ __forceinline__ void team_sum(const Team<CL> &T, double (&v)[K], doub
 
 constexpr int MOVE_THREADS = 512;
 constexpr int MAX_ROT = 2;
+constexpr int MAX_WPR = 4;  // warps per moved-atom row, at most
+
+// Warps per moved-atom row: as many as keep every warp of the team busy,
+// a power of two <= MAX_WPR.
+__device__ __forceinline__ int rows_wpr(int64_t nrows, int nwarps) {
+    int w = 1;
+    while (w < MAX_WPR && (int64_t)(2 * w) * nrows <= (int64_t)nwarps) w *= 2;
+    return w;
+}
 
 // Global scratch for the move kernels; every array is all-zero between
 // proposals (each proposal clears what it set).
@@ -83,7 +92,9 @@ struct MoveScratch {
                         // the atom to `affected`)
     double *xyz_new;    // [natoms*4]
     double *born_new;   // [natoms]
-    double *dE_atom;    // [natoms*2]
+    double *dE_atom;    // [natoms*2] per-atom ΔE slots (SASA in [2i+1])
+    double *hct_part;   // [natoms*MAX_WPR] per-segment hct sums of moved atoms
+    double *cross_part; // [natoms*MAX_WPR] per-segment cross-pair ΔE of moved atoms
     int32_t *affected;  // [natoms] atoms whose SASA is recomputed (per-system
                         // region), appended during the marking pass
     unsigned long long *ctr;  // [4*nsys] cumulative work counters: pair terms,
@@ -287,6 +298,14 @@ __device__ __forceinline__ int member(const MoveDesc &M, const int32_t *side_idx
 // smem_d: >= 32 doubles; s_nAff: shared counter.  Leaves group/xyz_new/
 // born_new set for the members (the caller commits or discards, then calls
 // move_clear).
+// New half-list Born radius of moved atom m from its segment sums
+// (update_born, physics_engine.cpp:2043-2051), segments summed in order.
+__device__ __forceinline__ double born_new_of(const MoveScratch &w, const double *prm64, int m, int wpr) {
+    double sum = 0.0;
+    for (int sg = 0; sg < wpr; ++sg) sum += w.hct_part[(size_t)m * MAX_WPR + sg];
+    return 1.0 / fmax(1.0 / prm64[4 * (size_t)m + 1] - 0.5 * sum, 2.0);
+}
+
 // Whole-team evaluation of a decoded, non-degenerate proposal of system s.
 // parity alternates between consecutive proposals (double-buffered queue
 // counters, CTA partials and drift flag).  Leaves group/body/xyz_new/
@@ -352,14 +371,18 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
     // changes (rigid bodies differ) and is within reach before or after the
     // move changes the SASA of its lower atom only: mark that atom.
     const int wid = T.gwarp(), nw = T.gwarps();
-    for (int64_t k = wid; k < nm; k += nw) {
+    const int wpr = rows_wpr(nm, nw);
+    for (int64_t it = wid; it < nm * wpr; it += nw) {
+        const int64_t k = it / wpr;
+        const int seg = (int)(it % wpr);
         int g;
         const int m = member(M, t.side_idx, k, g);
         const double4 pm = ld_xyz(w.xyz_new, m);
         R qm, rm, em;
         prm_of<R>(b.prm, b.prm64, m, qm, rm, em);
         double sum = 0.0;
-        for (int64_t e = C.nl.half_ptr[m] + lane; e < C.nl.half_ptr[m] + C.nl.half_len[m]; e += 32) {
+        const int64_t hb = C.nl.half_ptr[m], he = hb + C.nl.half_len[m];
+        for (int64_t e = hb + 32 * seg + lane; e < he; e += 32 * wpr) {
             const int j = (int)(C.nl.half_cols[e] & ALMA_IDX_MASK);
             R qj, rj, ej;
             prm_of<R>(b.prm, b.prm64, j, qj, rj, ej);
@@ -369,13 +392,14 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
         }
         sum = warp_sum(sum);
         if (lane == 0) {
-            w.born_new[m] = 1.0 / fmax(1.0 / b.prm64[4 * (size_t)m + 1] - 0.5 * sum, 2.0);
-            atomicAdd(&w.ctr[4 * s + 1], (unsigned long long)C.nl.half_len[m]);
+            w.hct_part[(size_t)m * MAX_WPR + seg] = sum;
+            if (seg == 0) atomicAdd(&w.ctr[4 * s + 1], (unsigned long long)C.nl.half_len[m]);
         }
         const double4 pmo = ld_xyz(b.xyz, m);
         const double rsm = b.prm64[4 * (size_t)m + 1] + C.P.probe_r;
         const int bm = w.body[m];
-        for (int64_t e = C.nl.full_ptr[m] + lane; e < C.nl.full_ptr[m] + C.nl.full_len[m]; e += 32) {
+        const int64_t fb = C.nl.full_ptr[m], fe = fb + C.nl.full_len[m];
+        for (int64_t e = fb + 32 * seg + lane; e < fe; e += 32 * wpr) {
             const int j = (int)(C.nl.full_cols[e] & ALMA_IDX_MASK);
             if (w.body[j] == bm) continue;
             const double dc = rsm + b.prm64[4 * (size_t)j + 1] + C.P.probe_r, dc2 = dc * dc;
@@ -396,18 +420,23 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
     // P3: cross pairs from the members' full rows (old and new geometry in
     // one pass), then SASA of the affected atoms (old and new, in row
     // order); boundary dihedrals and disulfides strided over threads.
-    for (int64_t k = wid; k < nm; k += nw) {
+    for (int64_t it = wid; it < nm * wpr; it += nw) {
+        const int64_t k = it / wpr;
+        const int seg = (int)(it % wpr);
         int g;
         const int m = member(M, t.side_idx, k, g);
         const int gm = g + 1;
         const double4 pmo = ld_xyz(b.xyz, m), pmn = ld_xyz(w.xyz_new, m);
         R qm, rm, em;
         prm_of<R>(b.prm, b.prm64, m, qm, rm, em);
-        const R amo = (R)b.born[m], amn = (R)w.born_new[m];
+        const double bn = born_new_of(w, b.prm64, m, wpr);
+        if (seg == 0 && lane == 0) w.born_new[m] = bn;
+        const R amo = (R)b.born[m], amn = (R)bn;
         const double rm64 = b.prm64[4 * (size_t)m + 1], em64 = b.prm64[4 * (size_t)m + 2];
         double acc = 0.0;
         int npair = 0;
-        for (int64_t e = C.nl.full_ptr[m] + lane; e < C.nl.full_ptr[m] + C.nl.full_len[m]; e += 32) {
+        const int64_t fb = C.nl.full_ptr[m], fe = fb + C.nl.full_len[m];
+        for (int64_t e = fb + 32 * seg + lane; e < fe; e += 32 * wpr) {
             const uint32_t ent = C.nl.full_cols[e];
             if (ent & ALMA_EXCL_BIT) continue;
             const int j = (int)(ent & ALMA_IDX_MASK);
@@ -423,7 +452,7 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
             prm_of<R>(b.prm, b.prm64, j, qj, rj, ej);
             const R qp = qm * qj, sig = rm + rj, ep = em * ej;
             const R ajo = (R)b.born[j];
-            const R ajn = gj ? (R)w.born_new[j] : ajo;
+            const R ajn = gj ? (R)born_new_of(w, b.prm64, j, wpr) : ajo;
             if (ino && inn) {
                 // FP64 sigma/epsilon only for contacts inside sigma (steep LJ)
                 double sig64 = (double)sig, eps64 = (double)ep;
@@ -442,7 +471,7 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
         acc = warp_sum(acc);
         npair = __reduce_add_sync(0xffffffffu, npair);
         if (lane == 0) {
-            w.dE_atom[2 * (size_t)m] = acc;
+            w.cross_part[(size_t)m * MAX_WPR + seg] = acc;
             atomicAdd(&w.ctr[4 * s + 0], (unsigned long long)npair);
         }
     }
@@ -524,10 +553,12 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
     // P4: deterministic sums — per-atom slots in atom order, then the CTA
     // partials in rank order.
     double c = 0.0, sa = 0.0;
-    for (int i = a0 + tid; i < a1; i += nthr) {
-        c += w.dE_atom[2 * (size_t)i];
-        sa += w.dE_atom[2 * (size_t)i + 1];
+    for (int64_t k = tid; k < nm; k += nthr) {
+        int g;
+        const int m = member(M, t.side_idx, k, g);
+        for (int sg = 0; sg < wpr; ++sg) c += w.cross_part[(size_t)m * MAX_WPR + sg];
     }
+    for (int i = a0 + tid; i < a1; i += nthr) sa += w.dE_atom[2 * (size_t)i + 1];
     double v[4] = {c, sa, ddih, dss};
     team_sum<CL, 4>(T, v, smem_d, part + 4 * parity);
     if (timer) atomicAdd(&w.phase[4 * s + 3], (unsigned long long)(clock64() - t0));
@@ -563,7 +594,6 @@ __device__ inline void move_finish(const MoveCtx &C, const MoveDesc &M, int s, i
         }
         w.group[m] = 0;
         w.body[m] = 0;
-        w.dE_atom[2 * (size_t)m] = 0.0;
     }
     const int naff = w.queue[8 * s + 4 * parity + 3];
     for (int k = tid; k < naff; k += nthr) {
