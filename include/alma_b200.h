@@ -114,10 +114,15 @@ typedef struct {
  * cols[ptr[i] .. ptr[i]+len[i]).  Each system owns the region
  * [base[s], base[s+1]) of the column arrays, so one system can be rebuilt
  * without touching the others.  Column entries carry the exclusion flag in
- * bit 31 (atom index = entry & 0x7fffffff).  need[2*s+0/1] receives the
- * full/half entry counts of system s at its last build; when a count
- * exceeds the region, the rows of that system are not written and
- * ALMA_ST_NL_OVERFLOW is raised. */
+ * bit 31 (atom index = entry & 0x7fffffff).  Optional short rows (sfull,
+ * shalf; set sfull_cols = NULL to skip them) are the order-preserving
+ * sub-rows of the pairs within SASA reach plus the skin at build time
+ * (r < R*_i + R*_j + 2 probe + skin): while every atom stays within half the
+ * skin of its build position no other pair can come within SASA reach, so
+ * the move kernels walk these instead.  need[4*s + k] receives the entry
+ * counts (k: full, half, short full, short half) of system s at its last
+ * build; when a count exceeds its region, the rows of that system are not
+ * written and ALMA_ST_NL_OVERFLOW is raised. */
 typedef struct {
     int64_t *full_ptr;        /* [natoms] */
     int32_t *full_len;        /* [natoms] */
@@ -128,7 +133,15 @@ typedef struct {
     uint32_t *half_cols;      /* [half_base[nsys]] */
     const int64_t *half_base; /* [nsys+1] */
     double *ref_xyz;          /* [natoms*4] positions at the last build     */
-    int64_t *need;            /* [nsys*2]                                   */
+    int64_t *need;            /* [nsys*4]                                   */
+    int64_t *sfull_ptr;       /* [natoms] short rows (optional)             */
+    int32_t *sfull_len;
+    uint32_t *sfull_cols;
+    const int64_t *sfull_base;
+    int64_t *shalf_ptr;
+    int32_t *shalf_len;
+    uint32_t *shalf_cols;
+    const int64_t *shalf_base;
 } AlmaNL;
 
 /* ---- library ------------------------------------------------------------ */
@@ -158,12 +171,13 @@ int alma_topo_sides_compact(int32_t n, const int64_t *adj_ptr, const int32_t *ad
 
 /* ---- device kernels ------------------------------------------------------ */
 /* Neighbor list for every system of the batch (replaces
- * NeighborList::build, physics_engine.cpp:293-342).  sys_mask: device
+ * NeighborList::build, physics_engine.cpp:293-342).  p: probe radius and
+ * skin of the short rows (NULL: reference preset).  sys_mask: device
  * uint8[nsys]; only systems with a nonzero entry are rebuilt (NULL: all).
  * workspace: device scratch of alma_nl_workspace_bytes(nsys, natoms,
  * max_cells) bytes. */
-int alma_nl_build(const AlmaBatch *b, const AlmaTopo *t, AlmaNL *nl, const uint8_t *sys_mask,
-                  void *workspace, int64_t max_cells, void *stream);
+int alma_nl_build(const AlmaBatch *b, const AlmaTopo *t, AlmaNL *nl, const AlmaParams *p,
+                  const uint8_t *sys_mask, void *workspace, int64_t max_cells, void *stream);
 
 /* Effective Born radii over the full rows (replaces born_radii,
  * physics_engine.cpp:2024-2039, and born_sum/born_finalize kernels,

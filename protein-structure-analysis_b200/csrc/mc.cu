@@ -24,7 +24,11 @@
 //          for a rebuild (NeighborList::needs_rebuild, :345-351); the CTA
 //          stops at the start of its next step, the host rebuilds the
 //          list, the Born radii and the energy for flagged systems only
-//          (alma_mc_after_rebuild) and relaunches.
+//          (alma_mc_after_rebuild) and relaunches.  A launch that finds
+//          any atom of a system already beyond the half skin (coordinates
+//          changed since the list was built) flags it before its first
+//          proposal, as the reference's check at the top of every step
+//          would.
 #include "move.cuh"
 
 namespace alma {
@@ -58,6 +62,9 @@ __global__ void __launch_bounds__(NT, 512 / NT) mc_kernel(MoveCtx C, MCConfigDev
     const Team<CL> T;
     const int s = blockIdx.x / CL;
     if (threadIdx.x == 0) S = states[s];
+    __syncthreads();
+    const bool rows_ok = system_within_skin(C, s);
+    if (threadIdx.x == 0 && !rows_ok && C.nl.ref_xyz && S.step < step_limit) S.need_rebuild = 1;
     __syncthreads();
     const int nrb = C.t.rb_off[s + 1] - C.t.rb_off[s];
     const int ncp = C.t.cp_off[s + 1] - C.t.cp_off[s];
@@ -125,7 +132,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) mc_kernel(MoveCtx C, MCConfigDev
             continue;
         }
         const int parity = S.parity & 1;
-        const MoveResult r = move_eval<R, CL>(C, M, s, sm, part, parity, T);
+        const MoveResult r = move_eval<R, CL>(C, M, s, sm, part, parity, rows_ok, T);
         if (threadIdx.x == 0) accept = (r.dE < 0.0) || (u[3] < exp(-r.dE / S.temperature));
         __syncthreads();
         const int acc = accept;

@@ -58,7 +58,8 @@ __global__ void __launch_bounds__(MOVE_THREADS) move_dE_kernel(MoveCtx C, const 
         }
         return;
     }
-    const MoveResult r = move_eval<R, 1>(C, M, s, sm, part, 0, T);
+    const bool rows_ok = system_within_skin(C, s);
+    const MoveResult r = move_eval<R, 1>(C, M, s, sm, part, 0, rows_ok, T);
     if (threadIdx.x == 0) {
         dE[s] = r.dE;
         dterms[4 * (size_t)s + 0] = r.dcross;

@@ -101,7 +101,8 @@ struct MoveScratch {
                               // hct terms, SASA neighbour visits, moved atoms
     unsigned long long *phase;  // [4*nsys] cumulative SM cycles of rank 0 in
                                 // the four phases of move_eval (+ finish)
-    int *queue;               // [8*nsys] per proposal parity: [3] = affected
+    int *queue;               // [8*nsys] per proposal parity: [2] = a trial
+                              // atom is beyond half the skin, [3] = affected
                               // atoms (other slots reserved), two parities
     int *drift;               // [2*nsys] drift flags, two proposals
 };
@@ -278,6 +279,21 @@ struct MoveCtx {
     MoveScratch w;
 };
 
+// True when every atom of system s is within half the skin of its position
+// at the last list build (the condition under which the lists are valid and
+// the short rows may stand in for the full ones).  Every thread of the CTA
+// gets the result; the CTA scans the whole system, so every CTA of a team
+// computes the same answer.
+__device__ __forceinline__ bool system_within_skin(const MoveCtx &C, int s) {
+    bool far = false;
+    if (C.nl.ref_xyz) {
+        const int a0 = C.b.atom_off[s], a1 = C.b.atom_off[s + 1];
+        for (int i = a0 + (int)threadIdx.x; i < a1 && !far; i += (int)blockDim.x)
+            far = d2_of(ld_xyz(C.b.xyz, i), ld_xyz(C.nl.ref_xyz, i)) > C.P.half_skin2;
+    }
+    return !__syncthreads_or(far) && C.nl.ref_xyz != nullptr;
+}
+
 // Number of member atoms and the k-th one (concatenated member lists).
 __device__ __forceinline__ int64_t n_members(const MoveDesc &M) {
     int64_t n = 0;
@@ -315,9 +331,16 @@ __device__ __forceinline__ double born_new_of(const MoveScratch &w, const double
 // proposal copy, (2) after the member Born radii and SASA marks (the marking
 // pass also builds the affected-atom list), (3) after the cross-pair and
 // SASA slots, (4) the CTA-partials exchange of team_sum.
+//
+// rows_ok: every committed atom of system s is within half the skin of its
+// position at the last list build.  Then, when every trial position is too,
+// the SASA reach tests walk the short rows (the pairs within SASA reach plus
+// the skin at build time, in row order): no pair outside them can come
+// within reach, and the SASA recurrence only consumes pairs within reach, so
+// the result is the same bit for bit.
 template <typename R, int CL>
 __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, double *smem_d, double *part,
-                                int parity, const Team<CL> &T) {
+                                int parity, bool rows_ok, const Team<CL> &T) {
     const AlmaBatch &b = C.b;
     const AlmaTopo &t = C.t;
     const MoveScratch &w = C.w;
@@ -328,6 +351,7 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
     int *q = w.queue + 8 * s + 4 * parity;  // this proposal's queue counters
     const bool timer = tid == 0;
     long long t0 = timer ? clock64() : 0;
+    rows_ok = rows_ok && C.nl.sfull_cols != nullptr && C.nl.ref_xyz != nullptr;
 
     // P1: move groups, rigid bodies and the proposed coordinates — every
     // rotation applied in order (the crankshaft's second rotation turns its
@@ -349,8 +373,10 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
         w.group[m] = (int8_t)(g + 1);
         w.body[m] = (int8_t)body;
         *reinterpret_cast<double4 *>(w.xyz_new + 4 * (size_t)m) = p;
+        if (rows_ok && d2_of(p, ld_xyz(C.nl.ref_xyz, m)) > C.P.half_skin2) q[2] = 1;
     }
     T.sync();
+    const bool short_rows = rows_ok && q[2] == 0;
     if (timer) {
         const long long t1 = clock64();
         atomicAdd(&w.phase[4 * s + 0], (unsigned long long)(t1 - t0));
@@ -398,9 +424,11 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
         const double4 pmo = ld_xyz(b.xyz, m);
         const double rsm = b.prm64[4 * (size_t)m + 1] + C.P.probe_r;
         const int bm = w.body[m];
-        const int64_t fb = C.nl.full_ptr[m], fe = fb + C.nl.full_len[m];
+        const uint32_t *rc = short_rows ? C.nl.sfull_cols : C.nl.full_cols;
+        const int64_t fb = short_rows ? C.nl.sfull_ptr[m] : C.nl.full_ptr[m];
+        const int64_t fe = fb + (short_rows ? C.nl.sfull_len[m] : C.nl.full_len[m]);
         for (int64_t e = fb + 32 * seg + lane; e < fe; e += 32 * wpr) {
-            const int j = (int)(C.nl.full_cols[e] & ALMA_IDX_MASK);
+            const int j = (int)(rc[e] & ALMA_IDX_MASK);
             if (w.body[j] == bm) continue;
             const double dc = rsm + b.prm64[4 * (size_t)j + 1] + C.P.probe_r, dc2 = dc * dc;
             const double4 pjo = ld_xyz(b.xyz, j), pjn = w.group[j] ? ld_xyz(w.xyz_new, j) : pjo;
@@ -486,13 +514,15 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
             const double rsi = b.prm64[4 * (size_t)i + 1] + C.P.probe_r;
             const double cs = pi2 * rsi * rsi;
             double sao = pi4 * rsi * rsi, san = sao;
-            const int64_t beg = C.nl.half_ptr[i], end = C.nl.half_ptr[i] + C.nl.half_len[i];
+            const uint32_t *rc = short_rows ? C.nl.shalf_cols : C.nl.half_cols;
+            const int64_t beg = short_rows ? C.nl.shalf_ptr[i] : C.nl.half_ptr[i];
+            const int64_t end = beg + (short_rows ? C.nl.shalf_len[i] : C.nl.half_len[i]);
             for (int64_t e0 = beg; e0 < end; e0 += 32) {
                 const int64_t e = e0 + lane;
                 double co = 0.0, cn = 0.0;
                 bool ho = false, hn = false;
                 if (e < end) {
-                    const int j = (int)(C.nl.half_cols[e] & ALMA_IDX_MASK);
+                    const int j = (int)(rc[e] & ALMA_IDX_MASK);
                     const double rsj = b.prm64[4 * (size_t)j + 1] + C.P.probe_r;
                     const double dc = rsi + rsj;
                     const double4 pjo = ld_xyz(b.xyz, j);

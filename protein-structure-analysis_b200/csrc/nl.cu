@@ -43,6 +43,8 @@ struct NLWork {
     int32_t *cell_atoms;  // [natoms]
     int32_t *full_cnt;    // [natoms]
     int32_t *half_cnt;    // [natoms]
+    int32_t *sfull_cnt;   // [natoms]
+    int32_t *shalf_cnt;   // [natoms]
     int64_t *tile_sums;   // scan scratch
     int64_t *total_cells; // [1]
     int32_t *ok;          // [1] 1 when the grid fit
@@ -69,6 +71,8 @@ static size_t carve(NLWork *w, char *base, int32_t nsys, int32_t natoms, int64_t
     t.cell_atoms = (int32_t *)take(sizeof(int32_t) * (size_t)natoms);
     t.full_cnt = (int32_t *)take(sizeof(int32_t) * (size_t)natoms);
     t.half_cnt = (int32_t *)take(sizeof(int32_t) * (size_t)natoms);
+    t.sfull_cnt = (int32_t *)take(sizeof(int32_t) * (size_t)natoms);
+    t.shalf_cnt = (int32_t *)take(sizeof(int32_t) * (size_t)natoms);
     t.tile_sums = (int64_t *)take(sizeof(int64_t) * (size_t)ntiles);
     t.total_cells = (int64_t *)take(sizeof(int64_t));
     t.ok = (int32_t *)take(sizeof(int32_t));
@@ -227,20 +231,25 @@ __device__ __forceinline__ bool excluded(const int64_t *__restrict__ excl_ptr, c
 }
 
 // One CTA per system: row pointers inside the system's region, overflow
-// check.  PASS 0 full rows, PASS 1 half rows.
+// check, for the four row kinds (full, half, short full, short half; the
+// short ones only when the list carries them).
 __global__ void nl_rowscan_kernel(const int32_t *__restrict__ atom_off, const uint8_t *__restrict__ mask,
                                   const int32_t *__restrict__ full_cnt, const int32_t *__restrict__ half_cnt,
+                                  const int32_t *__restrict__ sfull_cnt, const int32_t *__restrict__ shalf_cnt,
                                   AlmaNL nl, int32_t *__restrict__ sys_ok, uint32_t *__restrict__ status) {
     __shared__ int64_t sm[33];
     const int s = blockIdx.x;
     if (mask && !mask[s]) return;
     const int a0 = atom_off[s], a1 = atom_off[s + 1];
-    for (int pass = 0; pass < 2; ++pass) {
-        const int32_t *cnt = pass == 0 ? full_cnt : half_cnt;
-        int64_t *ptr = pass == 0 ? nl.full_ptr : nl.half_ptr;
-        int32_t *len = pass == 0 ? nl.full_len : nl.half_len;
-        const int64_t base = pass == 0 ? nl.full_base[s] : nl.half_base[s];
-        const int64_t cap = (pass == 0 ? nl.full_base[s + 1] : nl.half_base[s + 1]) - base;
+    const int nkind = nl.sfull_cols ? 4 : 2;
+    int fits = 1;
+    for (int kind = 0; kind < nkind; ++kind) {
+        const int32_t *cnt = kind == 0 ? full_cnt : kind == 1 ? half_cnt : kind == 2 ? sfull_cnt : shalf_cnt;
+        int64_t *ptr = kind == 0 ? nl.full_ptr : kind == 1 ? nl.half_ptr : kind == 2 ? nl.sfull_ptr : nl.shalf_ptr;
+        int32_t *len = kind == 0 ? nl.full_len : kind == 1 ? nl.half_len : kind == 2 ? nl.sfull_len : nl.shalf_len;
+        const int64_t *basev = kind == 0 ? nl.full_base : kind == 1 ? nl.half_base : kind == 2 ? nl.sfull_base
+                                                                                                : nl.shalf_base;
+        const int64_t base = basev[s], cap = basev[s + 1] - base;
         int64_t carry = 0;
         for (int b0 = a0; b0 < a1; b0 += blockDim.x) {
             const int i = b0 + threadIdx.x;
@@ -254,15 +263,14 @@ __global__ void nl_rowscan_kernel(const int32_t *__restrict__ atom_off, const ui
             carry += tot;
         }
         if (threadIdx.x == 0) {
-            nl.need[2 * s + pass] = carry;
-            if (carry > cap) {
-                sys_ok[s] = 0;
-                set_status(status, ALMA_ST_NL_OVERFLOW);
-            } else if (pass == 0) {
-                sys_ok[s] = 1;
-            }
+            nl.need[4 * s + kind] = carry;
+            if (carry > cap) fits = 0;
         }
         __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        sys_ok[s] = fits;
+        if (!fits) set_status(status, ALMA_ST_NL_OVERFLOW);
     }
 }
 
@@ -273,6 +281,8 @@ __global__ void nl_rows_kernel(const int32_t *__restrict__ atom_off, int nsys, i
                                const int32_t *__restrict__ ok, const int32_t *__restrict__ cell_of,
                                const int64_t *__restrict__ cell_start, const int32_t *__restrict__ cell_atoms,
                                int32_t *__restrict__ full_cnt, int32_t *__restrict__ half_cnt,
+                               int32_t *__restrict__ sfull_cnt, int32_t *__restrict__ shalf_cnt,
+                               const double *__restrict__ prm64, double reach_pad,
                                const int64_t *__restrict__ excl_ptr, const int32_t *__restrict__ excl_cols,
                                AlmaNL nl, const int32_t *__restrict__ sys_ok) {
     const int warps_per_block = blockDim.x >> 5;
@@ -286,13 +296,19 @@ __global__ void nl_rows_kernel(const int32_t *__restrict__ atom_off, int nsys, i
     const int c = cell_of[i];
     const int cx = c % g.nx, cy = (c / g.nx) % g.ny, cz = c / (g.nx * g.ny);
     const double4 pi = ld_xyz(xyz, i);
-    int64_t fo = 0, ho = 0;
+    const bool shorts = nl.sfull_cols != nullptr;
+    const double ri_pad = shorts ? prm64[4 * (size_t)i + 1] + reach_pad : 0.0;
+    int64_t fo = 0, ho = 0, sfo = 0, sho = 0;
     if (PASS == 1) {
         fo = nl.full_ptr[i];
         ho = nl.half_ptr[i];
+        if (shorts) {
+            sfo = nl.sfull_ptr[i];
+            sho = nl.shalf_ptr[i];
+        }
         if (lane == 0) *reinterpret_cast<double4 *>(nl.ref_xyz + 4 * (size_t)i) = pi;
     }
-    int nfull = 0, nhalf = 0;
+    int nfull = 0, nhalf = 0, nsfull = 0, nshalf = 0;
     for (int dz = -1; dz <= 1; ++dz) {
         const int cz2 = cz + dz;
         if (cz2 < 0 || cz2 >= g.nz) continue;
@@ -307,21 +323,34 @@ __global__ void nl_rows_kernel(const int32_t *__restrict__ atom_off, int nsys, i
                 for (int64_t k0 = beg; k0 < end; k0 += 32) {
                     const int64_t k = k0 + lane;
                     int j = -1;
-                    bool in = false;
+                    bool in = false, sh = false;
                     if (k < end) {
                         j = cell_atoms[k];
-                        in = (j != i) && d2_of(pi, ld_xyz(xyz, j)) < rcut2;
+                        const double r2 = d2_of(pi, ld_xyz(xyz, j));
+                        in = (j != i) && r2 < rcut2;
+                        if (in && shorts) {
+                            const double reach = ri_pad + prm64[4 * (size_t)j + 1];
+                            sh = r2 < reach * reach;
+                        }
                     }
                     const unsigned mf = __ballot_sync(0xffffffffu, in);
                     const unsigned mh = __ballot_sync(0xffffffffu, in && j > i);
+                    const unsigned msf = __ballot_sync(0xffffffffu, sh);
+                    const unsigned msh = __ballot_sync(0xffffffffu, sh && j > i);
                     if (PASS == 1 && in) {
                         const unsigned lt = (1u << lane) - 1u;
                         const uint32_t e = (uint32_t)j | (excluded(excl_ptr, excl_cols, i, j) ? ALMA_EXCL_BIT : 0u);
                         nl.full_cols[fo + nfull + __popc(mf & lt)] = e;
                         if (j > i) nl.half_cols[ho + nhalf + __popc(mh & lt)] = e;
+                        if (sh) {
+                            nl.sfull_cols[sfo + nsfull + __popc(msf & lt)] = e;
+                            if (j > i) nl.shalf_cols[sho + nshalf + __popc(msh & lt)] = e;
+                        }
                     }
                     nfull += __popc(mf);
                     nhalf += __popc(mh);
+                    nsfull += __popc(msf);
+                    nshalf += __popc(msh);
                 }
             }
         }
@@ -329,6 +358,8 @@ __global__ void nl_rows_kernel(const int32_t *__restrict__ atom_off, int nsys, i
     if (PASS == 0 && lane == 0) {
         full_cnt[i] = nfull;
         half_cnt[i] = nhalf;
+        sfull_cnt[i] = nsfull;
+        shalf_cnt[i] = nshalf;
     }
 }
 
@@ -340,13 +371,25 @@ extern "C" size_t alma_nl_workspace_bytes(int32_t nsys, int32_t natoms, int64_t 
     return carve(nullptr, nullptr, nsys, natoms, max_cells);
 }
 
-extern "C" int alma_nl_build(const AlmaBatch *b, const AlmaTopo *t, AlmaNL *nl, const uint8_t *sys_mask,
-                             void *workspace, int64_t max_cells, void *stream) {
+extern "C" int alma_nl_build(const AlmaBatch *b, const AlmaTopo *t, AlmaNL *nl, const AlmaParams *p,
+                             const uint8_t *sys_mask, void *workspace, int64_t max_cells, void *stream) {
     if (!b || !nl || !workspace || b->nsys <= 0 || b->natoms < 0 || max_cells <= 0)
         return alma_set_error(ALMA_EINVAL, "alma_nl_build: bad arguments");
     if (!nl->full_ptr || !nl->full_len || !nl->half_ptr || !nl->half_len || !nl->full_base || !nl->half_base ||
         !nl->ref_xyz || !nl->need || !b->xyz || !b->atom_off)
         return alma_set_error(ALMA_EINVAL, "alma_nl_build: null buffer");
+    if (nl->sfull_cols && (!nl->sfull_ptr || !nl->sfull_len || !nl->sfull_base || !nl->shalf_ptr || !nl->shalf_len ||
+                           !nl->shalf_cols || !nl->shalf_base || !b->prm64))
+        return alma_set_error(ALMA_EINVAL, "alma_nl_build: incomplete short rows");
+    AlmaParams pref;
+    if (!p) {
+        alma_params_reference(&pref);
+        p = &pref;
+    }
+    // SASA reach R*_i + R*_j + 2 probe, plus the skin (both atoms may each
+    // drift half the skin before a rebuild).
+    // A 1e-6 A margin keeps rounding at the boundary on the safe side.
+    const double reach_pad = 2.0 * p->probe_r + 2.0 * sqrt(p->half_skin2) + 1e-6;
     cudaStream_t st = (cudaStream_t)stream;
     const int nsys = b->nsys, natoms = b->natoms;
     NLWork w;
@@ -370,12 +413,13 @@ extern "C" int alma_nl_build(const AlmaBatch *b, const AlmaTopo *t, AlmaNL *nl, 
     const int64_t *ep = t ? t->excl_ptr : nullptr;
     const int32_t *ec = t ? t->excl_cols : nullptr;
     nl_rows_kernel<0><<<rb, wpb * 32, 0, st>>>(b->atom_off, nsys, natoms, sys_mask, b->xyz, rcut2, w.grid, w.ok,
-                                               w.cell_of, w.cell_start, w.cell_atoms, w.full_cnt, w.half_cnt, ep, ec,
-                                               *nl, w.sys_ok);
-    nl_rowscan_kernel<<<nsys, 1024, 0, st>>>(b->atom_off, sys_mask, w.full_cnt, w.half_cnt, *nl, w.sys_ok, b->status);
+                                               w.cell_of, w.cell_start, w.cell_atoms, w.full_cnt, w.half_cnt,
+                                               w.sfull_cnt, w.shalf_cnt, b->prm64, reach_pad, ep, ec, *nl, w.sys_ok);
+    nl_rowscan_kernel<<<nsys, 1024, 0, st>>>(b->atom_off, sys_mask, w.full_cnt, w.half_cnt, w.sfull_cnt, w.shalf_cnt,
+                                             *nl, w.sys_ok, b->status);
     nl_rows_kernel<1><<<rb, wpb * 32, 0, st>>>(b->atom_off, nsys, natoms, sys_mask, b->xyz, rcut2, w.grid, w.ok,
-                                               w.cell_of, w.cell_start, w.cell_atoms, w.full_cnt, w.half_cnt, ep, ec,
-                                               *nl, w.sys_ok);
+                                               w.cell_of, w.cell_start, w.cell_atoms, w.full_cnt, w.half_cnt,
+                                               w.sfull_cnt, w.shalf_cnt, b->prm64, reach_pad, ep, ec, *nl, w.sys_ok);
     ALMA_LAUNCH_CHECK_N("alma_nl_build", 11);
     return ALMA_OK;
 }

@@ -59,7 +59,9 @@ class AlmaTopo(C.Structure):
 class AlmaNL(C.Structure):
     _fields_ = [("full_ptr", _p), ("full_len", _p), ("full_cols", _p), ("full_base", _p),
                 ("half_ptr", _p), ("half_len", _p), ("half_cols", _p), ("half_base", _p),
-                ("ref_xyz", _p), ("need", _p)]
+                ("ref_xyz", _p), ("need", _p),
+                ("sfull_ptr", _p), ("sfull_len", _p), ("sfull_cols", _p), ("sfull_base", _p),
+                ("shalf_ptr", _p), ("shalf_len", _p), ("shalf_cols", _p), ("shalf_base", _p)]
 
 
 class AlmaMCConfig(C.Structure):
@@ -107,7 +109,7 @@ def lib():
     L.alma_move_scratch_bytes.argtypes = [_i32]
     L.alma_topo_sides.argtypes = [_i32, _p, _p, _i32, _p, _p, _p, _i64]
     L.alma_topo_sides_compact.argtypes = [_i32, _p, _p, _i32, _p, _p, _p, _p, _p, _p, _i64]
-    L.alma_nl_build.argtypes = [_p, _p, _p, _p, _p, _i64, _p]
+    L.alma_nl_build.argtypes = [_p, _p, _p, _p, _p, _p, _i64, _p]
     L.alma_born_radii.argtypes = [_p, _p, _p, C.c_int, _p, _p]
     L.alma_energy.argtypes = [_p, _p, _p, _p, C.c_int, _p, _p, _p, _p]
     L.alma_mc_run.argtypes = [_p, _p, _p, _p, C.c_int, _p, _p, _p, _i64, _p]

@@ -59,6 +59,7 @@ class DeviceBatch:
 
     NL_FULL_PER_ATOM = 640   # first-build capacity guesses (entries / atom)
     NL_HALF_PER_ATOM = 330
+    NL_SHORT_PER_ATOM = 200
 
     def __init__(self, systems, precision="mixed", stream=None):
         _require_cuda()
@@ -196,15 +197,16 @@ class DeviceBatch:
     def _alloc_nl(self, need):
         sizes = np.diff(self.atom_off_h).astype(np.int64)
         if need is None:
-            full = sizes * self.NL_FULL_PER_ATOM + 64
-            half = sizes * self.NL_HALF_PER_ATOM + 64
+            caps = [sizes * self.NL_FULL_PER_ATOM + 64, sizes * self.NL_HALF_PER_ATOM + 64,
+                    sizes * self.NL_SHORT_PER_ATOM + 64, sizes * (self.NL_SHORT_PER_ATOM // 2) + 64]
         else:
-            full = (need[:, 0] * 5) // 4 + 4096
-            half = (need[:, 1] * 5) // 4 + 4096
-        fb = np.zeros(self.nsys + 1, np.int64)
-        hb = np.zeros(self.nsys + 1, np.int64)
-        fb[1:] = np.cumsum(full)
-        hb[1:] = np.cumsum(half)
+            caps = [(need[:, k] * 5) // 4 + 4096 for k in range(4)]
+        bases = []
+        for c in caps:
+            bb = np.zeros(self.nsys + 1, np.int64)
+            bb[1:] = np.cumsum(c)
+            bases.append(bb)
+        fb, hb, sfb, shb = bases
         n = max(self.natoms, 1)
         self.full_base = _t(fb, torch.int64)
         self.half_base = _t(hb, torch.int64)
@@ -214,8 +216,16 @@ class DeviceBatch:
         self.half_len = torch.zeros(n, dtype=torch.int32, device=_DEV)
         self.full_cols = torch.zeros(int(fb[-1]) + 1, dtype=torch.int32, device=_DEV)
         self.half_cols = torch.zeros(int(hb[-1]) + 1, dtype=torch.int32, device=_DEV)
+        self.sfull_base = _t(sfb, torch.int64)
+        self.shalf_base = _t(shb, torch.int64)
+        self.sfull_ptr = torch.zeros(n, dtype=torch.int64, device=_DEV)
+        self.sfull_len = torch.zeros(n, dtype=torch.int32, device=_DEV)
+        self.shalf_ptr = torch.zeros(n, dtype=torch.int64, device=_DEV)
+        self.shalf_len = torch.zeros(n, dtype=torch.int32, device=_DEV)
+        self.sfull_cols = torch.zeros(int(sfb[-1]) + 1, dtype=torch.int32, device=_DEV)
+        self.shalf_cols = torch.zeros(int(shb[-1]) + 1, dtype=torch.int32, device=_DEV)
         self.ref_xyz = torch.zeros((n, 4), dtype=torch.float64, device=_DEV)
-        self.need = torch.zeros((self.nsys, 2), dtype=torch.int64, device=_DEV)
+        self.need = torch.zeros((self.nsys, 4), dtype=torch.int64, device=_DEV)
         self.max_cells = int(max(4096, 8 * self.natoms + 4096 * self.nsys))
         self.nl_ws = torch.zeros(self.L.alma_nl_workspace_bytes(self.nsys, self.natoms, self.max_cells),
                                  dtype=torch.uint8, device=_DEV)
@@ -228,6 +238,10 @@ class DeviceBatch:
         nl.half_ptr, nl.half_len, nl.half_cols, nl.half_base = (_ptr(self.half_ptr), _ptr(self.half_len),
                                                                 _ptr(self.half_cols), _ptr(self.half_base))
         nl.ref_xyz, nl.need = _ptr(self.ref_xyz), _ptr(self.need)
+        nl.sfull_ptr, nl.sfull_len, nl.sfull_cols, nl.sfull_base = (_ptr(self.sfull_ptr), _ptr(self.sfull_len),
+                                                                    _ptr(self.sfull_cols), _ptr(self.sfull_base))
+        nl.shalf_ptr, nl.shalf_len, nl.shalf_cols, nl.shalf_base = (_ptr(self.shalf_ptr), _ptr(self.shalf_len),
+                                                                    _ptr(self.shalf_cols), _ptr(self.shalf_base))
         return nl
 
     def _sp(self):
@@ -241,7 +255,8 @@ class DeviceBatch:
         for attempt in range(3):
             b, t, nl = self.batch_s, self.topo_s, self.nl_s
             rc = self.L.alma_nl_build(C.byref(b), C.byref(t) if self.use_topo else None, C.byref(nl),
-                                      _ptr(sys_mask) if sys_mask is not None else None, _ptr(self.nl_ws),
+                                      C.byref(self.params), _ptr(sys_mask) if sys_mask is not None else None,
+                                      _ptr(self.nl_ws),
                                       self.max_cells, self._sp())
             _lib.check(rc, "alma_nl_build")
             if not check:
@@ -339,12 +354,19 @@ class DeviceBatch:
             return x
         return x[self.atom_off_h[s]:self.atom_off_h[s + 1]]
 
-    def nl_host(self, s=0, half=True):
-        """(row_ptr, cols, excl_flags) of system s with local indices."""
+    def nl_host(self, s=0, half=True, short=False):
+        """(row_ptr, cols, excl_flags) of system s with local indices
+        (short=True: the SASA-reach sub-rows)."""
         a0, a1 = int(self.atom_off_h[s]), int(self.atom_off_h[s + 1])
-        ptr = (self.half_ptr if half else self.full_ptr)[a0:a1].cpu().numpy()
-        ln = (self.half_len if half else self.full_len)[a0:a1].cpu().numpy()
-        cols_all = (self.half_cols if half else self.full_cols).cpu().numpy().view(np.uint32)
+        if short:
+            arrs = (self.shalf_ptr, self.shalf_len, self.shalf_cols) if half else \
+                (self.sfull_ptr, self.sfull_len, self.sfull_cols)
+        else:
+            arrs = (self.half_ptr, self.half_len, self.half_cols) if half else \
+                (self.full_ptr, self.full_len, self.full_cols)
+        ptr = arrs[0][a0:a1].cpu().numpy()
+        ln = arrs[1][a0:a1].cpu().numpy()
+        cols_all = arrs[2].cpu().numpy().view(np.uint32)
         rp = np.zeros(a1 - a0 + 1, np.int64)
         rp[1:] = np.cumsum(ln)
         out = np.empty(int(rp[-1]), np.uint32)

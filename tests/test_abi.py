@@ -41,7 +41,7 @@ def test_reference_params():
 def test_errors_are_reported():
     from protein_physics_b200 import _lib
     L = _lib.lib()
-    rc = L.alma_nl_build(None, None, None, None, None, 0, None)
+    rc = L.alma_nl_build(None, None, None, None, None, None, 0, None)
     assert rc == _lib.ALMA_EINVAL
     assert b"alma_nl_build" in L.alma_last_error()
     with pytest.raises(ValueError):

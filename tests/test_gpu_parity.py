@@ -44,6 +44,29 @@ def test_nl_bit_exact(golden, oracle):
         assert set(fcols[frp[i]:frp[i + 1]].tolist()) == half_i | lower
 
 
+def test_nl_short_rows(golden):
+    """Short rows: the full/half rows filtered, in order, to the pairs within
+    R*_i + R*_j + 2 probe + skin (+1e-6) at build time."""
+    b = _batch(golden)
+    b.build_nl()
+    p = b.params
+    pad = 2.0 * p.probe_r + 2.0 * np.sqrt(p.half_skin2) + 1e-6
+    x, r = golden["xyz"], golden["r"]
+    for half in (True, False):
+        rp, cols, flags = b.nl_host(0, half=half)
+        srp, scols, sflags = b.nl_host(0, half=half, short=True)
+        for i in range(golden.n):
+            row = cols[rp[i]:rp[i + 1]]
+            fl = flags[rp[i]:rp[i + 1]]
+            reach = r[i] + pad + r[row]
+            keep = np.sum((x[row] - x[i]) ** 2, axis=1) < reach * reach
+            assert np.array_equal(scols[srp[i]:srp[i + 1]], row[keep]), i
+            assert np.array_equal(sflags[srp[i]:srp[i + 1]], fl[keep]), i
+    need = b.need.cpu().numpy()[0]
+    assert need[2] == len(b.nl_host(0, half=False, short=True)[1])
+    assert need[3] == len(b.nl_host(0, half=True, short=True)[1])
+
+
 @pytest.mark.parametrize("precision,rtol", [("fp64", 1e-12), ("mixed", 2e-6)])
 def test_born_radii(golden, oracle, precision, rtol):
     b = _batch(golden, precision)
