@@ -196,6 +196,78 @@ int alma_born_radii(const AlmaBatch *b, const AlmaNL *nl, const AlmaParams *p, i
 int alma_energy(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *nl, const AlmaParams *p,
                 int prec, const uint8_t *sys_mask, double *atom_e, double *terms, void *stream);
 
+/* Analytic gradient of the total energy (the backward of alma_energy; the
+ * reference has no gradient: this is the derivative of total_e,
+ * physics_engine.cpp:2205-2234, through born_radii :2024-2039, pair_e
+ * :2148-2164, sasa_nonpolar :2068-2083, dihedral_e :1912-1921 and ss_e
+ * :1965-1974).  grad: device double[natoms*4], dE/dx per atom (x, y, z, 0)
+ * in kcal/mol/Å.  b->born must hold the radii of the current coordinates
+ * (alma_born_radii or alma_energy) and nl a list valid for them; the HCT
+ * derivatives are recomputed, not stored.  Deterministic: every sum has a
+ * fixed order (pair and Born parts gathered over full rows, SASA and bonded
+ * parts added as 64-bit fixed point, 2^-32 kcal/mol/Å).  workspace:
+ * alma_forces_workspace_bytes(natoms) device bytes.  sys_mask as above. */
+size_t alma_forces_workspace_bytes(int32_t natoms);
+int alma_forces(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *nl, const AlmaParams *p, int prec,
+                const uint8_t *sys_mask, void *workspace, double *grad, void *stream);
+
+/* ---- torsion space: gradient, all-bond moves, gradient-guided sampling ----
+ * The reference moves one or two torsions per proposal (rodrigues,
+ * physics_engine.cpp:1848-1862); these entry points have no reference
+ * counterpart: they are the torsion-space side of the analytic gradient
+ * (descent minimisation, Langevin / MALA proposals). */
+
+/* Nesting of the rotatable bonds' j-sides, local indices per system (each
+ * system's rows start at its own bond / atom offset).  Built on the host by
+ * alma_torsion_tree, uploaded by the caller. */
+typedef struct {
+    const int32_t *rb_parent; /* [nrb] innermost bond whose j-side holds this bond's axis atom i, -1 none */
+    const int32_t *atom_rb;   /* [natoms] innermost bond whose j-side holds the atom, -1 none             */
+} AlmaTorsionTree;
+
+/* Host: the tree of one system from its j-sides (local atom indices:
+ * side_ptr [nrb+1] / side_idx explicit atoms, [side_lo, side_hi) range).
+ * ALMA_EINVAL when the j-sides are not nested (a ring in the bond graph). */
+int alma_torsion_tree(int32_t natoms, int32_t nrb, const int32_t *rb_ij, const int64_t *side_ptr,
+                      const int32_t *side_idx, const int32_t *side_lo, const int32_t *side_hi, int32_t *rb_parent,
+                      int32_t *atom_rb);
+size_t alma_torsion_workspace_bytes(int32_t natoms, int32_t nsys, int32_t nrb);
+/* gtheta[k] = dE/dθ_k = u_k · Σ_{m in j-side k} (x_m - x_i) × grad_m for every
+ * rotatable bond (grad: device double[natoms*4], e.g. from alma_forces). */
+int alma_torsion_grad(const AlmaBatch *b, const AlmaTopo *t, const double *grad, const uint8_t *sys_mask,
+                      void *workspace, double *gtheta, void *stream);
+/* Turns every rotatable bond k by delta[k] radians at once (the same
+ * structure as the reference's moves applied one after another with axes
+ * from the updated coordinates).  Coordinates change in place; Born radii
+ * and neighbor list are the caller's to refresh. */
+int alma_torsion_apply(const AlmaBatch *b, const AlmaTopo *t, const AlmaTorsionTree *tree, const double *delta,
+                       const uint8_t *sys_mask, void *workspace, void *stream);
+
+/* Per-system state of the Langevin (MALA) torsion sampler (48 bytes). */
+typedef struct {
+    double energy;            /* energy of the current state (kcal/mol)     */
+    double beta;              /* 1/T, T in kcal/mol                         */
+    int64_t step;             /* proposals made (the RNG counter)           */
+    int64_t n_proposed, n_accepted;
+    double log_alpha;         /* log acceptance ratio of the last proposal  */
+} AlmaMalaState;
+
+/* delta[k] = -½ σ_k² β ∇_θE_k + σ_k ξ_k, ξ ~ N(0,1) (Philox, keyed by seed,
+ * system, state.step, bond); σ_k <= 0 keeps bond k fixed. */
+int alma_mala_propose(const AlmaTopo *t, int32_t nsys, const double *gtheta, const double *sigma,
+                      const AlmaMalaState *states, uint64_t seed, const uint8_t *sys_mask, double *delta,
+                      void *stream);
+/* Metropolis–Hastings test of the proposal (energy terms_new[5s+4],
+ * torsion gradients before / after): accept[s], state energy / counters. */
+int alma_mala_accept(const AlmaTopo *t, int32_t nsys, const double *delta, const double *g_old, const double *g_new,
+                     const double *sigma, const double *terms_new, uint64_t seed, const uint8_t *sys_mask,
+                     AlmaMalaState *states, uint8_t *accept, void *stream);
+/* Rejected systems: xyz, born <- saved copies.  Accepted: g_cur <- g_new
+ * (both may be NULL). */
+int alma_mala_select(AlmaBatch *b, const AlmaTopo *t, const uint8_t *accept, const uint8_t *sys_mask,
+                     const double *xyz_old, const double *born_old, const double *g_new, double *g_cur,
+                     void *stream);
+
 /* Device scratch for the move / MC kernels: alma_move_scratch_bytes(natoms)
  * bytes, zeroed once by alma_move_scratch_init; every call leaves it zeroed.
  * Calls that share a scratch buffer must not overlap on the GPU. */

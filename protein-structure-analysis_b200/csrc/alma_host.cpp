@@ -154,4 +154,67 @@ int alma_topo_sides_compact(int32_t n, const int64_t *adj_ptr, const int32_t *ad
     return ALMA_OK;
 }
 
+// Nesting of the rotatable bonds' j-sides (one system, local indices).  On
+// a tree every two j-sides are nested or disjoint: atom_rb[m] = the bond
+// with the smallest side that holds atom m, rb_parent[k] = atom_rb[i_k]
+// (a side that holds the axis atom i_k holds all of side k).  Sides are
+// assigned in decreasing size, so the smallest one wins; the check
+// Σ_k |side_k| = Σ_m depth(m) rejects sides that overlap without nesting
+// (a ring, e.g. a disulfide, inside the bond graph).
+int alma_torsion_tree(int32_t natoms, int32_t nrb, const int32_t *rb_ij, const int64_t *side_ptr,
+                      const int32_t *side_idx, const int32_t *side_lo, const int32_t *side_hi, int32_t *rb_parent,
+                      int32_t *atom_rb) {
+    if (natoms < 0 || nrb < 0 || (natoms > 0 && !atom_rb) ||
+        (nrb > 0 && (!rb_ij || !side_ptr || !side_lo || !side_hi || !rb_parent)))
+        return alma_set_error(ALMA_EINVAL, "alma_torsion_tree: bad arguments");
+    std::vector<int64_t> size((size_t)nrb);
+    for (int32_t k = 0; k < nrb; ++k)
+        size[(size_t)k] = (side_ptr[k + 1] - side_ptr[k]) + std::max(0, side_hi[k] - side_lo[k]);
+    std::vector<int32_t> order((size_t)nrb);
+    for (int32_t k = 0; k < nrb; ++k) order[(size_t)k] = k;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int32_t a, int32_t b) { return size[(size_t)a] > size[(size_t)b]; });
+    for (int32_t m = 0; m < natoms; ++m) atom_rb[m] = -1;
+    int64_t total = 0;
+    for (int32_t k : order) {
+        for (int32_t m = side_lo[k]; m < side_hi[k]; ++m) {
+            if (m < 0 || m >= natoms) return alma_set_error(ALMA_EINVAL, "alma_torsion_tree: side atom out of range");
+            atom_rb[m] = k;
+        }
+        for (int64_t e = side_ptr[k]; e < side_ptr[k + 1]; ++e) {
+            const int32_t m = side_idx[e];
+            if (m < 0 || m >= natoms) return alma_set_error(ALMA_EINVAL, "alma_torsion_tree: side atom out of range");
+            atom_rb[m] = k;
+        }
+        total += size[(size_t)k];
+    }
+    for (int32_t k = 0; k < nrb; ++k) {
+        const int32_t i = rb_ij[2 * k];
+        if (i < 0 || i >= natoms) return alma_set_error(ALMA_EINVAL, "alma_torsion_tree: axis atom out of range");
+        rb_parent[k] = atom_rb[i];
+        if (rb_parent[k] == k || (rb_parent[k] >= 0 && size[(size_t)rb_parent[k]] <= size[(size_t)k]))
+            return alma_set_error(ALMA_EINVAL, "alma_torsion_tree: j-sides are not nested (ring in the bond graph)");
+    }
+    std::vector<int64_t> depth((size_t)nrb, -1);
+    int64_t sum = 0;
+    for (int32_t m = 0; m < natoms; ++m) {
+        int32_t k = atom_rb[m];
+        if (k < 0) continue;
+        if (depth[(size_t)k] < 0) {  // walk up to a known depth (sizes strictly grow: no cycle)
+            std::vector<int32_t> path;
+            int32_t c = k;
+            while (c >= 0 && depth[(size_t)c] < 0) {
+                path.push_back(c);
+                c = rb_parent[c];
+            }
+            int64_t d = c >= 0 ? depth[(size_t)c] : 0;
+            for (size_t q = path.size(); q-- > 0;) depth[(size_t)path[q]] = ++d;
+        }
+        sum += depth[(size_t)k];
+    }
+    if (sum != total)
+        return alma_set_error(ALMA_EINVAL, "alma_torsion_tree: j-sides are not nested (ring in the bond graph)");
+    return ALMA_OK;
+}
+
 }  // extern "C"

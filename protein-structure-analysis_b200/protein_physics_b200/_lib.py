@@ -86,6 +86,21 @@ STATE_DTYPE = np.dtype([("cur_max", "f8"), ("energy", "f8"), ("temperature", "f8
                         ("tot_win", "i4"), ("need_rebuild", "i4"), ("parity", "i4")])
 assert STATE_DTYPE.itemsize == C.sizeof(AlmaChainState) == 72
 
+
+
+class AlmaTorsionTree(C.Structure):
+    _fields_ = [("rb_parent", _p), ("atom_rb", _p)]
+
+
+class AlmaMalaState(C.Structure):
+    _fields_ = [("energy", C.c_double), ("beta", C.c_double), ("step", C.c_int64), ("n_proposed", C.c_int64),
+                ("n_accepted", C.c_int64), ("log_alpha", C.c_double)]
+
+
+MALA_STATE_DTYPE = np.dtype([("energy", "f8"), ("beta", "f8"), ("step", "i8"), ("n_proposed", "i8"),
+                             ("n_accepted", "i8"), ("log_alpha", "f8")])
+assert MALA_STATE_DTYPE.itemsize == C.sizeof(AlmaMalaState) == 48
+
 _lib = None
 
 
@@ -112,6 +127,17 @@ def lib():
     L.alma_nl_build.argtypes = [_p, _p, _p, _p, _p, _p, _i64, _p]
     L.alma_born_radii.argtypes = [_p, _p, _p, C.c_int, _p, _p]
     L.alma_energy.argtypes = [_p, _p, _p, _p, C.c_int, _p, _p, _p, _p]
+    L.alma_forces_workspace_bytes.restype = C.c_size_t
+    L.alma_forces_workspace_bytes.argtypes = [_i32]
+    L.alma_forces.argtypes = [_p, _p, _p, _p, C.c_int, _p, _p, _p, _p]
+    L.alma_torsion_tree.argtypes = [_i32, _i32, _p, _p, _p, _p, _p, _p, _p]
+    L.alma_torsion_workspace_bytes.restype = C.c_size_t
+    L.alma_torsion_workspace_bytes.argtypes = [_i32, _i32, _i32]
+    L.alma_torsion_grad.argtypes = [_p, _p, _p, _p, _p, _p, _p]
+    L.alma_torsion_apply.argtypes = [_p, _p, _p, _p, _p, _p, _p]
+    L.alma_mala_propose.argtypes = [_p, _i32, _p, _p, _p, C.c_uint64, _p, _p, _p]
+    L.alma_mala_accept.argtypes = [_p, _i32, _p, _p, _p, _p, _p, C.c_uint64, _p, _p, _p, _p]
+    L.alma_mala_select.argtypes = [_p, _p, _p, _p, _p, _p, _p, _p, _p]
     L.alma_mc_run.argtypes = [_p, _p, _p, _p, C.c_int, _p, _p, _p, _i64, _p]
     L.alma_mc_after_rebuild.argtypes = [_p, _p, _p, _i32, _p]
     L.alma_move_scratch_init.argtypes = [_p, _i32, _p]

@@ -101,6 +101,8 @@ class DeviceBatch:
         self.born = torch.zeros(max(n, 1), dtype=torch.float64, device=_DEV)
         self.status = torch.zeros(1, dtype=torch.int32, device=_DEV)
         self.atom_off = _t(self.atom_off_h, torch.int32)
+        self.atom_sys = torch.as_tensor(np.repeat(np.arange(self.nsys), np.diff(self.atom_off_h)), dtype=torch.int64,
+                                        device=_DEV)
 
     def _build_topology(self, topos):
         off = self.atom_off_h
@@ -313,6 +315,27 @@ class DeviceBatch:
                                       _ptr(sys_mask) if sys_mask is not None else None, _ptr(self._atom_e),
                                       _ptr(terms), self._sp()), "alma_energy")
         return terms
+
+    def forces(self, sys_mask=None, out=None, recompute_born=False):
+        """dE/dx [natoms, 4] float64 (x, y, z, 0) at the current coordinates
+        (alma_forces).  The Born radii must be those of the current
+        coordinates: energy_terms() leaves them so; recompute_born=True
+        recomputes them first."""
+        if not self.nl_ready:
+            self.build_nl()
+            recompute_born = True
+        if recompute_born:
+            self.born_radii(sys_mask)
+        g = out if out is not None else torch.zeros((max(self.natoms, 1), 4), dtype=torch.float64, device=_DEV)
+        if getattr(self, "_force_ws", None) is None:
+            self._force_ws = torch.zeros(self.L.alma_forces_workspace_bytes(self.natoms), dtype=torch.uint8,
+                                         device=_DEV)
+        b, t, nl = self.batch_s, self.topo_s, self.nl_s
+        _lib.check(self.L.alma_forces(C.byref(b), C.byref(t) if self.use_topo else None, C.byref(nl),
+                                      C.byref(self.params), self.prec,
+                                      _ptr(sys_mask) if sys_mask is not None else None, _ptr(self._force_ws),
+                                      _ptr(g), self._sp()), "alma_forces")
+        return g
 
     # ---- one proposal per system ---------------------------------------------
     def move_dE(self, kind, a, delta, apply=False):

@@ -1,0 +1,228 @@
+"""GPU checks of torsion space: all-bond moves, the torsion gradient,
+descent minimisation, MALA and the autograd wrapper (through the C ABI).
+
+  * alma_torsion_apply vs the reference's one-bond-at-a-time rotations
+    (numpy, axes from the updated coordinates): 1e-9 Å;
+  * alma_torsion_grad vs the projection of the FP64 torch-autograd gradient
+    (oracle/torch_energy.py) onto each bond: 1e-8 relative; and vs central
+    finite differences of the energy (h = 1e-5 rad, list fixed) for bonds
+    whose rotation moves no pair across the reference's 12 Å cutoff:
+    1e-5 relative + 1e-6;
+  * descent: monotone, ends below the start, final energy = a fresh
+    evaluation of the final coordinates;
+  * MALA: the device's log acceptance ratio equals a host recomputation
+    from the oracle energy and the autograd torsion gradient at the
+    proposal; runs are reproducible from the seed.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def _rot(p, o, u, d):
+    v = p - o
+    c, s = np.cos(d), np.sin(d)
+    return o + v * c + np.cross(u, v) * s + np.outer(v @ u, u) * (1 - c)
+
+
+def _sequential(x0, T, flat, delta):
+    xs = x0.copy()
+    for k in range(flat.nrb):
+        if delta[k] == 0.0:
+            continue
+        side = np.array(sorted(T.side_set(k)))
+        o = xs[flat.rb_i[k]]
+        u = xs[flat.rb_j[k]] - o
+        u /= np.linalg.norm(u)
+        xs[side] = _rot(xs[side], o, u, delta[k])
+    return xs
+
+
+def _golden_batch(name, precision="fp64"):
+    from conftest import Golden
+    from protein_physics_b200.device import DeviceBatch
+    from protein_physics_b200.topology import flatten
+    g = Golden(name)
+    T = g.topology()
+    flat = flatten(T)
+    b = DeviceBatch([(g["xyz"], g["q"], g["r"], g["eps"], flat)], precision=precision)
+    return g, T, flat, b
+
+
+def test_torsion_apply_matches_sequential():
+    from protein_physics_b200 import synth
+    from protein_physics_b200.device import DeviceBatch
+    from protein_physics_b200.topology import BondTopology, flatten
+    from protein_physics_b200.torsion import TorsionSpace
+    chains, topos, flats = [], [], []
+    for seed, nres in ((5, 10), (6, 14)):
+        ch = synth.chain(nres, seed)
+        T = BondTopology()
+        T.build(ch.resnames, ch.atomnames, ch.res_idx)
+        chains.append(ch)
+        topos.append(T)
+        flats.append(flatten(T))
+    b = DeviceBatch([(c.xyz, c.charge, c.radius, c.epsilon, f) for c, f in zip(chains, flats)])
+    ts = TorsionSpace(b)
+    rng = np.random.default_rng(1)
+    delta = rng.normal(0, 0.2, ts.nrb)
+    ts.apply(torch.as_tensor(delta, device="cuda"))
+    for s in range(2):
+        d = delta[b.rb_off_h[s]:b.rb_off_h[s + 1]]
+        ref = _sequential(chains[s].xyz, topos[s], flats[s], d)
+        assert np.abs(b.coords(s) - ref).max() < 1e-9
+    # masked: system 0 only
+    before = [b.coords(s).copy() for s in range(2)]
+    mask = torch.tensor([1, 0], dtype=torch.uint8, device="cuda")
+    ts.apply(torch.as_tensor(delta, device="cuda"), sys_mask=mask)
+    assert np.array_equal(b.coords(1), before[1])
+    assert not np.array_equal(b.coords(0), before[0])
+
+
+def _autograd_gtheta(x, gx, flat, T):
+    out = np.zeros(flat.nrb)
+    for k in range(flat.nrb):
+        side = np.array(sorted(T.side_set(k)))
+        o = x[flat.rb_i[k]]
+        u = x[flat.rb_j[k]] - o
+        u /= np.linalg.norm(u)
+        out[k] = np.sum(np.cross(u, x[side] - o) * gx[side])
+    return out
+
+
+def test_torsion_grad_vs_autograd_and_fd(oracle):
+    from torch_energy import TorchEnergy
+    from protein_physics_b200.torsion import TorsionSpace
+    g, T, flat, b = _golden_batch("insulin")
+    b.build_nl()
+    b.energy_terms()
+    ts = TorsionSpace(b)
+    gth = ts.gtheta(b.forces()).cpu().numpy()[:flat.nrb]
+    ptr, cols = oracle.nl_build(g["xyz"])
+    _, gx = TorchEnergy(g["q"], g["r"], g["eps"], ptr, cols, flat).energy_and_grad(g["xyz"])
+    ref = _autograd_gtheta(np.asarray(g["xyz"]), gx, flat, T)
+    assert np.abs(gth - ref).max() <= 1e-8 * max(1.0, np.abs(ref).max())
+    # finite differences along single torsions, list fixed
+    x0 = np.asarray(g["xyz"], np.float64)
+    I = np.repeat(np.arange(g.n), np.diff(ptr))
+    h = 1e-5
+    rng = np.random.default_rng(3)
+    checked = 0
+    for k in rng.permutation(flat.nrb):
+        side = np.array(sorted(T.side_set(k)))
+        if side.size > 40:
+            continue
+        xs = [_sequential(x0, T, flat, np.where(np.arange(flat.nrb) == k, d, 0.0)) for d in (h, -h)]
+        near = False
+        for xx in [x0] + xs:
+            r = np.sqrt(((xx[I] - xx[cols]) ** 2).sum(1))
+            near |= bool(np.any(np.abs(r - 12.0) < 1e-4))
+        if near:
+            continue
+        Es = []
+        for xx in xs:
+            b.xyz[:g.n, :3].copy_(torch.as_tensor(xx, device="cuda"))
+            b.nl_ready = True  # same list: displacements are far inside the skin
+            Es.append(float(b.energy_terms()[0, 4]))
+        fd = (Es[0] - Es[1]) / (2 * h)
+        assert abs(gth[k] - fd) <= 1e-5 * abs(fd) + 1e-6, (k, gth[k], fd)
+        checked += 1
+        if checked == 24:
+            break
+    assert checked >= 8
+
+
+def test_minimize_monotone():
+    from protein_physics_b200 import synth
+    from protein_physics_b200.device import DeviceBatch
+    from protein_physics_b200.topology import BondTopology, flatten
+    from protein_physics_b200.torsion import minimize
+    ch = synth.chain(24, 11)
+    T = BondTopology()
+    T.build(ch.resnames, ch.atomnames, ch.res_idx)
+    b = DeviceBatch([(ch.xyz, ch.charge, ch.radius, ch.epsilon, flatten(T))], precision="mixed")
+    hist, eta = minimize(b, steps=60)
+    E = hist[:, 0].cpu().numpy()
+    assert np.all(np.diff(E) <= 0.0)
+    assert E[-1] < E[0]
+    b.nl_ready = False
+    assert float(b.energy_terms()[0, 4]) == pytest.approx(E[-1], rel=1e-12)
+
+
+def test_mala_log_alpha_matches_host(oracle):
+    from oracle import TopoArrays
+    from torch_energy import TorchEnergy
+    from protein_physics_b200.torsion import MALARunner
+    g, T, flat, b = _golden_batch("insulin")
+    x0 = np.asarray(g["xyz"], np.float64).copy()
+    R = MALARunner(b, 0.6, seed=99, step=np.radians(0.5))
+    st0 = R.state()
+    g0 = R.cur.g.cpu().numpy()[:flat.nrb].copy()
+    R.step()
+    st1 = R.state()
+    delta = R.delta.cpu().numpy()[:flat.nrb]
+    sig = R.sigma.cpu().numpy()[:flat.nrb]
+    x1 = _sequential(x0, T, flat, delta)
+    E0 = oracle.calculate_potential(x0, g["q"], g["r"], g["eps"], TopoArrays(flat))[4]
+    E1 = oracle.calculate_potential(x1, g["q"], g["r"], g["eps"], TopoArrays(flat))[4]
+    assert st0["energy"][0] == pytest.approx(E0, rel=1e-10)
+    ptr, cols = oracle.nl_build(x1)
+    _, gx1 = TorchEnergy(g["q"], g["r"], g["eps"], ptr, cols, flat).energy_and_grad(x1)
+    g1 = _autograd_gtheta(x1, gx1, flat, T)
+    beta = 1.0 / 0.6
+    m = sig > 0
+    h = 0.5 * sig[m] ** 2 * beta
+    fwd = np.sum((delta[m] + h * g0[m]) ** 2 / (2 * sig[m] ** 2))
+    rev = np.sum((-delta[m] + h * g1[m]) ** 2 / (2 * sig[m] ** 2))
+    la = -beta * (E1 - E0) - rev + fwd
+    assert st1["log_alpha"][0] == pytest.approx(la, rel=1e-7, abs=1e-6)
+    acc = bool(R.accept.cpu().numpy()[0])
+    assert st1["n_accepted"][0] == int(acc)
+    assert np.abs(b.coords(0) - (x1 if acc else x0)).max() < 1e-9
+
+
+def test_mala_reproducible_and_mixing():
+    from protein_physics_b200 import synth
+    from protein_physics_b200.device import DeviceBatch
+    from protein_physics_b200.topology import BondTopology, flatten
+    from protein_physics_b200.torsion import MALARunner
+    ch = synth.chain(16, 4)
+    T = BondTopology()
+    T.build(ch.resnames, ch.atomnames, ch.res_idx)
+    flat = flatten(T)
+    out = []
+    for _ in range(2):
+        b = DeviceBatch([(ch.xyz, ch.charge, ch.radius, ch.epsilon, flat)] * 2, precision="mixed")
+        R = MALARunner(b, [0.5962, 0.9], seed=5, step=np.radians(0.5))
+        st = R.run(40)
+        out.append((st, b.coords(0), b.coords(1)))
+    assert np.array_equal(out[0][1], out[1][1]) and np.array_equal(out[0][2], out[1][2])
+    st = out[0][0]
+    assert np.all(st["n_proposed"] == 40)
+    assert np.all(st["n_accepted"] > 0) and np.all(st["n_accepted"] < 40)
+
+
+def test_autograd_energy_matches_forces():
+    from protein_physics_b200.autograd import EnergyModel
+    from protein_physics_b200.topology import flatten
+    from conftest import Golden
+    systems = []
+    for n in ("insulin", "synth64"):
+        g = Golden(n)
+        systems.append((g["xyz"], g["q"], g["r"], g["eps"], flatten(g.topology())))
+    model = EnergyModel(systems, precision="fp64")
+    x = model.coords().requires_grad_()
+    E = model(x)
+    w = torch.tensor([2.0, -0.5], dtype=torch.float64, device="cuda")
+    (E * w).sum().backward()
+    b = model.batch
+    f = b.forces()[:b.natoms, :3]
+    sys_of = b.atom_sys
+    assert torch.allclose(x.grad, f * w[sys_of].unsqueeze(1), rtol=0, atol=0)
+    for s, (xyz, q, r, e, flat) in enumerate(systems):
+        from protein_physics_b200.device import DeviceBatch
+        ref = float(DeviceBatch([(xyz, q, r, e, flat)], precision="fp64").energy_terms()[0, 4])
+        assert float(E[s]) == pytest.approx(ref, rel=1e-13)
