@@ -243,25 +243,40 @@ int alma_torsion_grad(const AlmaBatch *b, const AlmaTopo *t, const double *grad,
 int alma_torsion_apply(const AlmaBatch *b, const AlmaTopo *t, const AlmaTorsionTree *tree, const double *delta,
                        const uint8_t *sys_mask, void *workspace, void *stream);
 
-/* Per-system state of the Langevin (MALA) torsion sampler (48 bytes). */
+/* Per-system state of the Langevin (MALA) torsion sampler (64 bytes). */
 typedef struct {
     double energy;            /* energy of the current state (kcal/mol)     */
     double beta;              /* 1/T, T in kcal/mol                         */
+    double scale;             /* multiplies every bond's sigma (adapted)    */
+    double log_alpha;         /* log acceptance ratio of the last proposal  */
     int64_t step;             /* proposals made (the RNG counter)           */
     int64_t n_proposed, n_accepted;
-    double log_alpha;         /* log acceptance ratio of the last proposal  */
+    int32_t acc_win, tot_win; /* adaptation window                          */
 } AlmaMalaState;
 
-/* delta[k] = -½ σ_k² β ∇_θE_k + σ_k ξ_k, ξ ~ N(0,1) (Philox, keyed by seed,
- * system, state.step, bond); σ_k <= 0 keeps bond k fixed. */
+typedef struct {
+    uint64_t seed;            /* Philox key                                  */
+    double drift_clip;        /* drift clipped to ±drift_clip·σ per bond     */
+    int32_t tune_freq;        /* proposals per adaptation window, 0 = off    */
+    int32_t pad;
+    double target_lo, target_hi;  /* acceptance band of the window           */
+    double scale_up, scale_down;  /* scale factors outside the band          */
+    double scale_min, scale_max;
+} AlmaMalaConfig;
+
+/* delta[k] = clip(-½ σ_k² β ∇_θE_k, ±drift_clip σ_k) + σ_k ξ_k with
+ * σ_k = state.scale × sigma[k], ξ ~ N(0,1) (Philox, keyed by seed, system,
+ * state.step, bond); sigma[k] <= 0 keeps bond k fixed.  The truncated drift
+ * keeps clash gradients from throwing proposals away. */
 int alma_mala_propose(const AlmaTopo *t, int32_t nsys, const double *gtheta, const double *sigma,
-                      const AlmaMalaState *states, uint64_t seed, const uint8_t *sys_mask, double *delta,
-                      void *stream);
+                      const AlmaMalaConfig *cfg, const AlmaMalaState *states, const uint8_t *sys_mask,
+                      double *delta, void *stream);
 /* Metropolis–Hastings test of the proposal (energy terms_new[5s+4],
- * torsion gradients before / after): accept[s], state energy / counters. */
+ * torsion gradients before / after): accept[s], state energy / counters,
+ * then the scale adaptation. */
 int alma_mala_accept(const AlmaTopo *t, int32_t nsys, const double *delta, const double *g_old, const double *g_new,
-                     const double *sigma, const double *terms_new, uint64_t seed, const uint8_t *sys_mask,
-                     AlmaMalaState *states, uint8_t *accept, void *stream);
+                     const double *sigma, const double *terms_new, const AlmaMalaConfig *cfg,
+                     const uint8_t *sys_mask, AlmaMalaState *states, uint8_t *accept, void *stream);
 /* Rejected systems: xyz, born <- saved copies.  Accepted: g_cur <- g_new
  * (both may be NULL). */
 int alma_mala_select(AlmaBatch *b, const AlmaTopo *t, const uint8_t *accept, const uint8_t *sys_mask,

@@ -14,10 +14,10 @@
 //             atom m moves by T_k = A_root ∘ ... ∘ A_parent ∘ A_k, k = the
 //             innermost bond holding m.  T is built per bond by pointer
 //             jumping (log2(depth) rounds) inside one CTA per system;
-//   MALA      θ' = θ - ½ σ² β ∇_θE + σ ξ per bond (σ_k = step × lever
-//             scale), accepted with the Metropolis–Hastings ratio of the
-//             Langevin proposal densities; Philox draws keyed by (seed,
-//             system, step, bond).
+//   MALA      θ' = θ + clip(-½ σ² β ∇_θE, ±c σ) + σ ξ per bond (σ_k =
+//             state scale × step × lever scale), accepted with the
+//             Metropolis–Hastings ratio of the Langevin proposal densities;
+//             Philox draws keyed by (seed, system, step, bond).
 #include <algorithm>
 
 #include "alma_common.cuh"
@@ -264,15 +264,25 @@ __device__ __forceinline__ void mala_key(uint64_t seed, int s, uint32_t &k0, uin
     k1 = (uint32_t)(seed >> 32) ^ 0x27D4EB2Fu;
 }
 
+// Truncated Langevin drift of bond k (MALTA: Roberts & Tweedie, Bernoulli
+// 2:341, 1996): -½ σ² β g clipped to ±clip·σ.  Steep clashes give
+// gradients of 1e3-1e6 kcal/mol/rad whose untruncated drift would throw
+// the proposal far away; any deterministic drift keeps detailed balance as
+// long as the same function enters the forward and reverse densities.
+__device__ __forceinline__ double mala_drift(double sg, double beta, double g, double clip) {
+    const double mu = -0.5 * sg * sg * beta * g, lim = clip * sg;
+    return fmin(fmax(mu, -lim), lim);
+}
+
 __global__ void mala_propose_kernel(int nrb, int nsys, const int32_t *__restrict__ rb_off,
                                     const double *__restrict__ gtheta, const double *__restrict__ sigma,
-                                    const AlmaMalaState *__restrict__ st, uint64_t seed,
+                                    const AlmaMalaState *__restrict__ st, AlmaMalaConfig cfg,
                                     const uint8_t *__restrict__ mask, double *__restrict__ delta) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nrb) return;
     const int s = sys_of_bond(rb_off, nsys, k);
     if (mask && !mask[s]) return;
-    const double sg = sigma[k];
+    const double sg = sigma[k] * st[s].scale;
     if (!(sg > 0.0)) {
         delta[k] = 0.0;
         return;
@@ -280,32 +290,33 @@ __global__ void mala_propose_kernel(int nrb, int nsys, const int32_t *__restrict
     const int kl = k - rb_off[s];
     const uint64_t step = (uint64_t)st[s].step;
     uint32_t k0, k1;
-    mala_key(seed, s, k0, k1);
+    mala_key(cfg.seed, s, k0, k1);
     const Philox4 r = philox4x32_10((uint32_t)step, (uint32_t)(step >> 32), (uint32_t)s,
                                     0x40000000u + ((uint32_t)kl >> 1), k0, k1);
     // Box–Muller: two normals per draw, bond parity picks one
     const double u1 = 1.0 - u01_from(r.v[0], r.v[1]), u2 = u01_from(r.v[2], r.v[3]);
     const double rad = sqrt(-2.0 * log(u1));
     const double xi = (kl & 1) ? rad * sin(6.283185307179586 * u2) : rad * cos(6.283185307179586 * u2);
-    delta[k] = -0.5 * sg * sg * st[s].beta * gtheta[k] + sg * xi;
+    delta[k] = mala_drift(sg, st[s].beta, gtheta[k], cfg.drift_clip) + sg * xi;
 }
 
-// One CTA per system: Metropolis–Hastings test of the Langevin proposal.
+// One CTA per system: Metropolis–Hastings test of the Langevin proposal,
+// then the step-scale adaptation window.
 __global__ void mala_accept_kernel(int nsys, const int32_t *__restrict__ rb_off, const double *__restrict__ delta,
                                    const double *__restrict__ g_old, const double *__restrict__ g_new,
                                    const double *__restrict__ sigma, const double *__restrict__ terms_new,
-                                   uint64_t seed, const uint8_t *__restrict__ mask, AlmaMalaState *__restrict__ st,
-                                   uint8_t *__restrict__ accept) {
+                                   AlmaMalaConfig cfg, const uint8_t *__restrict__ mask,
+                                   AlmaMalaState *__restrict__ st, uint8_t *__restrict__ accept) {
     __shared__ double sm[32];
     const int s = blockIdx.x;
     if (mask && !mask[s]) return;
-    const double beta = st[s].beta;
+    const double beta = st[s].beta, scale = st[s].scale;
     double fwd = 0.0, rev = 0.0;
     for (int k = rb_off[s] + threadIdx.x; k < rb_off[s + 1]; k += blockDim.x) {
-        const double sg = sigma[k];
+        const double sg = sigma[k] * scale;
         if (!(sg > 0.0)) continue;
-        const double h = 0.5 * sg * sg * beta;
-        const double rf = delta[k] + h * g_old[k], rr = -delta[k] + h * g_new[k];
+        const double rf = delta[k] - mala_drift(sg, beta, g_old[k], cfg.drift_clip);
+        const double rr = -delta[k] - mala_drift(sg, beta, g_new[k], cfg.drift_clip);
         fwd += rf * rf / (2.0 * sg * sg);
         rev += rr * rr / (2.0 * sg * sg);
     }
@@ -316,7 +327,7 @@ __global__ void mala_accept_kernel(int nsys, const int32_t *__restrict__ rb_off,
         const double En = terms_new[5 * (size_t)s + 4];
         const double log_alpha = -beta * (En - S.energy) - rev + fwd;
         uint32_t k0, k1;
-        mala_key(seed, s, k0, k1);
+        mala_key(cfg.seed, s, k0, k1);
         const Philox4 r = philox4x32_10((uint32_t)S.step, (uint32_t)(S.step >> 32), (uint32_t)s, 0x3FFFFFFFu, k0, k1);
         const double u = u01_from(r.v[0], r.v[1]);
         const int acc = isfinite(En) && isfinite(log_alpha) && (log_alpha >= 0.0 || log(u) < log_alpha);
@@ -326,6 +337,14 @@ __global__ void mala_accept_kernel(int nsys, const int32_t *__restrict__ rb_off,
         if (acc) {
             S.energy = En;
             S.n_accepted++;
+        }
+        S.acc_win += acc;
+        if (cfg.tune_freq > 0 && ++S.tot_win == cfg.tune_freq) {
+            const double rate = (double)S.acc_win / (double)cfg.tune_freq;
+            if (rate > cfg.target_hi) S.scale = fmin(cfg.scale_max, S.scale * cfg.scale_up);
+            else if (rate < cfg.target_lo) S.scale = fmax(cfg.scale_min, S.scale * cfg.scale_down);
+            S.acc_win = 0;
+            S.tot_win = 0;
         }
         S.step++;
         st[s] = S;
@@ -407,24 +426,26 @@ extern "C" int alma_torsion_apply(const AlmaBatch *b, const AlmaTopo *t, const A
 }
 
 extern "C" int alma_mala_propose(const AlmaTopo *t, int32_t nsys, const double *gtheta, const double *sigma,
-                                 const AlmaMalaState *states, uint64_t seed, const uint8_t *sys_mask, double *delta,
-                                 void *stream) {
-    if (!t || nsys <= 0 || !t->rb_off || !gtheta || !sigma || !states || !delta)
+                                 const AlmaMalaConfig *cfg, const AlmaMalaState *states, const uint8_t *sys_mask,
+                                 double *delta, void *stream) {
+    if (!t || nsys <= 0 || !t->rb_off || !gtheta || !sigma || !cfg || !states || !delta)
         return alma_set_error(ALMA_EINVAL, "alma_mala_propose: bad arguments");
     if (t->nrb == 0) return ALMA_OK;
     mala_propose_kernel<<<(t->nrb + 255) / 256, 256, 0, (cudaStream_t)stream>>>(t->nrb, nsys, t->rb_off, gtheta,
-                                                                                sigma, states, seed, sys_mask, delta);
+                                                                                sigma, states, *cfg, sys_mask, delta);
     ALMA_LAUNCH_CHECK("alma_mala_propose");
     return ALMA_OK;
 }
 
 extern "C" int alma_mala_accept(const AlmaTopo *t, int32_t nsys, const double *delta, const double *g_old,
-                                const double *g_new, const double *sigma, const double *terms_new, uint64_t seed,
-                                const uint8_t *sys_mask, AlmaMalaState *states, uint8_t *accept, void *stream) {
-    if (!t || nsys <= 0 || !t->rb_off || !delta || !g_old || !g_new || !sigma || !terms_new || !states || !accept)
+                                const double *g_new, const double *sigma, const double *terms_new,
+                                const AlmaMalaConfig *cfg, const uint8_t *sys_mask, AlmaMalaState *states,
+                                uint8_t *accept, void *stream) {
+    if (!t || nsys <= 0 || !t->rb_off || !delta || !g_old || !g_new || !sigma || !terms_new || !cfg || !states ||
+        !accept)
         return alma_set_error(ALMA_EINVAL, "alma_mala_accept: bad arguments");
     mala_accept_kernel<<<nsys, 256, 0, (cudaStream_t)stream>>>(nsys, t->rb_off, delta, g_old, g_new, sigma, terms_new,
-                                                               seed, sys_mask, states, accept);
+                                                               *cfg, sys_mask, states, accept);
     ALMA_LAUNCH_CHECK("alma_mala_accept");
     return ALMA_OK;
 }

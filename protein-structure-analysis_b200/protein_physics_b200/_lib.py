@@ -93,13 +93,20 @@ class AlmaTorsionTree(C.Structure):
 
 
 class AlmaMalaState(C.Structure):
-    _fields_ = [("energy", C.c_double), ("beta", C.c_double), ("step", C.c_int64), ("n_proposed", C.c_int64),
-                ("n_accepted", C.c_int64), ("log_alpha", C.c_double)]
+    _fields_ = [("energy", C.c_double), ("beta", C.c_double), ("scale", C.c_double), ("log_alpha", C.c_double),
+                ("step", C.c_int64), ("n_proposed", C.c_int64), ("n_accepted", C.c_int64), ("acc_win", C.c_int32),
+                ("tot_win", C.c_int32)]
 
 
-MALA_STATE_DTYPE = np.dtype([("energy", "f8"), ("beta", "f8"), ("step", "i8"), ("n_proposed", "i8"),
-                             ("n_accepted", "i8"), ("log_alpha", "f8")])
-assert MALA_STATE_DTYPE.itemsize == C.sizeof(AlmaMalaState) == 48
+class AlmaMalaConfig(C.Structure):
+    _fields_ = [("seed", C.c_uint64), ("drift_clip", C.c_double), ("tune_freq", C.c_int32), ("pad", C.c_int32),
+                ("target_lo", C.c_double), ("target_hi", C.c_double), ("scale_up", C.c_double),
+                ("scale_down", C.c_double), ("scale_min", C.c_double), ("scale_max", C.c_double)]
+
+
+MALA_STATE_DTYPE = np.dtype([("energy", "f8"), ("beta", "f8"), ("scale", "f8"), ("log_alpha", "f8"), ("step", "i8"),
+                             ("n_proposed", "i8"), ("n_accepted", "i8"), ("acc_win", "i4"), ("tot_win", "i4")])
+assert MALA_STATE_DTYPE.itemsize == C.sizeof(AlmaMalaState) == 64
 
 _lib = None
 
@@ -135,8 +142,8 @@ def lib():
     L.alma_torsion_workspace_bytes.argtypes = [_i32, _i32, _i32]
     L.alma_torsion_grad.argtypes = [_p, _p, _p, _p, _p, _p, _p]
     L.alma_torsion_apply.argtypes = [_p, _p, _p, _p, _p, _p, _p]
-    L.alma_mala_propose.argtypes = [_p, _i32, _p, _p, _p, C.c_uint64, _p, _p, _p]
-    L.alma_mala_accept.argtypes = [_p, _i32, _p, _p, _p, _p, _p, C.c_uint64, _p, _p, _p, _p]
+    L.alma_mala_propose.argtypes = [_p, _i32, _p, _p, _p, _p, _p, _p, _p]
+    L.alma_mala_accept.argtypes = [_p, _i32, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p]
     L.alma_mala_select.argtypes = [_p, _p, _p, _p, _p, _p, _p, _p, _p]
     L.alma_mc_run.argtypes = [_p, _p, _p, _p, C.c_int, _p, _p, _p, _i64, _p]
     L.alma_mc_after_rebuild.argtypes = [_p, _p, _p, _i32, _p]

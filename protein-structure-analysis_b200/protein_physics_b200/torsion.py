@@ -155,24 +155,42 @@ def minimize(batch: DeviceBatch, steps=500, step0=0.02, grow=1.2, shrink=0.5, st
     return torch.stack(hist), eta
 
 
+def mala_config(seed, drift_clip=1.0, tune_freq=0, target=(0.4, 0.7), scale_up=1.1, scale_down=0.9,
+                scale_bounds=(0.01, 4.0)):
+    """AlmaMalaConfig: truncated drift at ±drift_clip·σ; every tune_freq
+    proposals (0: never) the step scale grows / shrinks when the window's
+    acceptance leaves the target band (as the reference adapts cur_max,
+    physics_engine.cpp:2515-2526)."""
+    cfg = _lib.AlmaMalaConfig()
+    cfg.seed = int(seed) & ((1 << 64) - 1)
+    cfg.drift_clip = float(drift_clip)
+    cfg.tune_freq = int(tune_freq)
+    cfg.target_lo, cfg.target_hi = target
+    cfg.scale_up, cfg.scale_down = scale_up, scale_down
+    cfg.scale_min, cfg.scale_max = scale_bounds
+    return cfg
+
+
 class MALARunner:
     """Metropolis-adjusted Langevin proposals in torsion space for every
     system of a batch: all rotatable bonds move at once by
-    -½ σ_k² β dE/dθ_k + σ_k ξ_k with σ_k = step × the bond's lever scale
-    (sidechain bonds × sidechain_mult), accepted by Metropolis–Hastings.
+    clip(-½ σ_k² β dE/dθ_k, ±clip σ_k) + σ_k ξ_k with σ_k = scale × step ×
+    the bond's lever scale (sidechain bonds × sidechain_mult), accepted by
+    Metropolis–Hastings.
 
     temperatures: kcal/mol per system (scalar broadcast)."""
 
     def __init__(self, batch: DeviceBatch, temperatures, seed, step=np.radians(0.5), sidechain_mult=2.5,
-                 ts: TorsionSpace | None = None):
+                 drift_clip=1.0, tune_freq=0, ts: TorsionSpace | None = None):
         self.b = batch
         self.ts = ts or TorsionSpace(batch)
-        self.seed = int(seed) & ((1 << 64) - 1)
+        self.cfg = mala_config(seed, drift_clip=drift_clip, tune_freq=tune_freq)
         T = np.broadcast_to(np.asarray(temperatures, np.float64), (batch.nsys,)).copy()
         if np.any(T <= 0):
             raise ValueError("temperature must be positive")
         st = np.zeros(batch.nsys, dtype=_lib.MALA_STATE_DTYPE)
         st["beta"] = 1.0 / T
+        st["scale"] = 1.0
         self.states = torch.from_numpy(st.view(np.uint8).copy()).to("cuda")
         kind = batch.rb_kind_h
         sig = float(step) * batch.rb_scale_h * np.where(kind == 2, sidechain_mult, 1.0)
@@ -204,15 +222,15 @@ class MALARunner:
 
     def step(self):
         b, ts, L = self.b, self.ts, self.b.L
-        topo = C.byref(b.topo_s)
-        _lib.check(L.alma_mala_propose(topo, b.nsys, _ptr(self.cur.g), _ptr(self.sigma), _ptr(self.states),
-                                       self.seed, None, _ptr(self.delta), b._sp()), "alma_mala_propose")
+        topo, cfg = C.byref(b.topo_s), C.byref(self.cfg)
+        _lib.check(L.alma_mala_propose(topo, b.nsys, _ptr(self.cur.g), _ptr(self.sigma), cfg, _ptr(self.states),
+                                       None, _ptr(self.delta), b._sp()), "alma_mala_propose")
         self.xyz_old.copy_(b.xyz)
         self.born_old.copy_(b.born)
         ts.apply(self.delta)
         self.new()
         _lib.check(L.alma_mala_accept(topo, b.nsys, _ptr(self.delta), _ptr(self.cur.g), _ptr(self.new.g),
-                                      _ptr(self.sigma), _ptr(self.new.terms), self.seed, None, _ptr(self.states),
+                                      _ptr(self.sigma), _ptr(self.new.terms), cfg, None, _ptr(self.states),
                                       _ptr(self.accept), b._sp()), "alma_mala_accept")
         ts.select(self.accept, self.xyz_old, self.born_old, g_new=self.new.g, g_cur=self.cur.g)
         b.nl_ready = False
