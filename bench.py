@@ -223,6 +223,8 @@ def run_ours(args, rank, world, local):
     if rank == 0:
         value = prop_total / (ms_max * 1e-3)
         cpu = cpu_baseline(chains[0], topos[0], temps[0], args) if world == 1 else None
+        plain = plain_gpu_baseline(chains[0], temps[0]) if (world == 1 and args.workload == "single") else None
+        ef = energy_force_rate(systems[0])
         out = {
             "metric": "Metropolis proposals/s", "value": value, "unit": "proposals/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
@@ -254,6 +256,8 @@ def run_ours(args, rank, world, local):
                                              "sasa_visits": float((c1 - c0)[2]), "proposals": 200},
                          "kernel_ms": k_ms, "traffic": None},
             "cpu_baseline": cpu,
+            "plain_gpu_path": plain,
+            "energy_force": ef,
         }
     if world > 1:
         import torch.distributed as dist
@@ -315,6 +319,73 @@ def cpu_baseline(ch, topo, T, args, budget_s=12.0):
     return {"value": n / dt, "unit": "proposals/s", "cores": 1, "kind": "reference",
             "sample": f"reference generate_ensemble(chain of {ch.n} atoms, 1 candidate, {n} proposals) in "
                       f"{dt:.1f} s; one chain runs on one thread (OpenMP spans candidates)"}
+
+
+def plain_gpu_baseline(ch, T, budget_s=8.0):
+    """The reference's own plain GPU path (src/physics_engine_cuda.cu built
+    unmodified for sm_100a into oracle/_ref): generate_ensemble on the same
+    chain, one candidate, on this GPU."""
+    import glob
+    hits = glob.glob(os.path.join(ROOT, "oracle", "_ref", "protein_physics_cuda*.so"))
+    cpu = glob.glob(os.path.join(ROOT, "oracle", "_ref", "protein_physics.*so"))
+    if not hits or not cpu:
+        return {"value": None, "unit": "proposals/s", "unavailable": "oracle/_ref/protein_physics_cuda not built"}
+    sys.path.insert(0, os.path.dirname(hits[0]))
+    import protein_physics as pp
+    import protein_physics_cuda as pc
+    R = pp.BondTopology()
+    R.build(ch.resnames, ch.atomnames, ch.res_idx)
+    P = [pc.Particle(*map(float, x), float(q), float(r), float(e)) for x, q, r, e in
+         zip(ch.xyz, ch.charge, ch.radius, ch.epsilon)]
+    eng = pc.PhysicsEngine()
+    t0 = time.perf_counter()
+    eng.generate_ensemble(P, R, 1, 5, T, 0.12)
+    dt5 = max(1e-3, time.perf_counter() - t0)
+    n = max(10, int(budget_s / dt5 * 5))
+    t0 = time.perf_counter()
+    eng.generate_ensemble(P, R, 1, n, T, 0.12)
+    dt = time.perf_counter() - t0
+    return {"value": n / dt, "unit": "proposals/s", "proposals": n, "seconds": dt,
+            "what": "reference protein_physics_cuda.generate_ensemble(chain, 1 candidate) on this B200 "
+                    "(physics_engine_cuda.cu built unmodified for sm_100a; host SASA and two H2D/D2H round "
+                    "trips per proposal)"}
+
+
+def energy_force_rate(system, steps=20):
+    """Full energy + analytic gradient evaluations per second on one system:
+    neighbor-list build, Born radii, energy terms and alma_forces per eval
+    (device events, inputs resident)."""
+    import torch
+    from protein_physics_b200.device import DeviceBatch
+    b = DeviceBatch([system], precision="mixed")
+    grad = torch.zeros((b.natoms, 4), dtype=torch.float64, device="cuda")
+    terms = torch.zeros((1, 5), dtype=torch.float64, device="cuda")
+
+    def ev():
+        b.nl_ready = False
+        b.build_nl(check=False)
+        b.energy_terms(recompute_born=True, out=terms)
+        b.forces(out=grad)
+
+    b.build_nl()
+    for _ in range(3):
+        ev()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        ev()
+    e1.record()
+    f0.record()
+    for _ in range(steps):
+        b.forces(out=grad)
+    f1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    return {"value": 1e3 / ms, "unit": "energy+force evals/s", "atoms": b.natoms, "ms_per_eval": ms,
+            "forces_ms": f0.elapsed_time(f1) / steps,
+            "what": "neighbor list + Born radii + energy terms + analytic dE/dx (alma_forces), mixed precision"}
 
 
 def run_reference(args, rank, world):
