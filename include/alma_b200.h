@@ -384,6 +384,20 @@ int alma_mc_run(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *nl, const A
 int alma_mc_after_rebuild(AlmaChainState *states, const double *terms, const uint8_t *sys_mask,
                           int32_t nsys, void *stream);
 
+/* Replica exchange between temperature neighbours (parallel tempering; the
+ * reference swaps landscape-segment states between Python threads,
+ * gui_main.py:1960-2013).  Every replica is a system of the batch;
+ * sys_of_temp[t] (device, a permutation) names the system at temperature
+ * slot t, slots in ascending temperature.  Round r tries the pairs
+ * (t, t+1), t ≡ r mod 2: swap with probability
+ * min(1, exp((1/T_a - 1/T_b)(E_a - E_b))), E = terms[5s+4] (fresh energies),
+ * T from mc_states.  A swap exchanges the systems' temperatures, cur_max and
+ * adaptation windows (and MALA beta / scale when mala_states is not NULL).
+ * attempts / accepts: device counters per slot pair [nsys].  nsys <= 2048. */
+int alma_replica_exchange(int32_t nsys, const double *terms, AlmaChainState *mc_states, AlmaMalaState *mala_states,
+                          int32_t *sys_of_temp, uint64_t seed, int64_t round, unsigned long long *attempts,
+                          unsigned long long *accepts, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
