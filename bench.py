@@ -1,7 +1,7 @@
 """Benchmark: Metropolis proposals/s of the B200 engine (and of the reference).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload single|batched]
+                    [--workload single|batched|globule|replica]
 
 Workload "single" (default): one synthetic 300-residue compact chain
 (~4,700 atoms, all-atom with hydrogens, seeded), torsion moves restricted to
@@ -12,6 +12,10 @@ Metropolis test.  One step = 1,000 proposals followed by a full energy
 recomputation (Born radii + energy).
 Workload "batched": 256 chains, 50-600 residues each (per-chain seeds),
 temperatures geometric over 280-400 K, one step = 100 proposals per chain.
+Workload "globule": a 1,000-residue chain: energy+force evals/s, 500
+torsion-space descent steps, then MALA proposals/s.
+Workload "replica": 16 replicas of a 4 x 1,000-residue chain, MALA:torsion
+1:3, replica exchange every 100 sweeps.
 
 value  = proposals/s of the whole job on the device (CUDA events, inputs
          resident), max over ranks;
@@ -428,6 +432,111 @@ def run_reference(args, rank, world):
             "e2e": {"value": value, "unit": "proposals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def _line(metric, value, unit, args, ms_per_step, config, clocks, launches, **extra):
+    out = {"metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f32 pair terms, f64 dE / accumulation", "data": "synthetic (seeded NeRF chains)",
+           "config": config, "clocks": clocks, "gpu_launches": int(launches)}
+    out.update(extra)
+    return out
+
+
+def run_globule(args):
+    """Differentiation workload: one 1,000-residue collapsed chain (~16k
+    atoms).  Reports energy+force evals/s, 500 descent steps, then the timed
+    MALA torsion proposals (step 0.5 deg, 300 K): one bench step = 10 MALA
+    proposals (each: all-bond move, list, Born, energy, forces, torsion
+    gradient, Metropolis-Hastings)."""
+    import numpy as np
+    import torch
+    from protein_physics_b200 import _lib, synth
+    from protein_physics_b200.device import DeviceBatch
+    from protein_physics_b200.topology import BondTopology, flatten
+    from protein_physics_b200.torsion import MALARunner, TorsionSpace, minimize
+    ch = synth.compact_chain(1000, seed=4)
+    T = BondTopology()
+    T.build(ch.resnames, ch.atomnames, ch.res_idx)
+    system = (ch.xyz, ch.charge, ch.radius, ch.epsilon, flatten(T))
+    ef = energy_force_rate(system)
+    b = DeviceBatch([system], precision="mixed")
+    ts = TorsionSpace(b)
+    torch.cuda.synchronize()
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g0.record()
+    hist, eta = minimize(b, steps=500, ts=ts)
+    g1.record()
+    torch.cuda.synchronize()
+    gd_ms = g0.elapsed_time(g1)
+    E = hist[:, 0].cpu().numpy()
+    R = MALARunner(b, 300.0 * KB, seed=2024, step=np.radians(0.5), ts=ts)
+    per = 10
+    for _ in range(args.warmup):
+        R.run(per)
+    st0 = R.state()
+    l0 = _lib.lib().alma_launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sampler = ClockSampler(0)
+    torch.cuda.synchronize()
+    with sampler:
+        e0.record()
+        for _ in range(args.steps):
+            R.run(per)
+        e1.record()
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    st1 = R.state()
+    n = int(st1["n_proposed"][0] - st0["n_proposed"][0])
+    acc = int(st1["n_accepted"][0] - st0["n_accepted"][0])
+    return _line("MALA torsion proposals/s", n / (ms * 1e-3), "proposals/s", args, ms / args.steps,
+                 {"workload": "1,000-residue collapsed chain, %d atoms, Rg %.1f A; 500 descent steps, then MALA "
+                              "(all %d rotatable bonds per proposal, step 0.5 deg, truncated drift), 300 K, "
+                              "10 proposals per step" % (ch.n, synth.radius_of_gyration(ch.xyz), ts.nrb),
+                  "atoms": ch.n, "mala_accept_rate": acc / max(1, n), "l2": "inputs > L2 (16k atoms x lists)"},
+                 sampler.summary(), _lib.lib().alma_launch_count() - l0,
+                 energy_force=ef,
+                 descent={"steps": 500, "ms": gd_ms, "steps_per_s": 500 / (gd_ms * 1e-3), "E_start": float(E[0]),
+                          "E_end": float(E[-1]), "unit": "kcal/mol"})
+
+
+def run_replica(args):
+    """Combined workload: 16 temperature replicas (300-450 K geometric) of a
+    4-domain chain (4 x 1,000 residues + 10-residue linkers); MALA and plain
+    torsion proposals 1:3, replica exchange every 100 sweeps.  One bench
+    step = one exchange interval (100 proposals per replica)."""
+    import torch
+    from protein_physics_b200 import _lib, synth
+    from protein_physics_b200.replica import ReplicaExchange, geometric_ladder
+    from protein_physics_b200.topology import BondTopology, flatten
+    ch = synth.multidomain_chain(4, 1000, 10, seed=11)
+    T = BondTopology()
+    T.build(ch.resnames, ch.atomnames, ch.res_idx)
+    F = flatten(T)
+    moveset = [k for k in range(F.nrb) if F.side_count[k] <= 0.25 * F.n]
+    RE = ReplicaExchange((ch.xyz, ch.charge, ch.radius, ch.epsilon, F), geometric_ladder(300, 450, 16), seed=9,
+                         moveset=moveset, minimize_steps=100)
+    for _ in range(args.warmup):
+        RE.interval(100)
+    torch.cuda.synchronize()
+    p0 = RE.proposals
+    l0 = _lib.lib().alma_launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sampler = ClockSampler(0)
+    with sampler:
+        e0.record()
+        for _ in range(args.steps):
+            RE.interval(100)
+        e1.record()
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    st = RE.stats()
+    return _line("Metropolis proposals/s (replica exchange)", (RE.proposals - p0) / (ms * 1e-3), "proposals/s", args,
+                 ms / args.steps,
+                 {"workload": "16 replicas x %d-atom 4-domain chain (%d atoms), T 300-450 K geometric, "
+                              "MALA:torsion 1:3, exchange every 100 sweeps" % (ch.n, 16 * ch.n),
+                  "atoms": 16 * ch.n, "l2": "inputs > L2"},
+                 sampler.summary(), _lib.lib().alma_launch_count() - l0, exchange=st)
+
+
 def run_profile_case(args):
     """Small case for ncu: the single-chain workload, 100 warm-up proposals,
     then exactly one mc_kernel launch of 200 proposals (no rebuild inside:
@@ -458,7 +567,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="single", choices=["single", "batched"])
+    ap.add_argument("--workload", default="single", choices=["single", "batched", "globule", "replica"])
     args = ap.parse_args()
     rank, world, local = rank_info()
     if args.profile:
@@ -466,6 +575,10 @@ def main():
         return
     if args.impl == "reference":
         out = run_reference(args, rank, world)
+    elif args.workload == "globule":
+        out = run_globule(args) if rank == 0 else None
+    elif args.workload == "replica":
+        out = run_replica(args) if rank == 0 else None
     else:
         out = run_ours(args, rank, world, local)
     if rank == 0 and out is not None:

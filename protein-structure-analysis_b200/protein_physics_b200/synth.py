@@ -290,7 +290,7 @@ class _Grid:
         return c
 
 
-def grow(sequence, draw_phipsi, rng, tries=12, heavy_cut=2.2, any_cut=1.3, back=3):
+def grow(sequence, draw_phipsi, rng, tries=12, heavy_cut=2.2, any_cut=1.3, back=3, budget_per_res=30, max_back=1000000):
     """Two-phase seeded build.
 
     1. Backbone (N CA C O H HA CB) residue by residue: (phi, psi of the
@@ -308,7 +308,7 @@ def grow(sequence, draw_phipsi, rng, tries=12, heavy_cut=2.2, any_cut=1.3, back=
     psi = np.zeros(n_res)
     frames = [None] * n_res
     bbpos = [None] * n_res
-    budget = 30 * n_res + 100
+    budget = budget_per_res * n_res + 100
     fails = np.zeros(n_res, int)
 
     def backbone_atoms(r, N, CA, C, ph, ps):
@@ -334,6 +334,8 @@ def grow(sequence, draw_phipsi, rng, tries=12, heavy_cut=2.2, any_cut=1.3, back=
             ps_prev = psi[r - 1] if r > 0 else 0.0
             if r > 0 and t >= tries // 2:
                 ps_prev = draw_phipsi(r - 1)[1]
+                if sequence[r] == "PRO":  # pre-proline residues sit in the PPII / beta basin
+                    ps_prev = float(rng.normal(145.0, 15.0))
             if r == 0:
                 N = np.zeros(3)
                 CA = np.array([bb["b_n_ca"], 0.0, 0.0])
@@ -346,6 +348,10 @@ def grow(sequence, draw_phipsi, rng, tries=12, heavy_cut=2.2, any_cut=1.3, back=
                 C = _place(pC, N, CA, bb["b_ca_c"], bb["a_n_ca_c"], ph)
             P, hv = backbone_atoms(r, N, CA, C, ph, ps)
             cost = grid.cost(P, hv, r, heavy_cut, any_cut) if r >= 2 else 0
+            if r >= 3 and ps_prev != psi[r - 1]:  # the redrawn psi moves residue r-1's O too: check it again
+                pN, pCA, pC = frames[r - 1]
+                Pp, hvp = backbone_atoms(r - 1, pN, pCA, pC, phi[r - 1], ps_prev)
+                cost += grid.cost(Pp, hvp, r - 1, heavy_cut, any_cut)
             if best is None or cost < best[0]:
                 best = (cost, ph, ps, ps_prev, P, hv, (N, CA, C))
             if cost == 0:
@@ -354,7 +360,7 @@ def grow(sequence, draw_phipsi, rng, tries=12, heavy_cut=2.2, any_cut=1.3, back=
         budget -= 1
         if cost > 0 and budget > 0 and r >= 2:
             fails[r] += 1
-            r -= min(r - 1, back * int(fails[r]))
+            r -= min(r - 1, back * min(int(fails[r]), max_back))
             continue
         if r > 0 and ps_prev != psi[r - 1]:
             psi[r - 1] = ps_prev
@@ -462,7 +468,7 @@ def _torsion(a, b, c, d):
     return math.degrees(math.atan2(np.linalg.norm(b2) * np.dot(b1, n2), np.dot(n1, n2)))
 
 
-def collapse(ch: Chain, seed, rg_target, moves=4000, k_rg=1.0, ca_clash=4.2, k_clash=5.0, temp=1.0, domains=None):
+def collapse(ch: Chain, seed, rg_target, moves=4000, k_rg=1.0, ca_clash=5.0, k_clash=50.0, temp=1.0, domains=None):
     """Seeded backbone collapse: torsion Monte Carlo on the C-alpha trace
     (phi/psi pivots) with the energy k_rg (Rg_CA - rg_target)^2 +
     k_clash sum (ca_clash - d)^2 over C-alpha pairs >= 3 residues apart, then
@@ -523,17 +529,14 @@ def collapse(ch: Chain, seed, rg_target, moves=4000, k_rg=1.0, ca_clash=4.2, k_c
     return pack_sidechains(ch.sequence, phi, psi, frames, bbpos, rng)
 
 
-def compact_chain(n_res, seed, rg_target=None, moves=None):
+def compact_chain(n_res, seed, rg_target=None, moves=4000):
     """A collapsed chain (default C-alpha Rg target 2.2 * n_res^0.38 Å).
-    Chains above 300 residues get 30 pivots per residue, a 20x stiffer Rg
-    restraint and twice the temperature (single pivots barely move long
-    chains otherwise); 1,000 residues end near Rg 39 Å for a 30 Å target."""
+    The pivot collapse reaches the target near 300 residues; longer chains
+    stay well above it (1,000 residues: Rg ~58 Å for a 30 Å target)."""
     ch = coil_chain(n_res, seed)
     if rg_target is None:
         rg_target = 2.2 * n_res ** 0.38
-    if n_res <= 300:
-        return collapse(ch, seed + 7919, rg_target, moves=moves or 4000)
-    return collapse(ch, seed + 7919, rg_target, moves=moves or 30 * n_res, k_rg=20.0, temp=2.0)
+    return collapse(ch, seed + 7919, rg_target, moves=moves)
 
 
 def multidomain_chain(n_domains, domain_res, linker_res, seed, moves=None):
@@ -543,5 +546,4 @@ def multidomain_chain(n_domains, domain_res, linker_res, seed, moves=None):
     n_res = n_domains * domain_res + (n_domains - 1) * linker_res
     ch = coil_chain(n_res, seed)
     doms = [(d * (domain_res + linker_res), d * (domain_res + linker_res) + domain_res) for d in range(n_domains)]
-    return collapse(ch, seed + 7919, 2.2 * domain_res ** 0.38, moves=moves or 10 * n_res, k_rg=20.0, temp=2.0,
-                    domains=doms)
+    return collapse(ch, seed + 7919, 2.2 * domain_res ** 0.38, moves=moves or 4 * n_res, domains=doms)

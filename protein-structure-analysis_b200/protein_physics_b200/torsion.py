@@ -116,13 +116,15 @@ class _Eval:
 
 
 def minimize(batch: DeviceBatch, steps=500, step0=0.02, grow=1.2, shrink=0.5, step_bounds=(1e-6, 0.3),
-             ts: TorsionSpace | None = None):
-    """Steepest descent in torsion space: every bond moves by
-    -eta_s * g_k / max_k |g_k| (the largest change is eta_s radians); a
-    step that lowers the energy is kept and eta_s grows, otherwise it is
-    undone and eta_s shrinks.  Runs on the device without host syncs
-    except the neighbor list's overflow check.  Returns the energies
-    [steps + 1, nsys] (device) and the final eta."""
+             clip=3.0, ts: TorsionSpace | None = None):
+    """Descent in torsion space along d = -clip(g, ±clip·mean|g|) (per
+    system; clip <= 0: plain steepest descent), scaled so the largest
+    torsion change is eta_s radians.  Clipping lets every bond caught in
+    a clash move at once instead of only the steepest one.  A step that
+    lowers the energy is kept and eta_s grows, otherwise it is undone and
+    eta_s shrinks.  Runs on the device without host syncs except the
+    neighbor list's overflow check.  Returns the energies [steps + 1,
+    nsys] (device) and the final eta."""
     ts = ts or TorsionSpace(batch)
     b = batch
     cur = _Eval(ts)()
@@ -137,10 +139,17 @@ def minimize(batch: DeviceBatch, steps=500, step0=0.02, grow=1.2, shrink=0.5, st
     for _ in range(int(steps)):
         if nb == 0:
             break
+        g = g_cur[:nb]
+        if clip > 0:
+            cnt = torch.zeros(b.nsys, dtype=torch.float64, device="cuda").index_add_(
+                0, ts.bond_sys, torch.ones_like(g))
+            mean = torch.zeros(b.nsys, dtype=torch.float64, device="cuda").index_add_(0, ts.bond_sys, g.abs())
+            lim = (clip * mean / torch.clamp(cnt, min=1.0))[ts.bond_sys]
+            g = torch.maximum(torch.minimum(g, lim), -lim)
         gmax = torch.zeros(b.nsys, dtype=torch.float64, device="cuda").scatter_reduce(
-            0, ts.bond_sys, g_cur[:nb].abs(), reduce="amax", include_self=True)
+            0, ts.bond_sys, g.abs(), reduce="amax", include_self=True)
         scale = eta / torch.clamp(gmax, min=1e-300)
-        delta = -(scale[ts.bond_sys] * g_cur[:nb])
+        delta = -(scale[ts.bond_sys] * g)
         xyz_old.copy_(b.xyz)
         born_old.copy_(b.born)
         ts.apply(delta)
