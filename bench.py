@@ -470,6 +470,7 @@ def run_globule(args):
     E = hist[:, 0].cpu().numpy()
     R = MALARunner(b, 300.0 * KB, seed=2024, step=np.radians(0.5), ts=ts)
     per = 10
+    R.run(300)  # step-scale adaptation (window 20) settles before the timed proposals
     for _ in range(args.warmup):
         R.run(per)
     st0 = R.state()
@@ -491,7 +492,8 @@ def run_globule(args):
                  {"workload": "1,000-residue collapsed chain, %d atoms, Rg %.1f A; 500 descent steps, then MALA "
                               "(all %d rotatable bonds per proposal, step 0.5 deg, truncated drift), 300 K, "
                               "10 proposals per step" % (ch.n, synth.radius_of_gyration(ch.xyz), ts.nrb),
-                  "atoms": ch.n, "mala_accept_rate": acc / max(1, n), "l2": "inputs > L2 (16k atoms x lists)"},
+                  "atoms": ch.n, "mala_accept_rate": acc / max(1, n), "mala_step_scale": float(st1["scale"][0]),
+                  "l2": "inputs > L2 (16k atoms x lists)"},
                  sampler.summary(), _lib.lib().alma_launch_count() - l0,
                  energy_force=ef,
                  descent={"steps": 500, "ms": gd_ms, "steps_per_s": 500 / (gd_ms * 1e-3), "E_start": float(E[0]),

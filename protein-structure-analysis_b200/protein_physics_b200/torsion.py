@@ -70,6 +70,11 @@ class TorsionSpace:
                               dtype=torch.uint8, device="cuda")
         self.bond_sys = torch.as_tensor(np.repeat(np.arange(batch.nsys), np.diff(batch.rb_off_h)),
                                         dtype=torch.int64, device="cuda")
+        cnt = np.diff(batch.rb_off_h)
+        self.max_nrb = int(max(1, cnt.max()))
+        self.nrb_sys = torch.as_tensor(cnt, dtype=torch.float64, device="cuda")
+        self.bond_local = torch.as_tensor(np.arange(self.nrb) - np.repeat(batch.rb_off_h[:-1], cnt),
+                                          dtype=torch.int64, device="cuda")
 
     def gtheta(self, grad, out=None, sys_mask=None):
         """dE/dθ [nrb] from a [natoms, 4] gradient."""
@@ -140,11 +145,11 @@ def minimize(batch: DeviceBatch, steps=500, step0=0.02, grow=1.2, shrink=0.5, st
         if nb == 0:
             break
         g = g_cur[:nb]
-        if clip > 0:
-            cnt = torch.zeros(b.nsys, dtype=torch.float64, device="cuda").index_add_(
-                0, ts.bond_sys, torch.ones_like(g))
-            mean = torch.zeros(b.nsys, dtype=torch.float64, device="cuda").index_add_(0, ts.bond_sys, g.abs())
-            lim = (clip * mean / torch.clamp(cnt, min=1.0))[ts.bond_sys]
+        if clip > 0:  # per-system mean |g|: rows of a padded [nsys, max bonds] matrix (no atomics)
+            pad = g.new_zeros((b.nsys, ts.max_nrb))
+            pad[ts.bond_sys, ts.bond_local] = g.abs()
+            mean = pad.sum(1) / torch.clamp(ts.nrb_sys, min=1.0)
+            lim = (clip * mean)[ts.bond_sys]
             g = torch.maximum(torch.minimum(g, lim), -lim)
         gmax = torch.zeros(b.nsys, dtype=torch.float64, device="cuda").scatter_reduce(
             0, ts.bond_sys, g.abs(), reduce="amax", include_self=True)
@@ -164,8 +169,8 @@ def minimize(batch: DeviceBatch, steps=500, step0=0.02, grow=1.2, shrink=0.5, st
     return torch.stack(hist), eta
 
 
-def mala_config(seed, drift_clip=1.0, tune_freq=0, target=(0.4, 0.7), scale_up=1.1, scale_down=0.9,
-                scale_bounds=(0.01, 4.0)):
+def mala_config(seed, drift_clip=1.0, tune_freq=20, target=(0.4, 0.7), scale_up=1.1, scale_down=0.8,
+                scale_bounds=(1e-3, 4.0)):
     """AlmaMalaConfig: truncated drift at ±drift_clip·σ; every tune_freq
     proposals (0: never) the step scale grows / shrinks when the window's
     acceptance leaves the target band (as the reference adapts cur_max,
@@ -190,7 +195,7 @@ class MALARunner:
     temperatures: kcal/mol per system (scalar broadcast)."""
 
     def __init__(self, batch: DeviceBatch, temperatures, seed, step=np.radians(0.5), sidechain_mult=2.5,
-                 drift_clip=1.0, tune_freq=0, ts: TorsionSpace | None = None):
+                 drift_clip=1.0, tune_freq=20, ts: TorsionSpace | None = None):
         self.b = batch
         self.ts = ts or TorsionSpace(batch)
         self.cfg = mala_config(seed, drift_clip=drift_clip, tune_freq=tune_freq)
