@@ -96,16 +96,17 @@ def _coil_chain(n_res, seed):
 
 def make_workload(kind, rank):
     from protein_physics_b200 import synth
+    from protein_physics_b200.dist import rank_seed
     from protein_physics_b200.topology import BondTopology, flatten
     if kind == "single":
-        chains = [synth.compact_chain(300, seed=2 + 1000 * rank)]
+        chains = [synth.compact_chain(300, seed=rank_seed(2, rank))]
         temps = [300.0 * KB]
     else:
         import multiprocessing as mp
         import numpy as np
-        rng = np.random.default_rng(3 + 1000 * rank)
+        rng = np.random.default_rng(rank_seed(3, rank))
         sizes = rng.integers(50, 601, size=256)
-        jobs = [(int(n), int(1000 * rank + k)) for k, n in enumerate(sizes)]
+        jobs = [(int(n), rank_seed(k, rank)) for k, n in enumerate(sizes)]
         # chain generation is host Python: spread it over the host cores
         with mp.get_context("spawn").Pool(min(32, os.cpu_count() or 1)) as pool:
             chains = pool.starmap(_coil_chain, jobs, chunksize=1)
@@ -129,8 +130,8 @@ def run_ours(args, rank, world, local):
     from protein_physics_b200.mc import MCRunner
     torch.cuda.set_device(local)
     if world > 1:
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+        from protein_physics_b200.dist import init
+        init("nccl", timeout_s=120)
     chains, systems, movesets, temps, topos = make_workload(args.workload, rank)
     per_step = 1000 if args.workload == "single" else 100
     batch = DeviceBatch(systems, precision="mixed")
@@ -179,15 +180,8 @@ def run_ours(args, rank, world, local):
     # mc kernel time alone (roofline): time one extra chunk without rebuilds
     dctr = (ctr1 - ctr0).sum(axis=0)
     ops = dctr[0] * OPS_PAIR + dctr[1] * OPS_HCT + dctr[2] * OPS_SASA
-    ms_max = ms
-    prop_total = proposals
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([ms, proposals], dtype=torch.float64, device="cuda")
-        tm = t.clone()
-        dist.all_reduce(tm[0:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(t[1:2], op=dist.ReduceOp.SUM)
-        ms_max, prop_total = float(tm[0]), float(t[1])
+    from protein_physics_b200.dist import reduce_timing
+    ms_max, prop_total = reduce_timing(ms, proposals, device="cuda")
     # isolated MC-kernel timing for the roofline: chunk without host rebuild logic
     ke0, ke1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     c0 = batch.move_counters().astype(np.float64).sum(axis=0)
