@@ -54,7 +54,7 @@ template <typename R, int NT, int CL>
 __global__ void __launch_bounds__(NT, 512 / NT) mc_kernel(MoveCtx C, MCConfigDev cfg,
                                                           AlmaChainState *__restrict__ states, int64_t step_limit) {
     __shared__ MoveDesc M;
-    __shared__ double sm[32];
+    __shared__ double sm[128];
     __shared__ double part[8];
     __shared__ AlmaChainState S;
     __shared__ double u[6];

@@ -38,7 +38,7 @@ __global__ void __launch_bounds__(MOVE_THREADS) move_dE_kernel(MoveCtx C, const 
                                                                const double *__restrict__ delta, int apply,
                                                                double *__restrict__ dE, double *__restrict__ dterms) {
     __shared__ MoveDesc M;
-    __shared__ double sm[32];
+    __shared__ double sm[128];
     __shared__ double part[8];
     const Team<1> T;
     const int s = blockIdx.x;

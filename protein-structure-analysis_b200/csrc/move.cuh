@@ -48,23 +48,44 @@ struct Team {
 };
 
 // Team-wide sums of K doubles; every thread of every CTA gets the same
-// totals (CTA partials combined in rank order through distributed shared
-// memory).  smem: >= 32 doubles; part: __shared__ double[K] per CTA.
+// totals.  One block reduction for all K values (warp trees, then warp 0
+// over the warp totals), then the CTA partials combined in rank order
+// through distributed shared memory.  smem: >= 32*K doubles; part:
+// __shared__ double[K] per CTA, double-buffered by the caller (proposal
+// parity) — no barrier follows the remote reads: the next write to the same
+// buffer is two proposals later, behind several team barriers, and every
+// caller passes a team barrier before it exits.
 template <int CL, int K>
 __device__ __forceinline__ void team_sum(const Team<CL> &T, double (&v)[K], double *smem, double *part) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (int)(blockDim.x >> 5);
 #pragma unroll
-    for (int k = 0; k < K; ++k) v[k] = block_sum(v[k], smem);
+    for (int k = 0; k < K; ++k) v[k] = warp_sum(v[k]);
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < K; ++k) smem[32 * k + wid] = v[k];
+    __syncthreads();
+    if (wid == 0) {
+        double t[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) t[k] = warp_sum(lane < nw ? smem[32 * k + lane] : 0.0);
+        if (lane == 0)
+#pragma unroll
+            for (int k = 0; k < K; ++k) part[k] = t[k];
+    }
     if constexpr (CL > 1) {
-        if (threadIdx.x == 0)
-            for (int k = 0; k < K; ++k) part[k] = v[k];
         T.sync();
         cg::cluster_group cl = cg::this_cluster();
+#pragma unroll
         for (int k = 0; k < K; ++k) v[k] = 0.0;
         for (int r = 0; r < CL; ++r) {
             const double *pr = cl.map_shared_rank(part, r);
+#pragma unroll
             for (int k = 0; k < K; ++k) v[k] += pr[k];
         }
-        T.sync();
+    } else {
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < K; ++k) v[k] = part[k];
     }
 }
 
@@ -311,7 +332,7 @@ __device__ __forceinline__ int member(const MoveDesc &M, const int32_t *side_idx
 }
 
 // Whole-CTA evaluation of a decoded, non-degenerate proposal of system s.
-// smem_d: >= 32 doubles; s_nAff: shared counter.  Leaves group/xyz_new/
+// smem_d: >= 128 doubles; s_nAff: shared counter.  Leaves group/xyz_new/
 // born_new set for the members (the caller commits or discards, then calls
 // move_clear).
 // New half-list Born radius of moved atom m from its segment sums
@@ -320,6 +341,53 @@ __device__ __forceinline__ double born_new_of(const MoveScratch &w, const double
     double sum = 0.0;
     for (int sg = 0; sg < wpr; ++sg) sum += w.hct_part[(size_t)m * MAX_WPR + sg];
     return 1.0 / fmax(1.0 / prm64[4 * (size_t)m + 1] - 0.5 * sum, 2.0);
+}
+
+// SASA change of affected atom k of system s (old and new geometry, the
+// ordered recurrence over its half row or its short half row); one warp.
+__device__ __forceinline__ void sasa_row(const MoveCtx &C, int s, int k, bool short_rows, double pi2, double pi4,
+                                         int lane, unsigned long long &nsasa) {
+    const AlmaBatch &b = C.b;
+    const MoveScratch &w = C.w;
+    const int a0 = b.atom_off[s];
+    const int i = w.affected[a0 + k];
+    const bool moved = w.group[i] != 0;
+    const double4 pio = ld_xyz(b.xyz, i), pin = moved ? ld_xyz(w.xyz_new, i) : pio;
+    const double rsi = b.prm64[4 * (size_t)i + 1] + C.P.probe_r;
+    const double cs = pi2 * rsi * rsi;
+    double sao = pi4 * rsi * rsi, san = sao;
+    const uint32_t *rc = short_rows ? C.nl.shalf_cols : C.nl.half_cols;
+    const int64_t beg = short_rows ? C.nl.shalf_ptr[i] : C.nl.half_ptr[i];
+    const int64_t end = beg + (short_rows ? C.nl.shalf_len[i] : C.nl.half_len[i]);
+    for (int64_t e0 = beg; e0 < end; e0 += 32) {
+        const int64_t e = e0 + lane;
+        double co = 0.0, cn = 0.0;
+        bool ho = false, hn = false;
+        if (e < end) {
+            const int j = (int)(rc[e] & ALMA_IDX_MASK);
+            const double rsj = b.prm64[4 * (size_t)j + 1] + C.P.probe_r;
+            const double dc = rsi + rsj;
+            const double4 pjo = ld_xyz(b.xyz, j);
+            const double ro = sqrt(d2_of(pio, pjo));
+            if (ro < dc) { ho = true; co = cs * ((dc - ro) / (2.0 * rsi)); }
+            const double4 pjn = w.group[j] ? ld_xyz(w.xyz_new, j) : pjo;
+            const double rn = sqrt(d2_of(pin, pjn));
+            if (rn < dc) { hn = true; cn = cs * ((dc - rn) / (2.0 * rsi)); }
+        }
+        unsigned mo = __ballot_sync(0xffffffffu, ho), mn = __ballot_sync(0xffffffffu, hn);
+        while (mo) {
+            const int l2 = __ffs(mo) - 1;
+            mo &= mo - 1;
+            sao -= fmin(sao * 0.85, __shfl_sync(0xffffffffu, co, l2));
+        }
+        while (mn) {
+            const int l2 = __ffs(mn) - 1;
+            mn &= mn - 1;
+            san -= fmin(san * 0.85, __shfl_sync(0xffffffffu, cn, l2));
+        }
+    }
+    if (lane == 0) w.dE_atom[2 * (size_t)i + 1] = C.P.gamma_sa * (fmax(0.0, san) - fmax(0.0, sao));
+    nsasa += 2ull * (unsigned long long)(end - beg);
 }
 
 // Whole-team evaluation of a decoded, non-degenerate proposal of system s.
@@ -396,19 +464,25 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
     // in i's half row and r < R*_i + R*_j + 2 probe; a pair whose distance
     // changes (rigid bodies differ) and is within reach before or after the
     // move changes the SASA of its lower atom only: mark that atom.
+    // Two task sets over the team's warps — Born segments of the moved rows,
+    // then mark segments — so the two kinds of work land on different warps.
     const int wid = T.gwarp(), nw = T.gwarps();
-    const int wpr = rows_wpr(nm, nw);
-    for (int64_t it = wid; it < nm * wpr; it += nw) {
-        const int64_t k = it / wpr;
-        const int seg = (int)(it % wpr);
+    const int wph = rows_wpr(2 * nm, nw);
+    const int64_t nhct = nm * wph;
+    for (int64_t it = wid; it < 2 * nhct; it += nw) {
+        const bool marking = it >= nhct;
+        const int64_t i2 = marking ? it - nhct : it;
+        const int64_t k = i2 / wph;
+        const int seg = (int)(i2 % wph);
         int g;
         const int m = member(M, t.side_idx, k, g);
         const double4 pm = ld_xyz(w.xyz_new, m);
+        if (!marking) {
         R qm, rm, em;
         prm_of<R>(b.prm, b.prm64, m, qm, rm, em);
         double sum = 0.0;
         const int64_t hb = C.nl.half_ptr[m], he = hb + C.nl.half_len[m];
-        for (int64_t e = hb + 32 * seg + lane; e < he; e += 32 * wpr) {
+        for (int64_t e = hb + 32 * seg + lane; e < he; e += 32 * wph) {
             const int j = (int)(C.nl.half_cols[e] & ALMA_IDX_MASK);
             R qj, rj, ej;
             prm_of<R>(b.prm, b.prm64, j, qj, rj, ej);
@@ -421,13 +495,15 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
             w.hct_part[(size_t)m * MAX_WPR + seg] = sum;
             if (seg == 0) atomicAdd(&w.ctr[4 * s + 1], (unsigned long long)C.nl.half_len[m]);
         }
+        continue;
+        }
         const double4 pmo = ld_xyz(b.xyz, m);
         const double rsm = b.prm64[4 * (size_t)m + 1] + C.P.probe_r;
         const int bm = w.body[m];
         const uint32_t *rc = short_rows ? C.nl.sfull_cols : C.nl.full_cols;
         const int64_t fb = short_rows ? C.nl.sfull_ptr[m] : C.nl.full_ptr[m];
         const int64_t fe = fb + (short_rows ? C.nl.sfull_len[m] : C.nl.full_len[m]);
-        for (int64_t e = fb + 32 * seg + lane; e < fe; e += 32 * wpr) {
+        for (int64_t e = fb + 32 * seg + lane; e < fe; e += 32 * wph) {
             const int j = (int)(rc[e] & ALMA_IDX_MASK);
             if (w.body[j] == bm) continue;
             const double dc = rsm + b.prm64[4 * (size_t)j + 1] + C.P.probe_r, dc2 = dc * dc;
@@ -448,23 +524,34 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
     // P3: cross pairs from the members' full rows (old and new geometry in
     // one pass), then SASA of the affected atoms (old and new, in row
     // order); boundary dihedrals and disulfides strided over threads.
-    for (int64_t it = wid; it < nm * wpr; it += nw) {
-        const int64_t k = it / wpr;
-        const int seg = (int)(it % wpr);
+    // One task space: cross-pair segments first, then the affected atoms'
+    // SASA, so the SASA rows go to warps without cross work.
+    const int naff = q[3];
+    const int wpc = rows_wpr(nm, nw - naff > nw / 2 ? nw - naff : nw / 2);
+    const int64_t ncross = nm * wpc;
+    const double pi4 = 4.0 * 3.14159265358979323846, pi2 = 2.0 * 3.14159265358979323846;
+    unsigned long long nsasa = 0;
+    for (int64_t it = wid; it < ncross + naff; it += nw) {
+        if (it >= ncross) {
+            sasa_row(C, s, (int)(it - ncross), short_rows, pi2, pi4, lane, nsasa);
+            continue;
+        }
+        const int64_t k = it / wpc;
+        const int seg = (int)(it % wpc);
         int g;
         const int m = member(M, t.side_idx, k, g);
         const int gm = g + 1;
         const double4 pmo = ld_xyz(b.xyz, m), pmn = ld_xyz(w.xyz_new, m);
         R qm, rm, em;
         prm_of<R>(b.prm, b.prm64, m, qm, rm, em);
-        const double bn = born_new_of(w, b.prm64, m, wpr);
+        const double bn = born_new_of(w, b.prm64, m, wph);
         if (seg == 0 && lane == 0) w.born_new[m] = bn;
         const R amo = (R)b.born[m], amn = (R)bn;
         const double rm64 = b.prm64[4 * (size_t)m + 1], em64 = b.prm64[4 * (size_t)m + 2];
         double acc = 0.0;
         int npair = 0;
         const int64_t fb = C.nl.full_ptr[m], fe = fb + C.nl.full_len[m];
-        for (int64_t e = fb + 32 * seg + lane; e < fe; e += 32 * wpr) {
+        for (int64_t e = fb + 32 * seg + lane; e < fe; e += 32 * wpc) {
             const uint32_t ent = C.nl.full_cols[e];
             if (ent & ALMA_EXCL_BIT) continue;
             const int j = (int)(ent & ALMA_IDX_MASK);
@@ -480,7 +567,7 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
             prm_of<R>(b.prm, b.prm64, j, qj, rj, ej);
             const R qp = qm * qj, sig = rm + rj, ep = em * ej;
             const R ajo = (R)b.born[j];
-            const R ajn = gj ? (R)born_new_of(w, b.prm64, j, wpr) : ajo;
+            const R ajn = gj ? (R)born_new_of(w, b.prm64, j, wph) : ajo;
             if (ino && inn) {
                 // FP64 sigma/epsilon only for contacts inside sigma (steep LJ)
                 double sig64 = (double)sig, eps64 = (double)ep;
@@ -501,51 +588,6 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
         if (lane == 0) {
             w.cross_part[(size_t)m * MAX_WPR + seg] = acc;
             atomicAdd(&w.ctr[4 * s + 0], (unsigned long long)npair);
-        }
-    }
-    const double pi4 = 4.0 * 3.14159265358979323846, pi2 = 2.0 * 3.14159265358979323846;
-    const int naff = q[3];
-    unsigned long long nsasa = 0;
-    for (int k = wid; k < naff; k += nw) {
-        {
-            const int i = w.affected[a0 + k];
-            const bool moved = w.group[i] != 0;
-            const double4 pio = ld_xyz(b.xyz, i), pin = moved ? ld_xyz(w.xyz_new, i) : pio;
-            const double rsi = b.prm64[4 * (size_t)i + 1] + C.P.probe_r;
-            const double cs = pi2 * rsi * rsi;
-            double sao = pi4 * rsi * rsi, san = sao;
-            const uint32_t *rc = short_rows ? C.nl.shalf_cols : C.nl.half_cols;
-            const int64_t beg = short_rows ? C.nl.shalf_ptr[i] : C.nl.half_ptr[i];
-            const int64_t end = beg + (short_rows ? C.nl.shalf_len[i] : C.nl.half_len[i]);
-            for (int64_t e0 = beg; e0 < end; e0 += 32) {
-                const int64_t e = e0 + lane;
-                double co = 0.0, cn = 0.0;
-                bool ho = false, hn = false;
-                if (e < end) {
-                    const int j = (int)(rc[e] & ALMA_IDX_MASK);
-                    const double rsj = b.prm64[4 * (size_t)j + 1] + C.P.probe_r;
-                    const double dc = rsi + rsj;
-                    const double4 pjo = ld_xyz(b.xyz, j);
-                    const double ro = sqrt(d2_of(pio, pjo));
-                    if (ro < dc) { ho = true; co = cs * ((dc - ro) / (2.0 * rsi)); }
-                    const double4 pjn = w.group[j] ? ld_xyz(w.xyz_new, j) : pjo;
-                    const double rn = sqrt(d2_of(pin, pjn));
-                    if (rn < dc) { hn = true; cn = cs * ((dc - rn) / (2.0 * rsi)); }
-                }
-                unsigned mo = __ballot_sync(0xffffffffu, ho), mn = __ballot_sync(0xffffffffu, hn);
-                while (mo) {
-                    const int l2 = __ffs(mo) - 1;
-                    mo &= mo - 1;
-                    sao -= fmin(sao * 0.85, __shfl_sync(0xffffffffu, co, l2));
-                }
-                while (mn) {
-                    const int l2 = __ffs(mn) - 1;
-                    mn &= mn - 1;
-                    san -= fmin(san * 0.85, __shfl_sync(0xffffffffu, cn, l2));
-                }
-            }
-            if (lane == 0) w.dE_atom[2 * (size_t)i + 1] = C.P.gamma_sa * (fmax(0.0, san) - fmax(0.0, sao));
-            nsasa += 2ull * (unsigned long long)(end - beg);
         }
     }
     if (lane == 0 && nsasa) atomicAdd(&w.ctr[4 * s + 2], nsasa);
@@ -586,7 +628,7 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
     for (int64_t k = tid; k < nm; k += nthr) {
         int g;
         const int m = member(M, t.side_idx, k, g);
-        for (int sg = 0; sg < wpr; ++sg) c += w.cross_part[(size_t)m * MAX_WPR + sg];
+        for (int sg = 0; sg < wpc; ++sg) c += w.cross_part[(size_t)m * MAX_WPR + sg];
     }
     for (int i = a0 + tid; i < a1; i += nthr) sa += w.dE_atom[2 * (size_t)i + 1];
     double v[4] = {c, sa, ddih, dss};
