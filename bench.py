@@ -141,8 +141,9 @@ def run_ours(args, rank, world, local):
     else:
         tuned = autotune(batch, temps, seed=777, policy=2, moveset=movesets,
                          proposals=300 if args.workload == "single" else 30)
+    tuned = (tuple(tuned) + (1,))[:3]
     runner = MCRunner(batch, temps, seed=12345 + rank, policy=2, cur_max0=0.12, moveset=movesets,
-                      cluster_size=tuned[0], threads=tuned[1])
+                      cluster_size=tuned[0], threads=tuned[1], spec_teams=tuned[2])
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     stream = torch.cuda.current_stream()
 
@@ -241,7 +242,7 @@ def run_ours(args, rank, world, local):
             "clocks": clocks,
             "gpu_launches": int(launches),
             "dE_error_vs_fp64": de_err,
-            "tuned": {"cluster_size": tuned[0], "threads_per_system": tuned[1]},
+            "tuned": {"cluster_size": tuned[0], "threads_per_system": tuned[1], "spec_teams": tuned[2]},
             "wall_s": t_wall,
             "e2e": {"value": e2e_val, "unit": "proposals/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "api": "PhysicsEngine.generate_ensemble(host particles, topology, 1, 1000)"},
@@ -556,7 +557,8 @@ def run_profile_case(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--profile", action="store_true", help="one mc_kernel launch on the single chain (for ncu)")
-    ap.add_argument("--config", default="", help="CL,NT: cluster size and CTA size instead of the autotuner")
+    ap.add_argument("--config", default="", help="CL,NT[,K]: cluster size, CTA size and speculative teams "
+                                                 "instead of the autotuner")
     ap.add_argument("--cluster", type=int, default=16)
     ap.add_argument("--threads", type=int, default=512)
     ap.add_argument("--gpus", type=int, default=1)

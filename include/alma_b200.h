@@ -50,7 +50,10 @@ enum {
     ALMA_ST_NL_OVERFLOW = 1,    /* neighbor list exceeded its capacity       */
     ALMA_ST_CELL_OVERFLOW = 2,  /* cell grid exceeded its capacity           */
     ALMA_ST_BAD_INDEX = 4,      /* topology index out of range               */
-    ALMA_ST_NONFINITE = 8       /* non-finite coordinate or energy seen      */
+    ALMA_ST_NONFINITE = 8,      /* non-finite coordinate or energy seen      */
+    ALMA_ST_SPEC_ABORT = 16     /* a team of a speculative MC round waited   */
+                                /* past its limit; the chain state of that   */
+                                /* launch was not written                    */
 };
 
 /* Energy-model constants (physics_engine.cpp:181-196).  Passed by value;
@@ -358,6 +361,13 @@ typedef struct {
     int32_t threads_per_system;   /* CTA size 256 or 512; 0 = by batch size  */
     int32_t cluster_size;         /* CTAs per system (1,2,4,8,16; 0 = 1): a  */
                                   /* thread-block cluster shares a proposal  */
+    int32_t spec_teams;           /* teams (clusters) per system, 0/1 = one: */
+                                  /* K > 1 evaluates the next K proposals at */
+                                  /* once against the committed state and    */
+                                  /* commits the first accepted one — the    */
+                                  /* same chain, up to K proposals per round */
+                                  /* (scratch: alma_mc_scratch_bytes)        */
+    int32_t pad;
 } AlmaMCConfig;
 
 /* Per-system chain state, device memory, one per system (72 bytes). */
@@ -372,6 +382,9 @@ typedef struct {
     int32_t parity;           /* scratch double-buffer selector (internal)   */
 } AlmaChainState;
 
+/* Scratch bytes of alma_mc_run for spec_teams = teams (zeroed once before
+ * first use; teams <= 1: alma_move_scratch_bytes(natoms)). */
+size_t alma_mc_scratch_bytes(int32_t natoms, int32_t nsys, int32_t teams);
 /* Runs proposals on every system until its state.step reaches step_limit
  * or it needs a neighbor-list rebuild (one CTA per system, no host sync).
  * The caller then rebuilds flagged systems (alma_nl_build + alma_born_radii

@@ -46,6 +46,66 @@ __device__ __forceinline__ int pick(double u, int n) {
     return k < n ? k : n - 1;
 }
 
+// One proposal of system s at RNG counter `step` (thread 0): the Philox
+// draws u[0..5], the move (kind, index, angles) under the policy and the
+// chain's cur_max, decoded into M.  Returns 1 when the proposal moves atoms
+// (0: no move in the set, or a degenerate move — only the step counts).
+__device__ int draw_proposal(const MoveCtx &C, const MCConfigDev &cfg, const AlmaChainState &S, int s, uint64_t step,
+                             int nrb, int ncp, int ncsp, int nset, MoveDesc &M, double *u) {
+    const uint64_t st = step;
+    const uint32_t k0 = (uint32_t)cfg.seed ^ (0x9E3779B9u * (uint32_t)(s + 1)), k1 = (uint32_t)(cfg.seed >> 32);
+    const Philox4 r0 = philox4x32_10((uint32_t)st, (uint32_t)(st >> 32), (uint32_t)s, 0u, k0, k1);
+    const Philox4 r1 = philox4x32_10((uint32_t)st, (uint32_t)(st >> 32), (uint32_t)s, 1u, k0, k1);
+    const Philox4 r2 = philox4x32_10((uint32_t)st, (uint32_t)(st >> 32), (uint32_t)s, 2u, k0, k1);
+    u[0] = u01_from(r0.v[0], r0.v[1]);
+    u[1] = u01_from(r0.v[2], r0.v[3]);
+    u[2] = u01_from(r1.v[0], r1.v[1]);
+    u[3] = u01_from(r1.v[2], r1.v[3]);
+    u[4] = u01_from(r2.v[0], r2.v[1]);
+    u[5] = u01_from(r2.v[2], r2.v[3]);
+    int kind = 0, idx = 0;
+    double delta[2] = {0.0, 0.0};
+    bool conc = false, crank = false;
+    if (cfg.policy == 1) {
+        conc = ncsp > 0 && u[0] < cfg.concerted_prob;
+        crank = !conc && ncp > 0 && u[4] < cfg.crank_prob;
+    } else if (cfg.policy == 0) {
+        crank = ncp > 0 && u[0] < cfg.crank_prob;
+    }
+    if (conc) {
+        kind = 2;
+        idx = pick(u[1], ncsp);
+        const int pi = C.t.csp_off[s] + idx;
+        const double sa = C.t.rb_scale[C.t.rb_off[s] + C.t.csp[2 * pi]];
+        const double sb = C.t.rb_scale[C.t.rb_off[s] + C.t.csp[2 * pi + 1]];
+        const double da = S.cur_max * cfg.sidechain_mult * sa, db = S.cur_max * cfg.sidechain_mult * sb;
+        delta[0] = -da + 2.0 * da * u[2];
+        delta[1] = -db + 2.0 * db * u[5];
+    } else if (crank) {
+        kind = 1;
+        idx = pick(u[1], ncp);
+        delta[0] = -S.cur_max + 2.0 * S.cur_max * u[2];
+    } else if (nset > 0) {
+        kind = 0;
+        const int q = pick(u[1], nset);
+        idx = cfg.moveset_off ? cfg.moveset[cfg.moveset_off[s] + q] : q;
+        const int k = C.t.rb_off[s] + idx;
+        const int bk = C.t.rb_kind[k];
+        double base = (bk == 0 || bk == 1) ? S.cur_max : S.cur_max * cfg.sidechain_mult;
+        base *= C.t.rb_scale[k];
+        delta[0] = -base + 2.0 * base * u[2];
+    } else {
+        kind = -1;
+    }
+    if (cfg.fixed_delta > 0.0) {
+        delta[0] = cfg.fixed_delta * (2.0 * u[2] - 1.0);
+        delta[1] = cfg.fixed_delta * (2.0 * u[5] - 1.0);
+    }
+    if (kind >= 0) decode_move(M, C.t, C.b.xyz, s, kind, idx, delta);
+    else M.degenerate = 1;
+    return !M.degenerate;
+}
+
 // One system per CTA (CL = 1) or per cluster of CL CTAs.  Every CTA of a
 // cluster keeps its own copy of the chain state and makes the same draws
 // and decisions (the ΔE totals are bit-identical in every CTA); rank 0
@@ -71,60 +131,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) mc_kernel(MoveCtx C, MCConfigDev
     const int ncsp = C.t.csp_off[s + 1] - C.t.csp_off[s];
     const int nset = cfg.moveset_off ? cfg.moveset_off[s + 1] - cfg.moveset_off[s] : nrb;
     while (S.step < step_limit && !S.need_rebuild) {
-        if (threadIdx.x == 0) {
-            const uint64_t st = (uint64_t)S.step;
-            const uint32_t k0 = (uint32_t)cfg.seed ^ (0x9E3779B9u * (uint32_t)(s + 1)), k1 = (uint32_t)(cfg.seed >> 32);
-            const Philox4 r0 = philox4x32_10((uint32_t)st, (uint32_t)(st >> 32), (uint32_t)s, 0u, k0, k1);
-            const Philox4 r1 = philox4x32_10((uint32_t)st, (uint32_t)(st >> 32), (uint32_t)s, 1u, k0, k1);
-            const Philox4 r2 = philox4x32_10((uint32_t)st, (uint32_t)(st >> 32), (uint32_t)s, 2u, k0, k1);
-            u[0] = u01_from(r0.v[0], r0.v[1]);
-            u[1] = u01_from(r0.v[2], r0.v[3]);
-            u[2] = u01_from(r1.v[0], r1.v[1]);
-            u[3] = u01_from(r1.v[2], r1.v[3]);
-            u[4] = u01_from(r2.v[0], r2.v[1]);
-            u[5] = u01_from(r2.v[2], r2.v[3]);
-            int kind = 0, idx = 0;
-            double delta[2] = {0.0, 0.0};
-            bool conc = false, crank = false;
-            if (cfg.policy == 1) {
-                conc = ncsp > 0 && u[0] < cfg.concerted_prob;
-                crank = !conc && ncp > 0 && u[4] < cfg.crank_prob;
-            } else if (cfg.policy == 0) {
-                crank = ncp > 0 && u[0] < cfg.crank_prob;
-            }
-            if (conc) {
-                kind = 2;
-                idx = pick(u[1], ncsp);
-                const int pi = C.t.csp_off[s] + idx;
-                const double sa = C.t.rb_scale[C.t.rb_off[s] + C.t.csp[2 * pi]];
-                const double sb = C.t.rb_scale[C.t.rb_off[s] + C.t.csp[2 * pi + 1]];
-                const double da = S.cur_max * cfg.sidechain_mult * sa, db = S.cur_max * cfg.sidechain_mult * sb;
-                delta[0] = -da + 2.0 * da * u[2];
-                delta[1] = -db + 2.0 * db * u[5];
-            } else if (crank) {
-                kind = 1;
-                idx = pick(u[1], ncp);
-                delta[0] = -S.cur_max + 2.0 * S.cur_max * u[2];
-            } else if (nset > 0) {
-                kind = 0;
-                const int q = pick(u[1], nset);
-                idx = cfg.moveset_off ? cfg.moveset[cfg.moveset_off[s] + q] : q;
-                const int k = C.t.rb_off[s] + idx;
-                const int bk = C.t.rb_kind[k];
-                double base = (bk == 0 || bk == 1) ? S.cur_max : S.cur_max * cfg.sidechain_mult;
-                base *= C.t.rb_scale[k];
-                delta[0] = -base + 2.0 * base * u[2];
-            } else {
-                kind = -1;
-            }
-            if (cfg.fixed_delta > 0.0) {
-                delta[0] = cfg.fixed_delta * (2.0 * u[2] - 1.0);
-                delta[1] = cfg.fixed_delta * (2.0 * u[5] - 1.0);
-            }
-            if (kind >= 0) decode_move(M, C.t, C.b.xyz, s, kind, idx, delta);
-            else M.degenerate = 1;
-            did_move = !M.degenerate;
-        }
+        if (threadIdx.x == 0) did_move = draw_proposal(C, cfg, S, s, (uint64_t)S.step, nrb, ncp, ncsp, nset, M, u);
         __syncthreads();
         if (!did_move) {
             if (threadIdx.x == 0) S.step++;
@@ -196,6 +203,245 @@ static cudaError_t launch_mc(const MoveCtx &C, const MCConfigDev &d, AlmaChainSt
     }
 }
 
+// ---- speculative rounds: K teams per system ---------------------------------
+//
+// A single chain fills 16 of 148 SMs, and most proposals are rejected; a
+// rejected proposal leaves the state as it was.  So K teams (clusters) of a
+// system evaluate the proposals of steps S.step + 0 .. S.step + K-1 at once,
+// all against the committed state, each in its own scratch; the first one
+// accepted is committed and the ones after it are dropped (their steps are
+// drawn again in the next round).  Every proposal uses the counter-keyed
+// draws of its own step, and a round never crosses a cur_max adaptation
+// boundary, so the chain is exactly the sequential kernel's.
+//
+// Teams meet twice per round (results, then the commit) at a barrier on a
+// per-system counter in global memory.  The counter is reset by the host
+// before the launch; a team that waits longer than SPEC_SPIN_LIMIT polls
+// (about a second) raises the abort flag and ALMA_ST_SPEC_ABORT, and every
+// team leaves its loop without writing the chain state.  The host launches
+// only when every cluster of the grid can be resident at once.
+constexpr int SPEC_MAX_TEAMS = 8;
+constexpr long long SPEC_SPIN_LIMIT = 1ll << 22;
+
+struct SpecSlot {
+    double dE;
+    int32_t flags;  // 1 proposal, 2 moves atoms, 4 accepted, 8 commit drifted
+    int32_t pad;
+};
+
+struct SpecRound {
+    unsigned int bar;
+    unsigned int abort;
+    int32_t pad[2];
+    SpecSlot slot[2][SPEC_MAX_TEAMS];
+};
+
+__device__ __forceinline__ MoveScratch scratch_at(const MoveScratch &w, size_t off) {
+    MoveScratch t = w;
+    auto sh = [off](auto *p) { return reinterpret_cast<decltype(p)>(reinterpret_cast<char *>(p) + off); };
+    t.group = sh(w.group);
+    t.body = sh(w.body);
+    t.mark = sh(w.mark);
+    t.xyz_new = sh(w.xyz_new);
+    t.born_new = sh(w.born_new);
+    t.dE_atom = sh(w.dE_atom);
+    t.hct_part = sh(w.hct_part);
+    t.cross_part = sh(w.cross_part);
+    t.affected = sh(w.affected);
+    t.queue = sh(w.queue);
+    t.drift = sh(w.drift);
+    return t;  // work counters and phase timers stay shared (team 0's)
+}
+
+__device__ __forceinline__ unsigned int ld_acquire(const unsigned int *p) {
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Cross-team barrier of one system; returns nonzero when the round aborts.
+template <int CL>
+__device__ __forceinline__ int spec_barrier(const Team<CL> &T, SpecRound *Rd, unsigned int target, int *abort_sh,
+                                            uint32_t *status) {
+    if (T.rank == 0 && threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(&Rd->bar, 1u);
+        int ab = 0;
+        long long it = 0;
+        while ((int)(ld_acquire(&Rd->bar) - target) < 0) {
+            if (*(volatile unsigned int *)&Rd->abort) {
+                ab = 1;
+                break;
+            }
+            __nanosleep(64);
+            if (++it > SPEC_SPIN_LIMIT) {
+                atomicExch(&Rd->abort, 1u);
+                set_status(status, ALMA_ST_SPEC_ABORT);
+                ab = 1;
+                break;
+            }
+        }
+        *abort_sh = ab;
+    }
+    T.sync();
+    int ab;
+    if constexpr (CL > 1) ab = *cg::this_cluster().map_shared_rank(abort_sh, 0);
+    else ab = *abort_sh;
+    __threadfence();  // the other teams' results and commit, seen by every thread
+    return ab;
+}
+
+template <typename R, int NT, int CL>
+__global__ void __launch_bounds__(NT, 512 / NT)
+mc_spec_kernel(MoveCtx C, MCConfigDev cfg, AlmaChainState *__restrict__ states, int64_t step_limit, int teams,
+               size_t team_stride, SpecRound *__restrict__ rounds) {
+    __shared__ MoveDesc M;
+    __shared__ double sm[128];
+    __shared__ double part[8];
+    __shared__ AlmaChainState S;
+    __shared__ double u[6];
+    __shared__ int did_move, acc_sh, a_sh, abort_sh;
+    const Team<CL> T;
+    const int grp = blockIdx.x / CL;
+    const int s = grp / teams, q = grp % teams;
+    MoveCtx Cq = C;
+    Cq.w = scratch_at(C.w, (size_t)q * team_stride);
+    SpecRound *Rd = rounds + s;
+    if (threadIdx.x == 0) {
+        S = states[s];
+        if (T.rank == 0) {
+            for (int k = 0; k < 8; ++k) Cq.w.queue[8 * s + k] = 0;  // this team's queues, both parities
+            Cq.w.drift[2 * s] = Cq.w.drift[2 * s + 1] = 0;
+        }
+    }
+    __syncthreads();
+    const bool rows_ok = system_within_skin(Cq, s);
+    if (threadIdx.x == 0 && !rows_ok && C.nl.ref_xyz && S.step < step_limit) S.need_rebuild = 1;
+    T.sync();
+    const int nrb = C.t.rb_off[s + 1] - C.t.rb_off[s];
+    const int ncp = C.t.cp_off[s + 1] - C.t.cp_off[s];
+    const int ncsp = C.t.csp_off[s + 1] - C.t.csp_off[s];
+    const int nset = cfg.moveset_off ? cfg.moveset_off[s + 1] - cfg.moveset_off[s] : nrb;
+    int parity = 0, aborted = 0;
+    unsigned int nbar = 0;
+    for (int round = 0; S.step < step_limit && !S.need_rebuild; ++round) {
+        // round size: within the step limit, no cur_max adaptation inside
+        int64_t keff = teams;
+        if (cfg.tune_freq > 0) keff = min(keff, (int64_t)(cfg.tune_freq - S.tot_win));
+        keff = min(keff, step_limit - S.step);
+        const int rp = round & 1;
+        if (threadIdx.x == 0)
+            did_move = q < keff ? draw_proposal(Cq, cfg, S, s, (uint64_t)(S.step + q), nrb, ncp, ncsp, nset, M, u) : 0;
+        __syncthreads();
+        double dE = 0.0;
+        int acc = 0;
+        if (did_move) {
+            const MoveResult r = move_eval<R, CL>(Cq, M, s, sm, part, parity, rows_ok, T);
+            if (threadIdx.x == 0) acc_sh = (r.dE < 0.0) || (u[3] < exp(-r.dE / S.temperature));
+            __syncthreads();
+            acc = acc_sh;
+            dE = r.dE;
+        }
+        if (T.rank == 0 && threadIdx.x == 0) {
+            Rd->slot[rp][q].dE = dE;
+            Rd->slot[rp][q].flags = (q < keff ? 1 : 0) | (did_move ? 2 : 0) | (acc ? 4 : 0);
+        }
+        nbar += (unsigned int)teams;
+        if (spec_barrier<CL>(T, Rd, nbar, &abort_sh, C.b.status)) {
+            aborted = 1;
+            break;
+        }
+        if (threadIdx.x == 0) {
+            int a = -1;
+            for (int i = 0; i < keff; ++i)
+                if (__ldcg(&Rd->slot[rp][i].flags) & 4) {
+                    a = i;
+                    break;
+                }
+            a_sh = a;
+        }
+        __syncthreads();
+        const int a = a_sh;
+        if (did_move) {
+            move_finish<CL>(Cq, M, s, q == a, parity, T);
+            T.sync();  // the commit and its drift flag, within the team
+            if (q == a && T.rank == 0 && threadIdx.x == 0 && Cq.w.drift[2 * s + parity])
+                Rd->slot[rp][q].flags |= 8;
+            parity ^= 1;
+        }
+        nbar += (unsigned int)teams;
+        if (spec_barrier<CL>(T, Rd, nbar, &abort_sh, C.b.status)) {
+            aborted = 1;
+            break;
+        }
+        if (threadIdx.x == 0) {  // the sequential kernel's bookkeeping, step by step
+            const int consumed = a >= 0 ? a + 1 : (int)keff;
+            for (int i = 0; i < consumed; ++i) {
+                const int f = __ldcg(&Rd->slot[rp][i].flags);
+                if (f & 2) {
+                    const int ai = i == a;
+                    S.n_proposed++;
+                    if (ai) {
+                        S.n_accepted++;
+                        S.energy += __ldcg(&Rd->slot[rp][i].dE);
+                        if (f & 8) S.need_rebuild = 1;
+                    }
+                    S.acc_win += ai;
+                    if (cfg.tune_freq > 0 && ++S.tot_win == cfg.tune_freq) {
+                        const double rate = (double)S.acc_win / (double)cfg.tune_freq;
+                        if (rate > cfg.target_hi) S.cur_max = fmin(cfg.angle_max, S.cur_max * cfg.scale_up);
+                        else if (rate < cfg.target_lo) S.cur_max = fmax(cfg.angle_min, S.cur_max * cfg.scale_down);
+                        S.acc_win = 0;
+                        S.tot_win = 0;
+                    }
+                }
+                S.step++;
+            }
+        }
+        __syncthreads();
+    }
+    // no CTA leaves while another of its cluster may still read its shared
+    // memory (the abort word of the last barrier)
+    T.sync();
+    // team 0 writes the state; its scratch parity is the clean one for a
+    // following one-team launch
+    if (threadIdx.x == 0 && T.rank == 0 && q == 0 && !aborted) {
+        S.parity = parity;
+        states[s] = S;
+    }
+}
+
+template <typename R, int NT, int CL>
+static cudaError_t launch_mc_spec(const MoveCtx &C, const MCConfigDev &d, AlmaChainState *states, int64_t step_limit,
+                                  int nsys, int teams, size_t team_stride, SpecRound *rounds, cudaStream_t st,
+                                  bool *fits) {
+    auto kfn = mc_spec_kernel<R, NT, CL>;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(nsys * teams * CL), 1, 1);
+    cfg.blockDim = dim3(NT, 1, 1);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = CL;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (CL > 8) {
+        cudaError_t e = cudaFuncSetAttribute(kfn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        if (e != cudaSuccess) return e;
+    }
+    int max_clusters = 0;
+    cudaError_t e = cudaOccupancyMaxActiveClusters(&max_clusters, kfn, &cfg);
+    if (e != cudaSuccess) return e;
+    // every team of every system must be resident at once (they wait on
+    // one another); otherwise decline
+    *fits = max_clusters >= nsys * teams;
+    if (!*fits) return cudaSuccess;
+    return cudaLaunchKernelEx(&cfg, kfn, C, d, states, step_limit, teams, team_stride, rounds);
+}
+
 // After a rebuild of the flagged systems: energy <- fresh total, flag
 // cleared, rebuild counted.
 __global__ void mc_after_rebuild_kernel(AlmaChainState *__restrict__ states, const double *__restrict__ terms,
@@ -210,6 +456,8 @@ __global__ void mc_after_rebuild_kernel(AlmaChainState *__restrict__ states, con
 }  // namespace alma
 
 using namespace alma;
+
+static size_t align_up256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 int alma_check_move_args(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *nl, const AlmaParams *p,
                          void *scratch, const char *who);
@@ -255,7 +503,35 @@ extern "C" int alma_mc_run(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *
     if (nt != 256 && nt != 512) return alma_set_error(ALMA_EINVAL, "alma_mc_run: threads_per_system must be 0, 256 or 512");
     if (cl != 1 && cl != 2 && cl != 4 && cl != 8 && cl != 16)
         return alma_set_error(ALMA_EINVAL, "alma_mc_run: cluster_size must be 1, 2, 4, 8 or 16");
+    const int teams = cfg->spec_teams <= 1 ? 1 : cfg->spec_teams;
+    if (teams > SPEC_MAX_TEAMS) return alma_set_error(ALMA_EINVAL, "alma_mc_run: spec_teams must be <= %d", SPEC_MAX_TEAMS);
     cudaError_t e = cudaSuccess;
+    if (teams > 1) {
+        const size_t stride = align_up256(alma_move_scratch_bytes(b->natoms));
+        SpecRound *rounds = (SpecRound *)((char *)scratch + (size_t)teams * stride);
+        ALMA_CUDA_TRY(cudaMemsetAsync(rounds, 0, sizeof(SpecRound) * (size_t)b->nsys, st));
+        bool fits = true;
+#define ALMA_SPEC_CASE(R, NT)                                                                                   \
+    switch (cl) {                                                                                               \
+        case 1: e = launch_mc_spec<R, NT, 1>(C, d, states, step_limit, b->nsys, teams, stride, rounds, st, &fits); break;   \
+        case 2: e = launch_mc_spec<R, NT, 2>(C, d, states, step_limit, b->nsys, teams, stride, rounds, st, &fits); break;   \
+        case 4: e = launch_mc_spec<R, NT, 4>(C, d, states, step_limit, b->nsys, teams, stride, rounds, st, &fits); break;   \
+        case 8: e = launch_mc_spec<R, NT, 8>(C, d, states, step_limit, b->nsys, teams, stride, rounds, st, &fits); break;   \
+        default: e = launch_mc_spec<R, NT, 16>(C, d, states, step_limit, b->nsys, teams, stride, rounds, st, &fits); break; \
+    }
+        if (prec == ALMA_PREC_FP64) {
+            if (nt == 512) { ALMA_SPEC_CASE(double, 512) } else { ALMA_SPEC_CASE(double, 256) }
+        } else {
+            if (nt == 512) { ALMA_SPEC_CASE(float, 512) } else { ALMA_SPEC_CASE(float, 256) }
+        }
+#undef ALMA_SPEC_CASE
+        if (e != cudaSuccess) return alma_cuda_error(e, "alma_mc_run launch");
+        if (!fits)
+            return alma_set_error(ALMA_EINVAL, "alma_mc_run: %d systems x %d teams x %d CTAs cannot all be resident",
+                                  b->nsys, teams, cl);
+        ALMA_LAUNCH_CHECK("alma_mc_run");
+        return ALMA_OK;
+    }
 #define ALMA_MC_CASE(R, NT)                                                              \
     switch (cl) {                                                                        \
         case 1: e = launch_mc<R, NT, 1>(C, d, states, step_limit, b->nsys, st); break;   \
@@ -273,6 +549,12 @@ extern "C" int alma_mc_run(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *
     if (e != cudaSuccess) return alma_cuda_error(e, "alma_mc_run launch");
     ALMA_LAUNCH_CHECK("alma_mc_run");
     return ALMA_OK;
+}
+
+extern "C" size_t alma_mc_scratch_bytes(int32_t natoms, int32_t nsys, int32_t teams) {
+    if (teams <= 1) return alma_move_scratch_bytes(natoms);
+    return (size_t)teams * align_up256(alma_move_scratch_bytes(natoms)) +
+           align_up256(sizeof(SpecRound) * (size_t)(nsys > 0 ? nsys : 1));
 }
 
 extern "C" int alma_mc_after_rebuild(AlmaChainState *states, const double *terms, const uint8_t *sys_mask,

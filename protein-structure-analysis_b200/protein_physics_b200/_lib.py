@@ -27,6 +27,7 @@ ST_NL_OVERFLOW = 1
 ST_CELL_OVERFLOW = 2
 ST_BAD_INDEX = 4
 ST_NONFINITE = 8
+ST_SPEC_ABORT = 16
 
 _p = C.c_void_p
 _i32 = C.c_int32
@@ -71,7 +72,8 @@ class AlmaMCConfig(C.Structure):
                 ("angle_max", C.c_double), ("angle_min", C.c_double),
                 ("sidechain_mult", C.c_double), ("crank_prob", C.c_double),
                 ("concerted_prob", C.c_double), ("fixed_delta", C.c_double),
-                ("moveset_off", _p), ("moveset", _p), ("threads_per_system", _i32), ("cluster_size", _i32)]
+                ("moveset_off", _p), ("moveset", _p), ("threads_per_system", _i32), ("cluster_size", _i32),
+                ("spec_teams", _i32), ("pad", _i32)]
 
 
 class AlmaChainState(C.Structure):
@@ -129,6 +131,8 @@ def lib():
     L.alma_nl_workspace_bytes.argtypes = [_i32, _i32, _i64]
     L.alma_move_scratch_bytes.restype = C.c_size_t
     L.alma_move_scratch_bytes.argtypes = [_i32]
+    L.alma_mc_scratch_bytes.restype = C.c_size_t
+    L.alma_mc_scratch_bytes.argtypes = [_i32, _i32, _i32]
     L.alma_topo_sides.argtypes = [_i32, _p, _p, _i32, _p, _p, _p, _i64]
     L.alma_topo_sides_compact.argtypes = [_i32, _p, _p, _i32, _p, _p, _p, _p, _p, _p, _i64]
     L.alma_nl_build.argtypes = [_p, _p, _p, _p, _p, _p, _i64, _p]

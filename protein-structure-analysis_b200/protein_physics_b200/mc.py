@@ -64,7 +64,7 @@ class MCRunner:
     initial max angle (the reference's max_angle)."""
 
     def __init__(self, batch: DeviceBatch, temperatures, seed, policy=0, cur_max0=0.12, tune_freq=200,
-                 fixed_delta=0.0, moveset=None, cluster_size=None, threads=0):
+                 fixed_delta=0.0, moveset=None, cluster_size=None, threads=0, spec_teams=1):
         self.b = batch
         self.L = batch.L
         self._keep = []
@@ -79,6 +79,13 @@ class MCRunner:
                     break
         self.cfg.cluster_size = int(cluster_size)
         self.cfg.threads_per_system = int(threads)
+        self.cfg.spec_teams = int(spec_teams)
+        if spec_teams > 1:
+            # K teams per system: K move scratches plus the round buffers, team 0
+            # at the start (the batch's counters and single-move calls use it)
+            need = self.L.alma_mc_scratch_bytes(batch.natoms, batch.nsys, int(spec_teams))
+            if batch.scratch.numel() < need:
+                batch.scratch = torch.zeros(need, dtype=torch.uint8, device="cuda")
         T = np.broadcast_to(np.asarray(temperatures, np.float64), (batch.nsys,)).copy()
         if np.any(T <= 0):
             raise ValueError("temperature must be positive")
@@ -116,6 +123,8 @@ class MCRunner:
         while True:
             self.launch(step_limit)
             st = self.state()
+            if self.cfg.spec_teams > 1 and int(self.b.status.item()) & _lib.ST_SPEC_ABORT:
+                raise RuntimeError("alma_mc_run: a speculative round timed out (teams not co-resident)")
             need = st["need_rebuild"] != 0
             if need.any():
                 mask = torch.from_numpy(need.astype(np.uint8)).to("cuda")
@@ -131,7 +140,7 @@ _TUNED = {}
 
 
 def autotune(batch, temperatures, seed, policy=0, moveset=None, proposals=200, candidates=None):
-    """Picks (cluster_size, threads_per_system) for this batch shape by
+    """Picks (cluster_size, threads_per_system, spec_teams) for this batch shape by
     timing `proposals` proposals per candidate on a scratch copy of the
     batch state; cached per (systems, atom-count bucket, policy)."""
     import time
@@ -140,26 +149,29 @@ def autotune(batch, temperatures, seed, policy=0, moveset=None, proposals=200, c
     if key in _TUNED:
         return _TUNED[key]
     if candidates is None:
-        candidates = [(cl, nt) for cl in (1, 2, 4, 8, 16) for nt in (256, 512) if batch.nsys * cl <= 2 * sms]
+        candidates = [(cl, nt, 1) for cl in (1, 2, 4, 8, 16) for nt in (256, 512) if batch.nsys * cl <= 2 * sms]
+        candidates += [(cl, 512, k) for cl in (8, 16) for k in (2, 4, 8) if batch.nsys * cl * k <= sms]
     xyz0, born0 = batch.xyz.clone(), batch.born.clone()
     best, best_rate = None, -1.0
-    for cl, nt in candidates:
+    for cand in candidates:
+        cl, nt, k = (tuple(cand) + (1,))[:3]
         try:
-            R = MCRunner(batch, temperatures, seed, policy=policy, moveset=moveset, cluster_size=cl, threads=nt)
+            R = MCRunner(batch, temperatures, seed, policy=policy, moveset=moveset, cluster_size=cl, threads=nt,
+                         spec_teams=k)
             R.run(max(10, proposals // 10))
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             R.run(proposals)
             torch.cuda.synchronize()
             rate = proposals * batch.nsys / (time.perf_counter() - t0)
-        except RuntimeError:
+        except (RuntimeError, ValueError):
             continue
         finally:
             batch.xyz.copy_(xyz0)
             batch.born.copy_(born0)
             batch.nl_ready = False
         if rate > best_rate:
-            best, best_rate = (cl, nt), rate
+            best, best_rate = (cl, nt, k), rate
     batch.build_nl()
     _TUNED[key] = best
     return best

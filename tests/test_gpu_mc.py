@@ -21,12 +21,14 @@ def _setup(name):
     return g, flatten(g.topology())
 
 
-def _gpu_run(g, F, nsys, seed, steps, precision="fp64", policy=0, fixed_delta=0.0, moveset=None, T=0.6):
+def _gpu_run(g, F, nsys, seed, steps, precision="fp64", policy=0, fixed_delta=0.0, moveset=None, T=0.6,
+             cluster_size=None, spec_teams=1):
     from protein_physics_b200.device import DeviceBatch
     from protein_physics_b200.mc import MCRunner
     b = DeviceBatch([(g["xyz"], g["q"], g["r"], g["eps"], F)] * nsys, precision=precision)
     R = MCRunner(b, T, seed, policy=policy, fixed_delta=fixed_delta,
-                 moveset=[moveset] * nsys if moveset is not None else None)
+                 moveset=[moveset] * nsys if moveset is not None else None, cluster_size=cluster_size,
+                 spec_teams=spec_teams)
     st = R.run_to(steps)
     return b, st
 
@@ -107,3 +109,40 @@ def test_dropin_mc_entry_points():
         eng.generate_ensemble(P, T, 0, 1)
     with pytest.raises(ValueError):
         eng.run_landscape_trajectory(P, T, 1, 0)
+
+
+# ---- speculative rounds (spec_teams > 1): the same chain as one team --------
+@pytest.mark.parametrize("teams,cl", [(2, 4), (4, 8), (8, 16)])
+def test_spec_teams_match_oracle(teams, cl):
+    g, F = _setup("insulin")
+    b, st = _gpu_run(g, F, 1, 11, 300, cluster_size=cl, spec_teams=teams)  # crosses a tune window (200)
+    x_o, st_o, _ = _oracle_run(g, F, 11, 300)
+    assert st["step"][0] == 300
+    assert st["n_accepted"][0] == st_o["n_accepted"]
+    assert st["n_proposed"][0] == st_o["n_proposed"]
+    assert st["cur_max"][0] == pytest.approx(st_o["cur_max"], rel=1e-15)
+    np.testing.assert_allclose(b.coords(0), x_o, rtol=0, atol=1e-9)
+
+
+def test_spec_teams_rebuild_and_batched():
+    g, F = _setup("insulin")
+    b, st = _gpu_run(g, F, 1, 5, 120, fixed_delta=0.6, T=50.0, cluster_size=4, spec_teams=4)
+    x_o, st_o, _ = _oracle_run(g, F, 5, 120, fixed_delta=0.6, T=50.0)
+    assert st_o["n_rebuild"] > 0 and st["n_rebuild"][0] == st_o["n_rebuild"]
+    np.testing.assert_allclose(b.coords(0), x_o, rtol=0, atol=1e-8)
+    b, st = _gpu_run(g, F, 3, 21, 80, cluster_size=2, spec_teams=4)
+    for s in range(3):
+        x_o, st_o, _ = _oracle_run(g, F, 21, 80, sys_index=s)
+        assert st["n_accepted"][s] == st_o["n_accepted"]
+        np.testing.assert_allclose(b.coords(s), x_o, rtol=0, atol=1e-9)
+
+
+def test_spec_teams_bitwise_equal_one_team():
+    """Mixed precision: K teams and one team (same cluster size) give the
+    same chain bit for bit, energy sum included."""
+    g, F = _setup("xq8")
+    b1, st1 = _gpu_run(g, F, 1, 3, 400, precision="mixed", cluster_size=8, spec_teams=1)
+    b4, st4 = _gpu_run(g, F, 1, 3, 400, precision="mixed", cluster_size=8, spec_teams=4)
+    assert np.array_equal(b1.coords(0), b4.coords(0))
+    for k in ("energy", "cur_max", "n_accepted", "n_proposed", "n_rebuild", "step"):
+        assert st1[k][0] == st4[k][0], k
