@@ -112,7 +112,7 @@ def test_dropin_mc_entry_points():
 
 
 # ---- speculative rounds (spec_teams > 1): the same chain as one team --------
-@pytest.mark.parametrize("teams,cl", [(2, 4), (4, 8), (8, 16)])
+@pytest.mark.parametrize("teams,cl", [(2, 4), (4, 8), (8, 8), (4, 16)])
 def test_spec_teams_match_oracle(teams, cl):
     g, F = _setup("insulin")
     b, st = _gpu_run(g, F, 1, 11, 300, cluster_size=cl, spec_teams=teams)  # crosses a tune window (200)
