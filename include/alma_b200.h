@@ -78,6 +78,13 @@ typedef struct {
     const double *prm64;     /* [natoms*4] charge, R*, epsilon, (unused)    */
     double *born;            /* [natoms] effective Born radii               */
     uint32_t *status;        /* [1] sticky ALMA_ST_* flags                  */
+    double *sasa;            /* [natoms] optional (NULL: none): per-atom    */
+                             /* SASA term gamma*max(0, sa_i) of the current */
+                             /* coordinates.  alma_energy fills it for the  */
+                             /* systems it evaluates; the move / MC kernels */
+                             /* read it instead of recomputing the old SASA */
+                             /* and keep it current on commit.  Pass NULL   */
+                             /* after changing coordinates any other way.   */
 } AlmaBatch;
 
 /* Flat topology of the batch (physics_engine.cpp:3746-3841 exports). */

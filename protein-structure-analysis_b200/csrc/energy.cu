@@ -68,7 +68,8 @@ __global__ void pair_sasa_kernel(DevParams P, int natoms, const int32_t *__restr
                                  const float *__restrict__ prm,
                                  const double *__restrict__ prm64, const double *__restrict__ born,
                                  const int64_t *__restrict__ half_ptr, const int32_t *__restrict__ half_len,
-                                 const uint32_t *__restrict__ half_cols, int use_excl, double *__restrict__ atom_e) {
+                                 const uint32_t *__restrict__ half_cols, int use_excl, double *__restrict__ atom_e,
+                                 double *__restrict__ sasa_out) {
     const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     if (i >= natoms) return;
@@ -114,6 +115,7 @@ __global__ void pair_sasa_kernel(DevParams P, int natoms, const int32_t *__restr
     if (lane == 0) {
         atom_e[2 * (size_t)i] = e;
         atom_e[2 * (size_t)i + 1] = P.gamma_sa * fmax(0.0, sa);
+        if (sasa_out) sasa_out[i] = atom_e[2 * (size_t)i + 1];
     }
 }
 
@@ -212,10 +214,10 @@ extern "C" int alma_energy(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *
         const int use_excl = t != nullptr;
         if (prec == ALMA_PREC_FP64)
             pair_sasa_kernel<double><<<nb, wpb * 32, 0, st>>>(P, b->natoms, b->atom_off, b->nsys, sys_mask, b->xyz, b->prm, b->prm64, b->born,
-                                                              nl->half_ptr, nl->half_len, nl->half_cols, use_excl, atom_e);
+                                                              nl->half_ptr, nl->half_len, nl->half_cols, use_excl, atom_e, b->sasa);
         else
             pair_sasa_kernel<float><<<nb, wpb * 32, 0, st>>>(P, b->natoms, b->atom_off, b->nsys, sys_mask, b->xyz, b->prm, b->prm64, b->born,
-                                                             nl->half_ptr, nl->half_len, nl->half_cols, use_excl, atom_e);
+                                                             nl->half_ptr, nl->half_len, nl->half_cols, use_excl, atom_e, b->sasa);
     }
     AlmaTopo tt;
     if (t) tt = *t;

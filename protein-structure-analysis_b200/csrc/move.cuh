@@ -113,7 +113,8 @@ struct MoveScratch {
                         // the atom to `affected`)
     double *xyz_new;    // [natoms*4]
     double *born_new;   // [natoms]
-    double *dE_atom;    // [natoms*2] per-atom ΔE slots (SASA in [2i+1])
+    double *dE_atom;    // [natoms*2] SASA of affected atoms: new term [2i],
+                        // change [2i+1]
     double *hct_part;   // [natoms*MAX_WPR] per-segment hct sums of moved atoms
     double *cross_part; // [natoms*MAX_WPR] per-segment cross-pair ΔE of moved atoms
     int32_t *affected;  // [natoms] atoms whose SASA is recomputed (per-system
@@ -343,8 +344,12 @@ __device__ __forceinline__ double born_new_of(const MoveScratch &w, const double
     return 1.0 / fmax(1.0 / prm64[4 * (size_t)m + 1] - 0.5 * sum, 2.0);
 }
 
-// SASA change of affected atom k of system s (old and new geometry, the
-// ordered recurrence over its half row or its short half row); one warp.
+// SASA change of affected atom k of system s: the ordered recurrence over
+// its half row (or short half row) at the new geometry, minus the old term
+// — read from b.sasa when the batch carries the current per-atom terms,
+// else recomputed at the old geometry in the same pass (the two
+// recurrences are independent and interleaved).  The new term goes to
+// dE_atom[2i] for the commit, the change to dE_atom[2i+1].  One warp.
 __device__ __forceinline__ void sasa_row(const MoveCtx &C, int s, int k, bool short_rows, double pi2, double pi4,
                                          int lane, unsigned long long &nsasa) {
     const AlmaBatch &b = C.b;
@@ -352,6 +357,7 @@ __device__ __forceinline__ void sasa_row(const MoveCtx &C, int s, int k, bool sh
     const int a0 = b.atom_off[s];
     const int i = w.affected[a0 + k];
     const bool moved = w.group[i] != 0;
+    const bool cached = b.sasa != nullptr;
     const double4 pio = ld_xyz(b.xyz, i), pin = moved ? ld_xyz(w.xyz_new, i) : pio;
     const double rsi = b.prm64[4 * (size_t)i + 1] + C.P.probe_r;
     const double cs = pi2 * rsi * rsi;
@@ -368,26 +374,31 @@ __device__ __forceinline__ void sasa_row(const MoveCtx &C, int s, int k, bool sh
             const double rsj = b.prm64[4 * (size_t)j + 1] + C.P.probe_r;
             const double dc = rsi + rsj;
             const double4 pjo = ld_xyz(b.xyz, j);
-            const double ro = sqrt(d2_of(pio, pjo));
-            if (ro < dc) { ho = true; co = cs * ((dc - ro) / (2.0 * rsi)); }
+            if (!cached) {
+                const double ro = sqrt(d2_of(pio, pjo));
+                if (ro < dc) { ho = true; co = cs * ((dc - ro) / (2.0 * rsi)); }
+            }
             const double4 pjn = w.group[j] ? ld_xyz(w.xyz_new, j) : pjo;
             const double rn = sqrt(d2_of(pin, pjn));
             if (rn < dc) { hn = true; cn = cs * ((dc - rn) / (2.0 * rsi)); }
         }
         unsigned mo = __ballot_sync(0xffffffffu, ho), mn = __ballot_sync(0xffffffffu, hn);
-        while (mo) {
-            const int l2 = __ffs(mo) - 1;
+        while (mo | mn) {  // independent recurrences: interleaved
+            const int lo2 = mo ? __ffs(mo) - 1 : 0, ln2 = mn ? __ffs(mn) - 1 : 0;
+            const double c_o = __shfl_sync(0xffffffffu, co, lo2), c_n = __shfl_sync(0xffffffffu, cn, ln2);
+            if (mo) sao -= fmin(sao * 0.85, c_o);
+            if (mn) san -= fmin(san * 0.85, c_n);
             mo &= mo - 1;
-            sao -= fmin(sao * 0.85, __shfl_sync(0xffffffffu, co, l2));
-        }
-        while (mn) {
-            const int l2 = __ffs(mn) - 1;
             mn &= mn - 1;
-            san -= fmin(san * 0.85, __shfl_sync(0xffffffffu, cn, l2));
         }
     }
-    if (lane == 0) w.dE_atom[2 * (size_t)i + 1] = C.P.gamma_sa * (fmax(0.0, san) - fmax(0.0, sao));
-    nsasa += 2ull * (unsigned long long)(end - beg);
+    if (lane == 0) {
+        const double tn = C.P.gamma_sa * fmax(0.0, san);
+        const double to = cached ? b.sasa[i] : C.P.gamma_sa * fmax(0.0, sao);
+        w.dE_atom[2 * (size_t)i] = tn;
+        w.dE_atom[2 * (size_t)i + 1] = tn - to;
+    }
+    nsasa += (cached ? 1ull : 2ull) * (unsigned long long)(end - beg);
 }
 
 // Whole-team evaluation of a decoded, non-degenerate proposal of system s.
@@ -524,10 +535,11 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
     // P3: cross pairs from the members' full rows (old and new geometry in
     // one pass), then SASA of the affected atoms (old and new, in row
     // order); boundary dihedrals and disulfides strided over threads.
-    // One task space: cross-pair segments first, then the affected atoms'
-    // SASA, so the SASA rows go to warps without cross work.
+    // One task space: cross-pair segments first (every warp gets one when
+    // the rows allow), then the affected atoms' SASA, which wraps round onto
+    // the warps: a short SASA row after a half row beats a full row.
     const int naff = q[3];
-    const int wpc = rows_wpr(nm, nw - naff > nw / 2 ? nw - naff : nw / 2);
+    const int wpc = rows_wpr(nm, nw);
     const int64_t ncross = nm * wpc;
     const double pi4 = 4.0 * 3.14159265358979323846, pi2 = 2.0 * 3.14159265358979323846;
     unsigned long long nsasa = 0;
@@ -670,7 +682,9 @@ __device__ inline void move_finish(const MoveCtx &C, const MoveDesc &M, int s, i
     const int naff = w.queue[8 * s + 4 * parity + 3];
     for (int k = tid; k < naff; k += nthr) {
         const int i = w.affected[a0 + k];
+        if (accept && C.b.sasa) C.b.sasa[i] = w.dE_atom[2 * (size_t)i];  // the committed atoms' SASA terms
         w.mark[i] = 0;
+        w.dE_atom[2 * (size_t)i] = 0.0;
         w.dE_atom[2 * (size_t)i + 1] = 0.0;
     }
     if (__any_sync(0xffffffffu, drift) && (threadIdx.x & 31) == 0) atomicOr(&w.drift[2 * s + parity], 1);

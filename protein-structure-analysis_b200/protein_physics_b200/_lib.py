@@ -43,7 +43,7 @@ class AlmaParams(C.Structure):
 
 class AlmaBatch(C.Structure):
     _fields_ = [("nsys", _i32), ("natoms", _i32), ("atom_off", _p), ("xyz", _p), ("prm", _p),
-                ("prm64", _p), ("born", _p), ("status", _p)]
+                ("prm64", _p), ("born", _p), ("status", _p), ("sasa", _p)]
 
 
 class AlmaTopo(C.Structure):

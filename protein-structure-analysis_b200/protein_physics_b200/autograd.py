@@ -29,6 +29,7 @@ class _Energy(torch.autograd.Function):
             raise ValueError(f"xyz must be a CUDA float64 tensor of shape ({n}, 3)")
         batch.xyz[:n, :3].copy_(xyz.detach())
         batch.nl_ready = False
+        batch.invalidate_sasa()
         batch.build_nl()
         terms = batch.energy_terms(recompute_born=True)
         if ctx.needs_input_grad[0]:

@@ -99,6 +99,11 @@ class DeviceBatch:
         self.prm64 = _t(prm64, torch.float64)
         self.prm = self.prm64.to(torch.float32)
         self.born = torch.zeros(max(n, 1), dtype=torch.float64, device=_DEV)
+        # per-atom SASA terms of the current coordinates (AlmaBatch.sasa):
+        # filled by energy_terms, kept current by the move kernels; any other
+        # change of the coordinates must call invalidate_sasa()
+        self.sasa = torch.zeros(max(n, 1), dtype=torch.float64, device=_DEV)
+        self.sasa_valid = False
         self.status = torch.zeros(1, dtype=torch.int32, device=_DEV)
         self.atom_off = _t(self.atom_off_h, torch.int32)
         self.atom_sys = torch.as_tensor(np.repeat(np.arange(self.nsys), np.diff(self.atom_off_h)), dtype=torch.int64,
@@ -193,7 +198,12 @@ class DeviceBatch:
         b.nsys, b.natoms = self.nsys, self.natoms
         b.atom_off, b.xyz, b.prm, b.prm64 = _ptr(self.atom_off), _ptr(self.xyz), _ptr(self.prm), _ptr(self.prm64)
         b.born, b.status = _ptr(self.born), _ptr(self.status)
+        b.sasa = _ptr(self.sasa) if self.sasa_valid else None
         return b
+
+    def invalidate_sasa(self):
+        """Coordinates changed outside the energy / move kernels."""
+        self.sasa_valid = False
 
     # ---- neighbor list ---------------------------------------------------------
     def _alloc_nl(self, need):
@@ -310,10 +320,13 @@ class DeviceBatch:
         if getattr(self, "_atom_e", None) is None:
             self._atom_e = torch.zeros((max(self.natoms, 1), 2), dtype=torch.float64, device=_DEV)
         b, t, nl = self.batch_s, self.topo_s, self.nl_s
+        b.sasa = _ptr(self.sasa)  # refreshed for the evaluated systems
         _lib.check(self.L.alma_energy(C.byref(b), C.byref(t) if self.use_topo else None, C.byref(nl),
                                       C.byref(self.params), self.prec,
                                       _ptr(sys_mask) if sys_mask is not None else None, _ptr(self._atom_e),
                                       _ptr(terms), self._sp()), "alma_energy")
+        if sys_mask is None:
+            self.sasa_valid = True
         return terms
 
     def forces(self, sys_mask=None, out=None, recompute_born=False):

@@ -170,6 +170,7 @@ def autotune(batch, temperatures, seed, policy=0, moveset=None, proposals=200, c
             batch.xyz.copy_(xyz0)
             batch.born.copy_(born0)
             batch.nl_ready = False
+            batch.invalidate_sasa()
         if rate > best_rate:
             best, best_rate = (cl, nt, k), rate
     batch.build_nl()

@@ -92,6 +92,7 @@ class TorsionSpace:
                                              _ptr(delta), _ptr(sys_mask) if sys_mask is not None else None,
                                              _ptr(self.ws), b._sp()), "alma_torsion_apply")
         b.nl_ready = False
+        b.invalidate_sasa()
 
     def select(self, accept, xyz_old, born_old, g_new=None, g_cur=None, sys_mask=None):
         b = self.b
@@ -99,6 +100,7 @@ class TorsionSpace:
                                            _ptr(sys_mask) if sys_mask is not None else None, _ptr(xyz_old),
                                            _ptr(born_old), _ptr(g_new), _ptr(g_cur), b._sp()),
                    "alma_mala_select")
+        b.invalidate_sasa()  # rejected systems went back to their saved coordinates
 
 
 class _Eval:
