@@ -116,6 +116,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) mc_kernel(MoveCtx C, MCConfigDev
     __shared__ MoveDesc M;
     __shared__ double sm[128];
     __shared__ double part[8];
+    __shared__ CrossCand cq[(NT / 32) * CROSS_BUF];
     __shared__ AlmaChainState S;
     __shared__ double u[6];
     __shared__ int did_move, accept;
@@ -139,7 +140,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) mc_kernel(MoveCtx C, MCConfigDev
             continue;
         }
         const int parity = S.parity & 1;
-        const MoveResult r = move_eval<R, CL>(C, M, s, sm, part, parity, rows_ok, T);
+        const MoveResult r = move_eval<R, CL>(C, M, s, sm, part, cq, parity, rows_ok, T);
         if (threadIdx.x == 0) accept = (r.dE < 0.0) || (u[3] < exp(-r.dE / S.temperature));
         __syncthreads();
         const int acc = accept;
@@ -298,6 +299,7 @@ mc_spec_kernel(MoveCtx C, MCConfigDev cfg, AlmaChainState *__restrict__ states, 
     __shared__ MoveDesc M;
     __shared__ double sm[128];
     __shared__ double part[8];
+    __shared__ CrossCand cq[(NT / 32) * CROSS_BUF];
     __shared__ AlmaChainState S;
     __shared__ double u[6];
     __shared__ int did_move, acc_sh, a_sh, abort_sh;
@@ -336,7 +338,7 @@ mc_spec_kernel(MoveCtx C, MCConfigDev cfg, AlmaChainState *__restrict__ states, 
         double dE = 0.0;
         int acc = 0;
         if (did_move) {
-            const MoveResult r = move_eval<R, CL>(Cq, M, s, sm, part, parity, rows_ok, T);
+            const MoveResult r = move_eval<R, CL>(Cq, M, s, sm, part, cq, parity, rows_ok, T);
             if (threadIdx.x == 0) acc_sh = (r.dE < 0.0) || (u[3] < exp(-r.dE / S.temperature));
             __syncthreads();
             acc = acc_sh;

@@ -40,6 +40,7 @@ __global__ void __launch_bounds__(MOVE_THREADS) move_dE_kernel(MoveCtx C, const 
     __shared__ MoveDesc M;
     __shared__ double sm[128];
     __shared__ double part[8];
+    __shared__ CrossCand cq[(MOVE_THREADS / 32) * CROSS_BUF];
     const Team<1> T;
     const int s = blockIdx.x;
     const int k = kind[s];
@@ -59,7 +60,7 @@ __global__ void __launch_bounds__(MOVE_THREADS) move_dE_kernel(MoveCtx C, const 
         return;
     }
     const bool rows_ok = system_within_skin(C, s);
-    const MoveResult r = move_eval<R, 1>(C, M, s, sm, part, 0, rows_ok, T);
+    const MoveResult r = move_eval<R, 1>(C, M, s, sm, part, cq, 0, rows_ok, T);
     if (threadIdx.x == 0) {
         dE[s] = r.dE;
         dterms[4 * (size_t)s + 0] = r.dcross;

@@ -90,6 +90,15 @@ __device__ __forceinline__ void team_sum(const Team<CL> &T, double (&v)[K], doub
 }
 
 constexpr int MOVE_THREADS = 512;
+
+// A cross pair that passed the filters (different groups, not excluded,
+// within the cutoff before or after): packed per warp so the pair
+// arithmetic runs with every lane busy.
+struct CrossCand {
+    double r2o, r2n;
+    int j, gj;
+};
+constexpr int CROSS_BUF = 64;  // per warp: < 32 waiting + one batch of 32
 constexpr int MAX_ROT = 2;
 constexpr int MAX_WPR = 4;  // warps per moved-atom row, at most
 
@@ -419,7 +428,7 @@ __device__ __forceinline__ void sasa_row(const MoveCtx &C, int s, int k, bool sh
 // the result is the same bit for bit.
 template <typename R, int CL>
 __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, double *smem_d, double *part,
-                                int parity, bool rows_ok, const Team<CL> &T) {
+                                CrossCand *cq, int parity, bool rows_ok, const Team<CL> &T) {
     const AlmaBatch &b = C.b;
     const AlmaTopo &t = C.t;
     const MoveScratch &w = C.w;
@@ -563,17 +572,16 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
         double acc = 0.0;
         int npair = 0;
         const int64_t fb = C.nl.full_ptr[m], fe = fb + C.nl.full_len[m];
-        for (int64_t e = fb + 32 * seg + lane; e < fe; e += 32 * wpc) {
-            const uint32_t ent = C.nl.full_cols[e];
-            if (ent & ALMA_EXCL_BIT) continue;
-            const int j = (int)(ent & ALMA_IDX_MASK);
-            const int gj = w.group[j];
-            if (gj == gm || (gj != 0 && j < m)) continue;
-            const double4 pjo = ld_xyz(b.xyz, j);
-            const double4 pjn = gj ? ld_xyz(w.xyz_new, j) : pjo;
-            const double r2o = d2_of(pmo, pjo), r2n = d2_of(pmn, pjn);
+        // Pass 1 walks the row with loads and distance tests only and packs
+        // the pairs within the cutoff into the warp's buffer (about one entry
+        // in eight); the pair arithmetic then runs on full batches of 32.
+        CrossCand *buf = cq + (threadIdx.x >> 5) * CROSS_BUF;
+        auto evaluate = [&](int cnt) {
+            if (lane >= cnt) return;
+            const CrossCand c = buf[lane];
+            const int j = c.j, gj = c.gj;
+            const double r2o = c.r2o, r2n = c.r2n;
             const bool ino = r2o <= C.P.pair_cut2, inn = r2n <= C.P.pair_cut2;
-            if (!ino && !inn) continue;
             npair += (int)ino + (int)inn;
             R qj, rj, ej;
             prm_of<R>(b.prm, b.prm64, j, qj, rj, ej);
@@ -594,7 +602,41 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
             } else {
                 acc += (double)pair_energy<R>(C.P, (R)r2n, qp, sig, ep, amn, ajn);
             }
+        };
+        const unsigned below = (1u << lane) - 1u;
+        int nq = 0;
+        for (int64_t e0 = fb + 32 * seg; e0 < fe; e0 += 32 * wpc) {
+            const int64_t e = e0 + lane;
+            bool pass = false;
+            CrossCand c;
+            if (e < fe) {
+                const uint32_t ent = C.nl.full_cols[e];
+                if (!(ent & ALMA_EXCL_BIT)) {
+                    c.j = (int)(ent & ALMA_IDX_MASK);
+                    c.gj = w.group[c.j];
+                    if (!(c.gj == gm || (c.gj != 0 && c.j < m))) {
+                        const double4 pjo = ld_xyz(b.xyz, c.j);
+                        const double4 pjn = c.gj ? ld_xyz(w.xyz_new, c.j) : pjo;
+                        c.r2o = d2_of(pmo, pjo);
+                        c.r2n = d2_of(pmn, pjn);
+                        pass = c.r2o <= C.P.pair_cut2 || c.r2n <= C.P.pair_cut2;
+                    }
+                }
+            }
+            const unsigned msk = __ballot_sync(0xffffffffu, pass);
+            if (pass) buf[nq + __popc(msk & below)] = c;
+            nq += __popc(msk);
+            __syncwarp();
+            if (nq >= 32) {
+                evaluate(32);
+                __syncwarp();
+                if (lane < nq - 32) buf[lane] = buf[32 + lane];
+                nq -= 32;
+                __syncwarp();
+            }
         }
+        if (nq > 0) evaluate(nq);
+        __syncwarp();  // the buffer is free for this warp's next task
         acc = warp_sum(acc);
         npair = __reduce_add_sync(0xffffffffu, npair);
         if (lane == 0) {
