@@ -535,28 +535,39 @@ def run_replica(args):
 
 
 def run_profile_case(args):
-    """Small case for ncu: the single-chain workload, 100 warm-up proposals,
-    then exactly one mc_kernel launch of 200 proposals (no rebuild inside:
-    the launch stops at the first drift flag)."""
+    """Small cases for ncu.  "mc": the single-chain workload, 100 warm-up
+    proposals, then exactly one mc launch of up to 200 proposals (it stops
+    at the first drift flag); --config CL,NT[,K] picks the launch shape.
+    "forces": the same chain, one energy evaluation and one alma_forces
+    call (4 gradient kernels)."""
     import torch
     from protein_physics_b200.device import DeviceBatch
     from protein_physics_b200.mc import MCRunner
     chains, systems, movesets, temps, topos = make_workload("single", 0)
     batch = DeviceBatch(systems, precision="mixed")
-    runner = MCRunner(batch, temps, seed=12345, policy=2, moveset=movesets, cluster_size=args.cluster,
-                      threads=args.threads)
+    if args.profile == "forces":
+        batch.energy_terms()
+        g = batch.forces()
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_case": "forces", "atoms": chains[0].n, "grad_norm": float(g.norm())}))
+        return
+    cl, nt, k = (tuple(int(v) for v in args.config.split(",")) + (1,))[:3] if args.config else \
+        (args.cluster, args.threads, 1)
+    runner = MCRunner(batch, temps, seed=12345, policy=2, moveset=movesets, cluster_size=cl, threads=nt,
+                      spec_teams=k)
     runner.run(100)
     lim = int(runner.state()["step"].max()) + 200
     runner.launch(lim)
     torch.cuda.synchronize()
     st = runner.state()
     print(json.dumps({"profile_case": "single chain", "atoms": chains[0].n, "steps_done": int(st["step"][0]),
-                      "cluster": args.cluster, "threads": args.threads}))
+                      "cluster": cl, "threads": nt, "spec_teams": k}))
 
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--profile", action="store_true", help="one mc_kernel launch on the single chain (for ncu)")
+    ap.add_argument("--profile", nargs="?", const="mc", default=None, choices=["mc", "forces"],
+                    help="a small case for ncu: one mc launch (mc) or one gradient evaluation (forces)")
     ap.add_argument("--config", default="", help="CL,NT[,K]: cluster size, CTA size and speculative teams "
                                                  "instead of the autotuner")
     ap.add_argument("--cluster", type=int, default=16)
