@@ -246,7 +246,9 @@ def run_ours(args, rank, world, local):
             "wall_s": t_wall,
             "e2e": {"value": e2e_val, "unit": "proposals/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "api": "PhysicsEngine.generate_ensemble(host particles, topology, 1, 1000)"},
-            "roofline": {"bound": "fp32", "kernel": "mc_kernel<float>", "achieved": achieved / 1e12,
+            "roofline": {"bound": "fp32", "kernel": ("mc_spec_kernel<float,%d,%d> x %d teams" % (tuned[1], tuned[0], tuned[2])
+                                                    if tuned[2] > 1 else "mc_kernel<float,%d,%d>" % (tuned[1], tuned[0])),
+                         "achieved": achieved / 1e12,
                          "peak": FP32_PEAK_NOMINAL / 1e12, "unit": "TOP/s (FP32+MUFU ops)",
                          "frac": achieved / FP32_PEAK_NOMINAL,
                          "peak_source": "nominal 148 SM x 128 FP32 lanes x 2 x 1965 MHz (no measured FP32 peak "

@@ -64,7 +64,7 @@ class MCRunner:
     initial max angle (the reference's max_angle)."""
 
     def __init__(self, batch: DeviceBatch, temperatures, seed, policy=0, cur_max0=0.12, tune_freq=200,
-                 fixed_delta=0.0, moveset=None, cluster_size=None, threads=0, spec_teams=1):
+                 fixed_delta=0.0, moveset=None, cluster_size=None, threads=0, spec_teams=None):
         self.b = batch
         self.L = batch.L
         self._keep = []
@@ -79,6 +79,9 @@ class MCRunner:
                     break
         self.cfg.cluster_size = int(cluster_size)
         self.cfg.threads_per_system = int(threads)
+        if spec_teams is None:  # a second team per system when the SMs are there
+            sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+            spec_teams = 2 if 2 * batch.nsys * int(cluster_size) <= sms else 1
         self.cfg.spec_teams = int(spec_teams)
         if spec_teams > 1:
             # K teams per system: K move scratches plus the round buffers, team 0
@@ -110,9 +113,12 @@ class MCRunner:
 
     def launch(self, step_limit):
         b = self.b
-        _lib.check(self.L.alma_mc_run(C.byref(b.batch_s), C.byref(b.topo_s), C.byref(b.nl_s), C.byref(b.params),
-                                      b.prec, _ptr(b.scratch), C.byref(self.cfg), _ptr(self.states),
-                                      int(step_limit), b._sp()), "alma_mc_run")
+        rc = self.L.alma_mc_run(C.byref(b.batch_s), C.byref(b.topo_s), C.byref(b.nl_s), C.byref(b.params), b.prec,
+                                _ptr(b.scratch), C.byref(self.cfg), _ptr(self.states), int(step_limit), b._sp())
+        if rc == _lib.ALMA_EINVAL and self.cfg.spec_teams > 1 and b"resident" in self.L.alma_last_error():
+            self.cfg.spec_teams = 1  # the teams would not all fit on the GPU at once: one team
+            return self.launch(step_limit)
+        _lib.check(rc, "alma_mc_run")
 
     def run(self, nsteps):
         """Advances every system by nsteps proposals (host loop over rebuilds)."""
