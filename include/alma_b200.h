@@ -375,6 +375,12 @@ typedef struct {
                                   /* same chain, up to K proposals per round */
                                   /* (scratch: alma_mc_scratch_bytes)        */
     int32_t pad;
+    void *rebuild_ws;             /* optional device workspace of             */
+                                  /* alma_mc_rebuild_bytes(natoms, nsys): a   */
+                                  /* chain that drifts rebuilds its neighbor  */
+                                  /* list, Born radii and energy inside the   */
+                                  /* persistent kernel (one team); NULL: it   */
+                                  /* stops for the host rebuild                */
 } AlmaMCConfig;
 
 /* Per-system chain state, device memory, one per system (72 bytes). */
@@ -389,6 +395,8 @@ typedef struct {
     int32_t parity;           /* scratch double-buffer selector (internal)   */
 } AlmaChainState;
 
+/* Workspace bytes of the in-kernel rebuild (AlmaMCConfig.rebuild_ws). */
+size_t alma_mc_rebuild_bytes(int32_t natoms, int32_t nsys);
 /* Scratch bytes of alma_mc_run for spec_teams = teams (zeroed once before
  * first use; teams <= 1: alma_move_scratch_bytes(natoms)). */
 size_t alma_mc_scratch_bytes(int32_t natoms, int32_t nsys, int32_t teams);

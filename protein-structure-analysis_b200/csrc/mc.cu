@@ -29,9 +29,28 @@
 //          changed since the list was built) flags it before its first
 //          proposal, as the reference's check at the top of every step
 //          would.
+#include "alma_block_scan.cuh"
+#include "energy_core.cuh"
 #include "move.cuh"
+#include "nl_core.cuh"
 
 namespace alma {
+
+// Device workspace of the in-kernel rebuild (per system: a cell region of
+// REB_CELLS_PER_ATOM cells per atom + REB_CELLS_PAD; per atom: cell, slot,
+// four row counts, two energy slots).
+constexpr int REB_CELLS_PER_ATOM = 16;
+constexpr int REB_CELLS_PAD = 256;
+
+struct RebuildWS {
+    int32_t *ccount;     // [cells] counts, then fill counters
+    int64_t *cstart;     // [cells] absolute starts in cell_atoms
+    int32_t *cell_of;    // [natoms]
+    int32_t *cell_atoms; // [natoms]
+    int32_t *cnt;        // [4*natoms] row counts (kind-major); kind 0 doubles as sort scratch
+    double *atom_e;      // [2*natoms]
+    int32_t *flag;       // [nsys] rows fit their regions
+};
 
 struct MCConfigDev {
     uint64_t seed;
@@ -39,6 +58,8 @@ struct MCConfigDev {
     double target_lo, target_hi, scale_up, scale_down, angle_max, angle_min;
     double sidechain_mult, crank_prob, concerted_prob, fixed_delta;
     const int32_t *moveset_off, *moveset;
+    RebuildWS rw;         // rw.ccount == nullptr: no in-kernel rebuild
+    double reach_pad;     // short-row reach padding of the list build
 };
 
 __device__ __forceinline__ int pick(double u, int n) {
@@ -106,6 +127,211 @@ __device__ int draw_proposal(const MoveCtx &C, const MCConfigDev &cfg, const Alm
     return !M.degenerate;
 }
 
+// Team-wide min (lo) and max (hi) of three coordinates.  rsm: >= 192
+// doubles of shared memory; rpart: __shared__ double[6] per CTA.
+template <int CL>
+__device__ void team_minmax3(const Team<CL> &T, double (&lo)[3], double (&hi)[3], double *rsm, double *rpart) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (int)(blockDim.x >> 5);
+    for (int d = 0; d < 3; ++d) {
+        double a = lo[d], b = hi[d];
+        for (int o = 16; o > 0; o >>= 1) {
+            a = fmin(a, __shfl_xor_sync(0xffffffffu, a, o));
+            b = fmax(b, __shfl_xor_sync(0xffffffffu, b, o));
+        }
+        if (lane == 0) {
+            rsm[32 * d + wid] = a;
+            rsm[32 * (3 + d) + wid] = b;
+        }
+    }
+    __syncthreads();
+    if (wid == 0) {
+        for (int d = 0; d < 3; ++d) {
+            double a = lane < nw ? rsm[32 * d + lane] : 1e300, b = lane < nw ? rsm[32 * (3 + d) + lane] : -1e300;
+            for (int o = 16; o > 0; o >>= 1) {
+                a = fmin(a, __shfl_xor_sync(0xffffffffu, a, o));
+                b = fmax(b, __shfl_xor_sync(0xffffffffu, b, o));
+            }
+            if (lane == 0) {
+                rpart[d] = a;
+                rpart[3 + d] = b;
+            }
+        }
+    }
+    if constexpr (CL > 1) {
+        T.sync();
+        cg::cluster_group cl = cg::this_cluster();
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = 1e300;
+            hi[d] = -1e300;
+        }
+        for (int r = 0; r < CL; ++r) {
+            const double *pr = cl.map_shared_rank(rpart, r);
+            for (int d = 0; d < 3; ++d) {
+                lo[d] = fmin(lo[d], pr[d]);
+                hi[d] = fmax(hi[d], pr[3 + d]);
+            }
+        }
+        T.sync();  // rpart is read before anyone writes it again
+    } else {
+        __syncthreads();
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = rpart[d];
+            hi[d] = rpart[3 + d];
+        }
+        __syncthreads();
+    }
+}
+
+// Neighbor list, Born radii and energy of system s rebuilt by its own team
+// inside the persistent kernel (the host path: alma_nl_build + alma_born_radii
+// + alma_energy for the system).  The same per-atom row, Born and pair/SASA
+// code as those entry points, so the rows come out identical, order
+// included.  Returns false, leaving the list untouched where it matters,
+// when the cell grid or the rows do not fit: the chain then stops for a
+// host rebuild, which grows the regions.  E: the fresh total energy.
+template <typename R, int CL>
+__device__ bool team_rebuild(const MoveCtx &C, const MCConfigDev &cfg, int s, const Team<CL> &T, double *sm,
+                             double *rsm, double *rpart, int64_t *ssm, double &E) {
+    const RebuildWS &ws = cfg.rw;
+    const AlmaBatch &b = C.b;
+    const AlmaNL &nl = C.nl;
+    const int a0 = b.atom_off[s], a1 = b.atom_off[s + 1], n = a1 - a0;
+    const int tid = T.gtid(), nthr = T.gthreads(), wid = T.gwarp(), nw = T.gwarps(), lane = threadIdx.x & 31;
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int i = a0 + tid; i < a1; i += nthr) {
+        const double4 p = ld_xyz(b.xyz, i);
+        lo[0] = fmin(lo[0], p.x); hi[0] = fmax(hi[0], p.x);
+        lo[1] = fmin(lo[1], p.y); hi[1] = fmax(hi[1], p.y);
+        lo[2] = fmin(lo[2], p.z); hi[2] = fmax(hi[2], p.z);
+    }
+    team_minmax3<CL>(T, lo, hi, rsm, rpart);
+    SysGrid g = grid_from_box(lo, hi, C.P.nl_rcut2, n);
+    if (g.ncell > (int64_t)REB_CELLS_PER_ATOM * n + REB_CELLS_PAD) return false;  // same answer in every thread
+    g.cell_off = (int64_t)REB_CELLS_PER_ATOM * a0 + (int64_t)(REB_CELLS_PAD + 1) * s;
+    int32_t *cnt_c = ws.ccount + g.cell_off;
+    int64_t *start = ws.cstart + g.cell_off;
+    const int NA = b.natoms;
+    for (int64_t c = tid; c < g.ncell; c += nthr) cnt_c[c] = 0;
+    T.sync();
+    for (int i = a0 + tid; i < a1; i += nthr) {
+        const int c = cell_of_point(g, ld_xyz(b.xyz, i));
+        ws.cell_of[i] = c;
+        atomicAdd(&cnt_c[c], 1);
+    }
+    T.sync();
+    if (T.rank == 0) {  // cell starts; the counts become fill counters
+        int64_t carry = a0;
+        for (int64_t b0 = 0; b0 < g.ncell; b0 += blockDim.x) {
+            const int64_t c = b0 + threadIdx.x;
+            const int64_t v = c < g.ncell ? cnt_c[c] : 0;
+            int64_t ex;
+            const int64_t tot = block_exclusive_scan(v, ex, ssm);
+            if (c < g.ncell) {
+                start[c] = carry + ex;
+                cnt_c[c] = 0;
+            }
+            carry += tot;
+        }
+        if (threadIdx.x == 0) start[g.ncell] = carry;
+    }
+    T.sync();
+    for (int i = a0 + tid; i < a1; i += nthr) {
+        const int c = ws.cell_of[i];
+        ws.cell_atoms[start[c] + atomicAdd(&cnt_c[c], 1)] = i;
+    }
+    T.sync();
+    int32_t *tmp = ws.cnt;  // ascending atoms in every cell: rank sort, one warp per cell
+    for (int64_t c = wid; c < g.ncell; c += nw) {
+        const int64_t b0 = start[c];
+        const int m = (int)(start[c + 1] - b0);
+        if (m <= 1) continue;
+        for (int k = lane; k < m; k += 32) {
+            const int v = ws.cell_atoms[b0 + k];
+            int rank = 0;
+            for (int q = 0; q < m; ++q) rank += ws.cell_atoms[b0 + q] < v;
+            tmp[b0 + rank] = v;
+        }
+        __syncwarp();
+        for (int k = lane; k < m; k += 32) ws.cell_atoms[b0 + k] = tmp[b0 + k];
+        __syncwarp();
+    }
+    T.sync();
+    const double rcut2 = C.P.nl_rcut2;
+    const int64_t *ep = C.t.excl_ptr;
+    const int32_t *ec = C.t.excl_cols;
+    for (int i = a0 + wid; i < a1; i += nw) {
+        int nf, nh, nsf, nsh;
+        nl_row_atom<0>(i, lane, g, b.xyz, rcut2, ws.cell_of, ws.cstart, ws.cell_atoms, b.prm64, cfg.reach_pad, ep, ec,
+                       nl, nf, nh, nsf, nsh);
+        if (lane == 0) {
+            ws.cnt[i] = nf;
+            ws.cnt[(size_t)NA + i] = nh;
+            ws.cnt[2 * (size_t)NA + i] = nsf;
+            ws.cnt[3 * (size_t)NA + i] = nsh;
+        }
+    }
+    T.sync();
+    if (T.rank == 0) {  // row pointers inside the system's regions
+        const int nkind = nl.sfull_cols ? 4 : 2;
+        int fits = 1;
+        for (int kind = 0; kind < nkind; ++kind) {
+            const int32_t *cnt = ws.cnt + (size_t)kind * NA;
+            int64_t *ptr = kind == 0 ? nl.full_ptr : kind == 1 ? nl.half_ptr : kind == 2 ? nl.sfull_ptr : nl.shalf_ptr;
+            int32_t *len = kind == 0 ? nl.full_len : kind == 1 ? nl.half_len : kind == 2 ? nl.sfull_len : nl.shalf_len;
+            const int64_t *basev = kind == 0 ? nl.full_base : kind == 1 ? nl.half_base : kind == 2 ? nl.sfull_base
+                                                                                                    : nl.shalf_base;
+            const int64_t base = basev[s], cap = basev[s + 1] - base;
+            int64_t carry = 0;
+            for (int i0 = a0; i0 < a1; i0 += blockDim.x) {
+                const int i = i0 + threadIdx.x;
+                const int64_t v = i < a1 ? cnt[i] : 0;
+                int64_t ex;
+                const int64_t tot = block_exclusive_scan(v, ex, ssm);
+                if (i < a1) {
+                    ptr[i] = base + carry + ex;
+                    len[i] = (int32_t)v;
+                }
+                carry += tot;
+            }
+            if (threadIdx.x == 0) nl.need[4 * s + kind] = carry;
+            if (carry > cap) fits = 0;
+        }
+        if (threadIdx.x == 0) ws.flag[s] = fits;
+    }
+    T.sync();
+    if (!__ldcg(&ws.flag[s])) return false;
+    for (int i = a0 + wid; i < a1; i += nw) {
+        int nf, nh, nsf, nsh;
+        nl_row_atom<1>(i, lane, g, b.xyz, rcut2, ws.cell_of, ws.cstart, ws.cell_atoms, b.prm64, cfg.reach_pad, ep, ec,
+                       nl, nf, nh, nsf, nsh);
+    }
+    T.sync();
+    for (int i = a0 + wid; i < a1; i += nw)
+        born_atom<R>(i, lane, b.xyz, b.prm, b.prm64, nl.full_ptr, nl.full_len, nl.full_cols, b.born);
+    T.sync();
+    for (int i = a0 + wid; i < a1; i += nw)
+        pair_sasa_atom<R>(C.P, i, lane, b.xyz, b.prm, b.prm64, b.born, nl.half_ptr, nl.half_len, nl.half_cols,
+                          ep != nullptr, ws.atom_e, b.sasa);
+    T.sync();
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int i = a0 + tid; i < a1; i += nthr) {
+        v[0] += ws.atom_e[2 * (size_t)i];
+        v[1] += ws.atom_e[2 * (size_t)i + 1];
+    }
+    if (C.t.dih_off)
+        for (int r = C.t.dih_off[s] + tid; r < C.t.dih_off[s + 1]; r += nthr) v[2] += dih_record_energy(b.xyz, C.t, r);
+    if (C.t.ss_off)
+        for (int k = C.t.ss_off[s] + tid; k < C.t.ss_off[s + 1]; k += nthr) {
+            const double dr = sqrt(dist2(b.xyz, C.t.ss_ij[2 * k], C.t.ss_ij[2 * k + 1])) - C.P.r0_ss;
+            v[3] += C.P.k_ss * dr * dr;
+        }
+    team_sum<CL, 4>(T, v, sm, rpart);
+    T.sync();  // the partials are read before anyone writes them again
+    const double sasa = n > 0 ? C.P.beta_sa + v[1] : 0.0;
+    E = sasa + v[2] + v[3] + v[0];
+    return true;
+}
+
 // One system per CTA (CL = 1) or per cluster of CL CTAs.  Every CTA of a
 // cluster keeps its own copy of the chain state and makes the same draws
 // and decisions (the ΔE totals are bit-identical in every CTA); rank 0
@@ -120,18 +346,32 @@ __global__ void __launch_bounds__(NT, 512 / NT) mc_kernel(MoveCtx C, MCConfigDev
     __shared__ AlmaChainState S;
     __shared__ double u[6];
     __shared__ int did_move, accept;
+    __shared__ double rsm[192], rpart[8];
+    __shared__ int64_t ssm[33];
     const Team<CL> T;
     const int s = blockIdx.x / CL;
     if (threadIdx.x == 0) S = states[s];
     __syncthreads();
-    const bool rows_ok = system_within_skin(C, s);
+    bool rows_ok = system_within_skin(C, s);
     if (threadIdx.x == 0 && !rows_ok && C.nl.ref_xyz && S.step < step_limit) S.need_rebuild = 1;
     __syncthreads();
     const int nrb = C.t.rb_off[s + 1] - C.t.rb_off[s];
     const int ncp = C.t.cp_off[s + 1] - C.t.cp_off[s];
     const int ncsp = C.t.csp_off[s + 1] - C.t.csp_off[s];
     const int nset = cfg.moveset_off ? cfg.moveset_off[s + 1] - cfg.moveset_off[s] : nrb;
-    while (S.step < step_limit && !S.need_rebuild) {
+    while (S.step < step_limit) {
+        if (S.need_rebuild) {  // drifted: rebuild this chain in place, or stop for the host
+            double E = 0.0;
+            if (!cfg.rw.ccount || !C.nl.ref_xyz || !team_rebuild<R, CL>(C, cfg, s, T, sm, rsm, rpart, ssm, E)) break;
+            if (threadIdx.x == 0) {
+                S.energy = E;
+                S.n_rebuild++;
+                S.need_rebuild = 0;
+            }
+            rows_ok = true;
+            __syncthreads();
+            continue;
+        }
         if (threadIdx.x == 0) did_move = draw_proposal(C, cfg, S, s, (uint64_t)S.step, nrb, ncp, ncsp, nset, M, u);
         __syncthreads();
         if (!did_move) {
@@ -461,6 +701,37 @@ using namespace alma;
 
 static size_t align_up256(size_t x) { return (x + 255) & ~(size_t)255; }
 
+static size_t rebuild_bytes(int32_t natoms, int32_t nsys, RebuildWS *ws, void *base) {
+    const size_t n = natoms > 0 ? (size_t)natoms : 1, S = nsys > 0 ? (size_t)nsys : 1;
+    const size_t cells = (size_t)REB_CELLS_PER_ATOM * n + (size_t)(REB_CELLS_PAD + 1) * S;
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        char *q = base ? (char *)base + off : nullptr;
+        off += align_up256(bytes);
+        return q;
+    };
+    RebuildWS t;
+    t.ccount = (int32_t *)take(sizeof(int32_t) * cells);
+    t.cstart = (int64_t *)take(sizeof(int64_t) * cells);
+    t.cell_of = (int32_t *)take(sizeof(int32_t) * n);
+    t.cell_atoms = (int32_t *)take(sizeof(int32_t) * n);
+    t.cnt = (int32_t *)take(sizeof(int32_t) * 4 * n);
+    t.atom_e = (double *)take(sizeof(double) * 2 * n);
+    t.flag = (int32_t *)take(sizeof(int32_t) * S);
+    if (ws) *ws = t;
+    return off;
+}
+
+static RebuildWS carve_rebuild(void *base, int32_t natoms, int32_t nsys) {
+    RebuildWS t = {};
+    if (base) rebuild_bytes(natoms, nsys, &t, base);
+    return t;
+}
+
+extern "C" size_t alma_mc_rebuild_bytes(int32_t natoms, int32_t nsys) {
+    return rebuild_bytes(natoms, nsys, nullptr, nullptr);
+}
+
 int alma_check_move_args(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *nl, const AlmaParams *p,
                          void *scratch, const char *who);
 MoveCtx alma_make_move_ctx(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *nl, const AlmaParams *p,
@@ -490,6 +761,8 @@ extern "C" int alma_mc_run(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *
     d.fixed_delta = cfg->fixed_delta;
     d.moveset_off = cfg->moveset_off;
     d.moveset = cfg->moveset;
+    d.reach_pad = 2.0 * p->probe_r + 2.0 * sqrt(p->half_skin2) + 1e-6;  // as alma_nl_build
+    d.rw = carve_rebuild(cfg->rebuild_ws, b->natoms, b->nsys);
     cudaStream_t st = (cudaStream_t)stream;
     // Threads per system: 512 when the batch fits one CTA per SM, else 256
     // (two CTAs per SM), so every chain of a persistent launch is resident.

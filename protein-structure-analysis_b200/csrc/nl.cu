@@ -24,15 +24,9 @@
 
 #include "alma_common.cuh"
 #include "alma_scan.cuh"
+#include "nl_core.cuh"
 
 namespace alma {
-
-struct SysGrid {
-    double xlo, ylo, zlo, cs;
-    int32_t nx, ny, nz, pad;
-    int64_t cell_off;  // first global cell of this system
-    int64_t ncell;
-};
 
 struct NLWork {
     SysGrid *grid;        // [nsys]
@@ -112,18 +106,7 @@ __global__ void nl_grid_kernel(const int32_t *__restrict__ atom_off, const uint8
             lo[d] = red[d][0]; hi[d] = red[3 + d][0];
             for (int w = 1; w < nw; ++w) { lo[d] = fmin(lo[d], red[d][w]); hi[d] = fmax(hi[d], red[3 + d][w]); }
         }
-        SysGrid g;
-        g.cs = sqrt(nl_rcut2) + 1e-6;
-        const double mg = g.cs;
-        g.xlo = lo[0] - mg; g.ylo = lo[1] - mg; g.zlo = lo[2] - mg;
-        const double lx = hi[0] - g.xlo + 2.0 * mg, ly = hi[1] - g.ylo + 2.0 * mg, lz = hi[2] - g.zlo + 2.0 * mg;
-        g.nx = max(1, (int)ceil(lx / g.cs));
-        g.ny = max(1, (int)ceil(ly / g.cs));
-        g.nz = max(1, (int)ceil(lz / g.cs));
-        if (a1 <= a0) { g.nx = g.ny = g.nz = 1; }
-        g.pad = 0;
-        g.ncell = (int64_t)g.nx * g.ny * g.nz;
-        g.cell_off = 0;
+        SysGrid g = grid_from_box(lo, hi, nl_rcut2, a1 - a0);
         grid[s] = g;
     }
 }
@@ -152,11 +135,7 @@ __global__ void nl_bin_kernel(const int32_t *__restrict__ atom_off, int nsys, in
     const int s = sys_of_atom(atom_off, nsys, i);
     if (mask && !mask[s]) return;
     const SysGrid g = grid[s];
-    const double4 p = ld_xyz(xyz, i);
-    const int cx = min(g.nx - 1, max(0, (int)floor((p.x - g.xlo) / g.cs)));
-    const int cy = min(g.ny - 1, max(0, (int)floor((p.y - g.ylo) / g.cs)));
-    const int cz = min(g.nz - 1, max(0, (int)floor((p.z - g.zlo) / g.cs)));
-    const int c = cx + g.nx * (cy + g.ny * cz);
+    const int c = cell_of_point(g, ld_xyz(xyz, i));
     cell_of[i] = c;
     atomicAdd(&cell_count[g.cell_off + c], 1);
 }
@@ -215,19 +194,6 @@ __global__ void nl_cellsort_kernel(const int64_t *__restrict__ total_cells, cons
             __syncthreads();
         }
     }
-}
-
-__device__ __forceinline__ bool excluded(const int64_t *__restrict__ excl_ptr, const int32_t *__restrict__ excl_cols,
-                                         int i, int j) {
-    if (!excl_ptr) return false;
-    int lo_i = i < j ? i : j, hi_j = i < j ? j : i;
-    int64_t lo = excl_ptr[lo_i], hi = excl_ptr[lo_i + 1];
-    while (lo < hi) {
-        const int64_t mid = (lo + hi) >> 1;
-        if (excl_cols[mid] < hi_j) lo = mid + 1;
-        else hi = mid;
-    }
-    return lo < excl_ptr[lo_i + 1] && excl_cols[lo] == hi_j;
 }
 
 // One CTA per system: row pointers inside the system's region, overflow
@@ -293,68 +259,9 @@ __global__ void nl_rows_kernel(const int32_t *__restrict__ atom_off, int nsys, i
     if (mask && !mask[s]) return;
     if (PASS == 1 && !sys_ok[s]) return;
     const SysGrid g = grid[s];
-    const int c = cell_of[i];
-    const int cx = c % g.nx, cy = (c / g.nx) % g.ny, cz = c / (g.nx * g.ny);
-    const double4 pi = ld_xyz(xyz, i);
-    const bool shorts = nl.sfull_cols != nullptr;
-    const double ri_pad = shorts ? prm64[4 * (size_t)i + 1] + reach_pad : 0.0;
-    int64_t fo = 0, ho = 0, sfo = 0, sho = 0;
-    if (PASS == 1) {
-        fo = nl.full_ptr[i];
-        ho = nl.half_ptr[i];
-        if (shorts) {
-            sfo = nl.sfull_ptr[i];
-            sho = nl.shalf_ptr[i];
-        }
-        if (lane == 0) *reinterpret_cast<double4 *>(nl.ref_xyz + 4 * (size_t)i) = pi;
-    }
-    int nfull = 0, nhalf = 0, nsfull = 0, nshalf = 0;
-    for (int dz = -1; dz <= 1; ++dz) {
-        const int cz2 = cz + dz;
-        if (cz2 < 0 || cz2 >= g.nz) continue;
-        for (int dy = -1; dy <= 1; ++dy) {
-            const int cy2 = cy + dy;
-            if (cy2 < 0 || cy2 >= g.ny) continue;
-            for (int dx = -1; dx <= 1; ++dx) {
-                const int cx2 = cx + dx;
-                if (cx2 < 0 || cx2 >= g.nx) continue;
-                const int64_t cell = g.cell_off + cx2 + (int64_t)g.nx * (cy2 + (int64_t)g.ny * cz2);
-                const int64_t beg = cell_start[cell], end = cell_start[cell + 1];
-                for (int64_t k0 = beg; k0 < end; k0 += 32) {
-                    const int64_t k = k0 + lane;
-                    int j = -1;
-                    bool in = false, sh = false;
-                    if (k < end) {
-                        j = cell_atoms[k];
-                        const double r2 = d2_of(pi, ld_xyz(xyz, j));
-                        in = (j != i) && r2 < rcut2;
-                        if (in && shorts) {
-                            const double reach = ri_pad + prm64[4 * (size_t)j + 1];
-                            sh = r2 < reach * reach;
-                        }
-                    }
-                    const unsigned mf = __ballot_sync(0xffffffffu, in);
-                    const unsigned mh = __ballot_sync(0xffffffffu, in && j > i);
-                    const unsigned msf = __ballot_sync(0xffffffffu, sh);
-                    const unsigned msh = __ballot_sync(0xffffffffu, sh && j > i);
-                    if (PASS == 1 && in) {
-                        const unsigned lt = (1u << lane) - 1u;
-                        const uint32_t e = (uint32_t)j | (excluded(excl_ptr, excl_cols, i, j) ? ALMA_EXCL_BIT : 0u);
-                        nl.full_cols[fo + nfull + __popc(mf & lt)] = e;
-                        if (j > i) nl.half_cols[ho + nhalf + __popc(mh & lt)] = e;
-                        if (sh) {
-                            nl.sfull_cols[sfo + nsfull + __popc(msf & lt)] = e;
-                            if (j > i) nl.shalf_cols[sho + nshalf + __popc(msh & lt)] = e;
-                        }
-                    }
-                    nfull += __popc(mf);
-                    nhalf += __popc(mh);
-                    nsfull += __popc(msf);
-                    nshalf += __popc(msh);
-                }
-            }
-        }
-    }
+    int nfull, nhalf, nsfull, nshalf;
+    nl_row_atom<PASS>(i, lane, g, xyz, rcut2, cell_of, cell_start, cell_atoms, prm64, reach_pad, excl_ptr, excl_cols,
+                      nl, nfull, nhalf, nsfull, nshalf);
     if (PASS == 0 && lane == 0) {
         full_cnt[i] = nfull;
         half_cnt[i] = nhalf;

@@ -73,7 +73,7 @@ class AlmaMCConfig(C.Structure):
                 ("sidechain_mult", C.c_double), ("crank_prob", C.c_double),
                 ("concerted_prob", C.c_double), ("fixed_delta", C.c_double),
                 ("moveset_off", _p), ("moveset", _p), ("threads_per_system", _i32), ("cluster_size", _i32),
-                ("spec_teams", _i32), ("pad", _i32)]
+                ("spec_teams", _i32), ("pad", _i32), ("rebuild_ws", _p)]
 
 
 class AlmaChainState(C.Structure):
@@ -133,6 +133,8 @@ def lib():
     L.alma_move_scratch_bytes.argtypes = [_i32]
     L.alma_mc_scratch_bytes.restype = C.c_size_t
     L.alma_mc_scratch_bytes.argtypes = [_i32, _i32, _i32]
+    L.alma_mc_rebuild_bytes.restype = C.c_size_t
+    L.alma_mc_rebuild_bytes.argtypes = [_i32, _i32]
     L.alma_topo_sides.argtypes = [_i32, _p, _p, _i32, _p, _p, _p, _i64]
     L.alma_topo_sides_compact.argtypes = [_i32, _p, _p, _i32, _p, _p, _p, _p, _p, _p, _i64]
     L.alma_nl_build.argtypes = [_p, _p, _p, _p, _p, _p, _i64, _p]

@@ -22,15 +22,15 @@ def _setup(name):
 
 
 def _gpu_run(g, F, nsys, seed, steps, precision="fp64", policy=0, fixed_delta=0.0, moveset=None, T=0.6,
-             cluster_size=None, spec_teams=1):
+             cluster_size=None, spec_teams=1, device_rebuild=True, runner=False):
     from protein_physics_b200.device import DeviceBatch
     from protein_physics_b200.mc import MCRunner
     b = DeviceBatch([(g["xyz"], g["q"], g["r"], g["eps"], F)] * nsys, precision=precision)
     R = MCRunner(b, T, seed, policy=policy, fixed_delta=fixed_delta,
                  moveset=[moveset] * nsys if moveset is not None else None, cluster_size=cluster_size,
-                 spec_teams=spec_teams)
+                 spec_teams=spec_teams, device_rebuild=device_rebuild)
     st = R.run_to(steps)
-    return b, st
+    return (b, st, R) if runner else (b, st)
 
 
 def _oracle_run(g, F, seed, steps, sys_index=0, policy=0, fixed_delta=0.0, moveset=None, T=0.6):
@@ -146,3 +146,39 @@ def test_spec_teams_bitwise_equal_one_team():
     assert np.array_equal(b1.coords(0), b4.coords(0))
     for k in ("energy", "cur_max", "n_accepted", "n_proposed", "n_rebuild", "step"):
         assert st1[k][0] == st4[k][0], k
+
+
+# ---- rebuilds inside the persistent kernel ----------------------------------
+@pytest.mark.parametrize("cl", [1, 8])
+def test_device_rebuild_matches_oracle_and_host_build(cl):
+    """Large fixed angles drift the chain past half the skin many times: the
+    in-kernel rebuild gives the oracle's trajectory, and the list it leaves
+    equals a fresh host build of the same coordinates, row order included."""
+    from protein_physics_b200.device import DeviceBatch
+    g, F = _setup("insulin")
+    b, st, R = _gpu_run(g, F, 1, 5, 120, fixed_delta=0.6, T=50.0, cluster_size=cl, spec_teams=1, runner=True)
+    x_o, st_o, _ = _oracle_run(g, F, 5, 120, fixed_delta=0.6, T=50.0)
+    assert st_o["n_rebuild"] > 0
+    assert st["n_rebuild"][0] == st_o["n_rebuild"]
+    assert st["n_accepted"][0] == st_o["n_accepted"]
+    np.testing.assert_allclose(b.coords(0), x_o, rtol=0, atol=1e-8)
+    assert R.rebuilds == 0  # every rebuild ran on the device
+    ref = b.ref_xyz[:g.n, :3].cpu().numpy()
+    h = DeviceBatch([(ref, g["q"], g["r"], g["eps"], F)], precision="fp64")
+    h.build_nl()
+    for half in (True, False):
+        for short in (False, True):
+            a1, a2, a3 = b.nl_host(0, half=half, short=short)
+            b1, b2, b3 = h.nl_host(0, half=half, short=short)
+            assert np.array_equal(a1, b1) and np.array_equal(a2, b2) and np.array_equal(a3, b3), (half, short)
+
+
+def test_device_rebuild_batched_equals_host_rebuild():
+    g, F = _setup("insulin")
+    b1, st1 = _gpu_run(g, F, 3, 21, 120, fixed_delta=0.5, T=30.0, cluster_size=1, spec_teams=1, device_rebuild=True)
+    b2, st2 = _gpu_run(g, F, 3, 21, 120, fixed_delta=0.5, T=30.0, cluster_size=1, spec_teams=1, device_rebuild=False)
+    for s in range(3):
+        assert st1["n_rebuild"][s] == st2["n_rebuild"][s] > 0
+        assert st1["n_accepted"][s] == st2["n_accepted"][s]
+        assert np.array_equal(b1.coords(s), b2.coords(s))
+        assert st1["energy"][s] == pytest.approx(st2["energy"][s], rel=1e-11)
