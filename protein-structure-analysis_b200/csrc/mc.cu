@@ -38,8 +38,10 @@ namespace alma {
 
 // Device workspace of the in-kernel rebuild (per system: a cell region of
 // REB_CELLS_PER_ATOM cells per atom + REB_CELLS_PAD; per atom: cell, slot,
-// four row counts, two energy slots).
-constexpr int REB_CELLS_PER_ATOM = 16;
+// four row counts, two energy slots).  A chain whose grid is sparser
+// (an extended chain in a large box: the per-cell passes of one team would
+// cost more than the whole-GPU host build) stops for the host rebuild.
+constexpr int REB_CELLS_PER_ATOM = 2;
 constexpr int REB_CELLS_PAD = 256;
 
 struct RebuildWS {
@@ -240,15 +242,25 @@ __device__ bool team_rebuild(const MoveCtx &C, const MCConfigDev &cfg, int s, co
         ws.cell_atoms[start[c] + atomicAdd(&cnt_c[c], 1)] = i;
     }
     T.sync();
-    int32_t *tmp = ws.cnt;  // ascending atoms in every cell: rank sort, one warp per cell
-    for (int64_t c = wid; c < g.ncell; c += nw) {
+    // ascending atoms in every cell: cells holding two or more atoms are
+    // listed (at most n/2 of them), then rank-sorted one warp per cell
+    int32_t *tmp = ws.cnt;                      // kind-0 counts: free until the count pass
+    int32_t *multi = ws.cnt + (size_t)NA + a0;  // kind-1 counts: the list of cells to sort
+    int *nmulti = reinterpret_cast<int *>(ws.flag + s);
+    if (tid == 0) *nmulti = 0;
+    T.sync();
+    for (int64_t c = tid; c < g.ncell; c += nthr)
+        if (start[c + 1] - start[c] > 1) multi[atomicAdd(nmulti, 1)] = (int32_t)c;
+    T.sync();
+    const int nm = __ldcg(nmulti);
+    for (int q = wid; q < nm; q += nw) {
+        const int64_t c = multi[q];
         const int64_t b0 = start[c];
         const int m = (int)(start[c + 1] - b0);
-        if (m <= 1) continue;
         for (int k = lane; k < m; k += 32) {
             const int v = ws.cell_atoms[b0 + k];
             int rank = 0;
-            for (int q = 0; q < m; ++q) rank += ws.cell_atoms[b0 + q] < v;
+            for (int q2 = 0; q2 < m; ++q2) rank += ws.cell_atoms[b0 + q2] < v;
             tmp[b0 + rank] = v;
         }
         __syncwarp();
