@@ -64,7 +64,7 @@ class MCRunner:
     initial max angle (the reference's max_angle)."""
 
     def __init__(self, batch: DeviceBatch, temperatures, seed, policy=0, cur_max0=0.12, tune_freq=200,
-                 fixed_delta=0.0, moveset=None, cluster_size=None, threads=0, spec_teams=None, device_rebuild=True):
+                 fixed_delta=0.0, moveset=None, cluster_size=None, threads=0, spec_teams=None, device_rebuild=False):
         self.b = batch
         self.L = batch.L
         self._keep = []
@@ -83,9 +83,11 @@ class MCRunner:
             sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
             spec_teams = 2 if 2 * batch.nsys * int(cluster_size) <= sms else 1
         self.cfg.spec_teams = int(spec_teams)
-        # a drifted chain rebuilds its list, radii and energy inside the
-        # persistent kernel (one-team launches); the host loop below remains
-        # for the speculative mode and for lists that outgrow their regions
+        # device_rebuild: a drifted chain rebuilds its list, radii and energy
+        # inside the persistent kernel (one-team launches) instead of
+        # stopping for the host.  Off by default: one team has a small share
+        # of the GPU for the list's 27-cell scan, and on the bench workloads
+        # the whole-GPU host rebuild of all flagged chains is faster.
         self.rebuild_ws = None
         if device_rebuild:
             self.rebuild_ws = torch.empty(self.L.alma_mc_rebuild_bytes(batch.natoms, batch.nsys), dtype=torch.uint8,
