@@ -293,6 +293,16 @@ int alma_mala_select(AlmaBatch *b, const AlmaTopo *t, const uint8_t *accept, con
                      const double *xyz_old, const double *born_old, const double *g_new, double *g_cur,
                      void *stream);
 
+/* Ensemble metrics of snapshots resident on the device (replaces
+ * compute_mean_dist_matrix and compute_contact_freq_matrix,
+ * analysis_ext.cpp:85-170).  coords: device double[n_snaps*n_ca*3];
+ * out: device double[n_ca*n_ca], the mean distance (or the fraction of
+ * snapshots with distance < cutoff) of every residue pair, 0 on the
+ * diagonal.  Each cell sums its snapshots in order. */
+int alma_mean_dist_matrix(const double *coords, int32_t n_snaps, int32_t n_ca, double *out, void *stream);
+int alma_contact_freq_matrix(const double *coords, int32_t n_snaps, int32_t n_ca, double cutoff, double *out,
+                             void *stream);
+
 /* Device scratch for the move / MC kernels: alma_move_scratch_bytes(natoms)
  * bytes, zeroed once by alma_move_scratch_init; every call leaves it zeroed.
  * Calls that share a scratch buffer must not overlap on the GPU. */

@@ -151,6 +151,8 @@ def lib():
     L.alma_mala_propose.argtypes = [_p, _i32, _p, _p, _p, _p, _p, _p, _p]
     L.alma_mala_accept.argtypes = [_p, _i32, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p]
     L.alma_mala_select.argtypes = [_p, _p, _p, _p, _p, _p, _p, _p, _p]
+    L.alma_mean_dist_matrix.argtypes = [_p, _i32, _i32, _p, _p]
+    L.alma_contact_freq_matrix.argtypes = [_p, _i32, _i32, C.c_double, _p, _p]
     L.alma_replica_exchange.argtypes = [_i32, _p, _p, _p, _p, C.c_uint64, _i64, _p, _p, _p]
     L.alma_mc_run.argtypes = [_p, _p, _p, _p, C.c_int, _p, _p, _p, _i64, _p]
     L.alma_mc_after_rebuild.argtypes = [_p, _p, _p, _i32, _p]
