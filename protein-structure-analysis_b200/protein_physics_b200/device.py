@@ -65,7 +65,7 @@ class DeviceBatch:
         _require_cuda()
         self.L = _lib.lib()
         self.prec = _lib.PREC_FP64 if precision == "fp64" else _lib.PREC_MIXED
-        self.stream = stream or torch.cuda.current_stream()
+        self.stream = stream  # None: launch on torch's current stream (graph capture included)
         self.nsys = len(systems)
         if self.nsys == 0:
             raise ValueError("empty batch")
@@ -257,7 +257,7 @@ class DeviceBatch:
         return nl
 
     def _sp(self):
-        return C.c_void_p(self.stream.cuda_stream)
+        return C.c_void_p((self.stream or torch.cuda.current_stream()).cuda_stream)
 
     def build_nl(self, sys_mask=None, check=True):
         """Neighbor lists (all systems, or those with sys_mask[s] != 0)."""

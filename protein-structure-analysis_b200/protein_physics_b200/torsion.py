@@ -108,6 +108,7 @@ class _Eval:
 
     def __init__(self, ts: TorsionSpace):
         self.ts = ts
+        self.check = True  # the list's overflow check (a host sync; off inside a CUDA graph)
         b = ts.b
         self.terms = torch.zeros((b.nsys, 5), dtype=torch.float64, device="cuda")
         self.grad = torch.zeros((max(b.natoms, 1), 4), dtype=torch.float64, device="cuda")
@@ -115,7 +116,8 @@ class _Eval:
 
     def __call__(self):
         b = self.ts.b
-        b.build_nl()
+        b.nl_ready = False
+        b.build_nl(check=self.check)
         b.energy_terms(recompute_born=True, out=self.terms)
         b.forces(out=self.grad)
         self.ts.gtheta(self.grad, out=self.g)
@@ -218,6 +220,8 @@ class MALARunner:
         self.accept = torch.zeros(batch.nsys, dtype=torch.uint8, device="cuda")
         self.xyz_old = torch.empty_like(batch.xyz)
         self.born_old = torch.empty_like(batch.born)
+        self._graph = None
+        self._graph_capture = False
         self.refresh()
 
     def refresh(self):
@@ -238,6 +242,7 @@ class MALARunner:
 
     def step(self):
         b, ts, L = self.b, self.ts, self.b.L
+        self.new.check = self._graph_capture is False
         topo, cfg = C.byref(b.topo_s), C.byref(self.cfg)
         _lib.check(L.alma_mala_propose(topo, b.nsys, _ptr(self.cur.g), _ptr(self.sigma), cfg, _ptr(self.states),
                                        None, _ptr(self.delta), b._sp()), "alma_mala_propose")
@@ -251,7 +256,48 @@ class MALARunner:
         ts.select(self.accept, self.xyz_old, self.born_old, g_new=self.new.g, g_cur=self.cur.g)
         b.nl_ready = False
 
-    def run(self, n):
-        for _ in range(int(n)):
-            self.step()
+    def run(self, n, graph=False, chunk=64):
+        """n proposals.  graph=True replays one captured CUDA graph per
+        proposal (no host work between proposals); the list's overflow
+        check then runs once per chunk, and a chunk that overflowed is
+        undone and redone eagerly (which grows the list regions)."""
+        if not graph:
+            for _ in range(int(n)):
+                self.step()
+            return self.state()
+        done = 0
+        while done < n:
+            k = min(int(chunk), int(n) - done)
+            if self._graph is None:
+                self._capture()
+            snap = [t.clone() for t in (self.b.xyz, self.b.born, self.states, self.cur.g)]
+            for _ in range(k):
+                self._graph.replay()
+            if int(self.b.status.item()) & (_lib.ST_NL_OVERFLOW | _lib.ST_CELL_OVERFLOW):
+                for dst, src in zip((self.b.xyz, self.b.born, self.states, self.cur.g), snap):
+                    dst.copy_(src)
+                self.b.status.zero_()
+                self.b.invalidate_sasa()
+                self._graph = None
+                for _ in range(k):
+                    self.step()
+            done += k
+        self.b.nl_ready = False
+        self.b.invalidate_sasa()
         return self.state()
+
+    def _capture(self):
+        self.step()  # warm: every buffer exists before the capture
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            self.step()
+        torch.cuda.current_stream().wait_stream(side)
+        g = torch.cuda.CUDAGraph()
+        self._graph_capture = True
+        try:
+            with torch.cuda.graph(g):
+                self.step()
+        finally:
+            self._graph_capture = False
+        self._graph = g

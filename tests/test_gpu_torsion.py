@@ -227,3 +227,25 @@ def test_autograd_energy_matches_forces():
         from protein_physics_b200.device import DeviceBatch
         ref = float(DeviceBatch([(xyz, q, r, e, flat)], precision="fp64").energy_terms()[0, 4])
         assert float(E[s].detach()) == pytest.approx(ref, rel=1e-13)
+
+
+def test_mala_graph_replay_equals_eager():
+    """One captured CUDA graph per proposal gives the eager chain bit for bit."""
+    from protein_physics_b200 import synth
+    from protein_physics_b200.device import DeviceBatch
+    from protein_physics_b200.topology import BondTopology, flatten
+    from protein_physics_b200.torsion import MALARunner, minimize
+    ch = synth.chain(16, 4)
+    T = BondTopology()
+    T.build(ch.resnames, ch.atomnames, ch.res_idx)
+    flat = flatten(T)
+    out = []
+    for graph in (False, True):
+        b = DeviceBatch([(ch.xyz, ch.charge, ch.radius, ch.epsilon, flat)] * 2, precision="mixed")
+        minimize(b, steps=50)
+        R = MALARunner(b, [0.5962, 0.9], seed=8, step=np.radians(0.5))
+        st = R.run(70, graph=graph, chunk=32)
+        out.append((st, b.coords(0), b.coords(1)))
+    assert np.array_equal(out[0][1], out[1][1]) and np.array_equal(out[0][2], out[1][2])
+    for k in ("energy", "n_accepted", "n_proposed", "step", "scale"):
+        assert np.array_equal(out[0][0][k], out[1][0][k]), k
