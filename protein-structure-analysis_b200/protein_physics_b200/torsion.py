@@ -286,8 +286,14 @@ class MALARunner:
         self.b.invalidate_sasa()
         return self.state()
 
+    def _chain_tensors(self):
+        return (self.b.xyz, self.b.born, self.states, self.cur.g)
+
     def _capture(self):
-        self.step()  # warm: every buffer exists before the capture
+        # the warm-up steps make every buffer exist before the capture; the
+        # chain is put back afterwards, so replays are its only proposals
+        snap = [t.clone() for t in self._chain_tensors()]
+        self.step()
         side = torch.cuda.Stream()
         side.wait_stream(torch.cuda.current_stream())
         with torch.cuda.stream(side):
@@ -300,4 +306,6 @@ class MALARunner:
                 self.step()
         finally:
             self._graph_capture = False
+        for dst, src in zip(self._chain_tensors(), snap):
+            dst.copy_(src)
         self._graph = g
