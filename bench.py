@@ -465,6 +465,7 @@ def run_globule(args):
     torch.cuda.synchronize()
     gd_ms = g0.elapsed_time(g1)
     E = hist[:, 0].cpu().numpy()
+    fd = force_fd_check(b, system)
     R = MALARunner(b, 300.0 * KB, seed=2024, step=np.radians(0.5), ts=ts)
     per = 10
     R.run(300)  # step-scale adaptation (window 20) settles before the timed proposals
@@ -501,9 +502,54 @@ def run_globule(args):
                   "launch": "one CUDA graph per proposal (%.0f proposals/s when launched from the host)" % eager_rate,
                   "l2": "inputs > L2 (16k atoms x lists)"},
                  sampler.summary(), _lib.lib().alma_launch_count() - l0,
-                 energy_force=ef,
+                 energy_force=ef, force_check=fd,
                  descent={"steps": 500, "ms": gd_ms, "steps_per_s": 500 / (gd_ms * 1e-3), "E_start": float(E[0]),
                           "E_end": float(E[-1]), "unit": "kcal/mol"})
+
+
+def force_fd_check(b, system, n_atoms=64, h=1e-4, seed=64):
+    """Analytic forces (mixed and FP64) vs central finite differences of the
+    FP64 device energy (h = 1e-4 Å, list fixed) on n_atoms random atoms of
+    the batch's current coordinates; atoms with a pair within 1e-3 Å of the
+    12 Å cutoff (where the reference energy jumps) are not drawn."""
+    import numpy as np
+    import torch
+    from protein_physics_b200.device import DeviceBatch
+    x0 = b.coords(0).copy()
+    _, q, r, e, F = system
+    b64 = DeviceBatch([(x0, q, r, e, F)], precision="fp64")
+    b64.build_nl()
+    b64.energy_terms()
+    g64 = b64.forces()[:b64.natoms, :3].cpu().numpy()
+    bm = DeviceBatch([(x0, q, r, e, F)], precision="mixed")
+    bm.build_nl()
+    bm.energy_terms()
+    gm = bm.forces()[:bm.natoms, :3].cpu().numpy()
+    rp, cols, _ = b64.nl_host(0, half=True)
+    I = np.repeat(np.arange(x0.shape[0]), np.diff(rp))
+    dist = np.sqrt(((x0[I] - x0[cols]) ** 2).sum(1))
+    near = np.zeros(x0.shape[0], bool)
+    bad = np.abs(dist - 12.0) < 1e-3 + 2 * h
+    near[I[bad]] = True
+    near[cols[bad]] = True
+    atoms = np.random.default_rng(seed).choice(np.flatnonzero(~near), size=n_atoms, replace=False)
+    xd = b64.xyz
+
+    def E(i, c, d):
+        xd[i, c] += d
+        b64.nl_ready = True
+        v = float(b64.energy_terms()[0, 4])
+        xd[i, c] -= d
+        return v
+
+    worst = {"fp64": 0.0, "mixed": 0.0}
+    for i in atoms:
+        fdv = np.array([(E(int(i), c, h) - E(int(i), c, -h)) / (2 * h) for c in range(3)])
+        scale = max(np.abs(fdv).max(), 1.0)
+        worst["fp64"] = max(worst["fp64"], float(np.abs(g64[i] - fdv).max() / scale))
+        worst["mixed"] = max(worst["mixed"], float(np.abs(gm[i] - fdv).max() / scale))
+    return {"atoms": int(n_atoms), "h_A": h, "max_rel_err_fp64": worst["fp64"], "max_rel_err_mixed": worst["mixed"],
+            "what": "max over atoms of max|F - FD| / max(|FD|, 1 kcal/mol/A); FD of the FP64 energy, list fixed"}
 
 
 def run_replica(args):
