@@ -383,6 +383,16 @@ class DeviceBatch:
                                              self._sp()), "alma_move_counters")
         return (out[0], out[1]) if phases else out[0]
 
+    def load_coords(self, xyz):
+        """New coordinates [natoms, 3] for every system (same atoms, same
+        topology): the list, radii and SASA cache are rebuilt on next use."""
+        x = torch.as_tensor(np.ascontiguousarray(xyz, np.float64) if not isinstance(xyz, torch.Tensor) else xyz,
+                            dtype=torch.float64).reshape(self.natoms, 3)
+        self.xyz[:self.natoms, :3].copy_(x)
+        self.nl_ready = False
+        self.invalidate_sasa()
+        self.status.zero_()
+
     # ---- host views -------------------------------------------------------------
     def coords(self, s=None):
         x = self.xyz[:, :3].cpu().numpy()

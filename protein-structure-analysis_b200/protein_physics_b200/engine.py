@@ -57,6 +57,34 @@ class PhysicsEngine:
         self.precision = precision
         self._seed = int(np.random.SeedSequence().entropy % (1 << 63)) if seed is None else int(seed)
         self._calls = 0
+        self._batches = {}  # device batches of recent calls, reused when only coordinates change
+
+    def _batch(self, xyz, q, r, e, flat, copies=1):
+        """A DeviceBatch of `copies` systems with these parameters and
+        topology, loaded with xyz: reused across calls on the same system
+        (the key hashes every parameter and topology array), so repeated
+        calls pay no topology upload or list allocation."""
+        import hashlib
+        from .device import DeviceBatch
+        h = hashlib.blake2b(digest_size=16)
+        for a in (q, r, e):
+            h.update(np.ascontiguousarray(a, np.float64).tobytes())
+        if flat is not None:
+            for name in ("excl_ptr", "excl_cols", "rb_i", "rb_j", "rb_kind", "rb_scale", "side_ptr", "side_idx",
+                         "side_lo", "side_hi", "dih_abcd", "term_off", "term_v2", "term_n", "term_gamma", "ss",
+                         "crank", "conc_sc"):
+                h.update(np.ascontiguousarray(getattr(flat, name)).tobytes())
+        key = (int(copies), len(q), flat is not None, h.hexdigest())
+        b = self._batches.pop(key, None)
+        X = np.tile(np.asarray(xyz, np.float64).reshape(-1, 3), (int(copies), 1))
+        if b is None:
+            b = DeviceBatch([(xyz, q, r, e, flat)] * int(copies), precision=self.precision)
+        else:
+            b.load_coords(X)
+        self._batches[key] = b
+        while len(self._batches) > 4:
+            self._batches.pop(next(iter(self._batches)))
+        return b
 
     # ---- energies ----------------------------------------------------------------
     def calculate_potential(self, particles, topology=None):
@@ -73,7 +101,9 @@ class PhysicsEngine:
         flat = _topology.flatten(topology) if topology is not None else None
         if flat is not None and flat.n != len(particles):
             raise ValueError(f"topology has {flat.n} atoms, particle list {len(particles)}")
-        b = DeviceBatch([(xyz, q, r, e, flat)], precision=self.precision)
+        if not np.all(np.isfinite(xyz)):
+            raise ValueError("non-finite coordinates")
+        b = self._batch(xyz, q, r, e, flat)
         return b.energy_terms()[0].cpu().numpy()
 
     def lowest_energy_structure(self, ensemble):

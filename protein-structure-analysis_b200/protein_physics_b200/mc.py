@@ -215,7 +215,9 @@ def generate_ensemble(engine, initial_state, topology, n_candidates, steps_per_c
     if n_candidates <= 0 or steps_per_cand <= 0:
         raise ValueError("ncand/steps must be positive")
     xyz, q, r, e = particle_arrays(initial_state)
-    batch = DeviceBatch([(xyz, q, r, e, flat)] * int(n_candidates), precision=engine.precision)
+    if not np.all(np.isfinite(xyz)):
+        raise ValueError("non-finite coordinates")
+    batch = engine._batch(xyz, q, r, e, flat, copies=int(n_candidates))
     runner = MCRunner(batch, temperature, engine._next_seed(), policy=0, cur_max0=max_angle)
     runner.run(steps_per_cand)
     X = batch.coords()
@@ -232,6 +234,8 @@ def run_landscape(engine, initial_state, topology, n_snapshots, steps_per_snapsh
     if n_snapshots <= 0 or steps_per_snapshot <= 0:
         raise ValueError("n_snapshots/steps_per_snapshot must be positive")
     xyz, q, r, e = particle_arrays(initial_state)
+    if not np.all(np.isfinite(xyz)):
+        raise ValueError("non-finite coordinates")
     batch = DeviceBatch([(xyz, q, r, e, flat)], precision=engine.precision)
     runner = MCRunner(batch, temperature, engine._next_seed(), policy=1, cur_max0=max_angle)
     snaps, energies = [], []
@@ -239,7 +243,7 @@ def run_landscape(engine, initial_state, topology, n_snapshots, steps_per_snapsh
         runner.run(steps_per_snapshot)
         X = batch.coords(0)
         snaps.append(particles_from(X, initial_state))
-        shot = DeviceBatch([(X, q, r, e, flat)], precision=engine.precision)
+        shot = engine._batch(X, q, r, e, flat)  # calculate_potential of the snapshot: fresh list
         energies.append(float(shot.energy_terms()[0, 4].item()))
     cur_max = float(runner.state()["cur_max"][0])
     return snaps, energies, cur_max

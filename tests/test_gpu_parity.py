@@ -190,3 +190,23 @@ def test_dropin_api(golden):
     assert eng.calculate_potential(P) == pytest.approx(golden["energy_notopo"][4], rel=1e-6)
     assert eng.calculate_potential([]) == 0.0
     assert "B200" in PhysicsEngine.device_name() or len(PhysicsEngine.device_name()) > 0
+
+
+def test_engine_reuses_batch_across_calls(golden):
+    """Repeated calls on one system reuse the device batch (coordinates
+    reloaded): energies equal a fresh engine's, also after the coordinates
+    change, and a different parameter set gets its own batch."""
+    from protein_physics_b200 import Particle, PhysicsEngine
+    T = golden.topology()
+    eng = PhysicsEngine()
+    P = [Particle(*x, q, r, e) for x, q, r, e in zip(golden["xyz"], golden["q"], golden["r"], golden["eps"])]
+    E1 = eng.calculate_potential(P, T)
+    x2 = np.asarray(golden["xyz"]) + np.random.default_rng(2).normal(0, 0.05, (golden.n, 3))
+    P2 = [Particle(*x, q, r, e) for x, q, r, e in zip(x2, golden["q"], golden["r"], golden["eps"])]
+    E2 = eng.calculate_potential(P2, T)
+    assert len(eng._batches) == 1
+    assert E2 == PhysicsEngine().calculate_potential(P2, T)
+    assert eng.calculate_potential(P, T) == E1
+    P3 = [Particle(*x, 0.5 * q, r, e) for x, q, r, e in zip(golden["xyz"], golden["q"], golden["r"], golden["eps"])]
+    assert eng.calculate_potential(P3, T) == PhysicsEngine().calculate_potential(P3, T)
+    assert len(eng._batches) == 2
