@@ -245,7 +245,9 @@ def run_ours(args, rank, world, local):
             "tuned": {"cluster_size": tuned[0], "threads_per_system": tuned[1], "spec_teams": tuned[2]},
             "wall_s": t_wall,
             "e2e": {"value": e2e_val, "unit": "proposals/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "api": "PhysicsEngine.generate_ensemble(host particles, topology, 1, 1000)"},
+                    "api": "PhysicsEngine.generate_ensemble(host particles, topology, 1, 1000)",
+                    "workload": "the reference's own move policy (25 % crankshaft, every rotatable bond), as the "
+                                "reference arm runs it: heavier moves and more list rebuilds than the timed value"},
             "roofline": {"bound": "fp32", "kernel": ("mc_spec_kernel<float,%d,%d> x %d teams" % (tuned[1], tuned[0], tuned[2])
                                                     if tuned[2] > 1 else "mc_kernel<float,%d,%d>" % (tuned[1], tuned[0])),
                          "achieved": achieved / 1e12,
