@@ -342,9 +342,7 @@ __global__ void mala_accept_kernel(int nsys, const int32_t *__restrict__ rb_off,
         if (cfg.tune_freq > 0 && ++S.tot_win == cfg.tune_freq) {
             const double rate = (double)S.acc_win / (double)cfg.tune_freq;
             if (rate > cfg.target_hi) S.scale = fmin(cfg.scale_max, S.scale * cfg.scale_up);
-            else if (rate < cfg.target_lo)  // a window without one acceptance shrinks twice as fast
-                S.scale = fmax(cfg.scale_min, S.scale * (S.acc_win == 0 ? cfg.scale_down * cfg.scale_down
-                                                                          : cfg.scale_down));
+            else if (rate < cfg.target_lo) S.scale = fmax(cfg.scale_min, S.scale * cfg.scale_down);
             S.acc_win = 0;
             S.tot_win = 0;
         }
