@@ -36,7 +36,7 @@ class ReplicaExchange:
     restricted to `moveset` when given)."""
 
     def __init__(self, system, temps_K, seed, mala_fraction=0.25, mala_step=np.radians(0.5), moveset=None,
-                 precision="mixed", minimize_steps=0, cluster_size=None, threads=0):
+                 precision="mixed", minimize_steps=0, mala_warmup=0, cluster_size=None, threads=0):
         temps_K = np.asarray(temps_K, np.float64)
         if np.any(np.diff(temps_K) < 0):
             raise ValueError("temperatures must ascend")
@@ -49,6 +49,8 @@ class ReplicaExchange:
         ms = [moveset] * self.R if moveset is not None else None
         self.mc = MCRunner(self.batch, T, seed, policy=2, moveset=ms, cluster_size=cluster_size, threads=threads)
         self.mala = MALARunner(self.batch, T, seed + 1, step=mala_step, ts=self.ts)
+        if mala_warmup:  # let the MALA step scale adapt before sampling starts
+            self.mala.run(int(mala_warmup))
         self.mala_fraction = float(mala_fraction)
         self.seed = int(seed) & ((1 << 64) - 1)
         self.sys_of_temp = torch.arange(self.R, dtype=torch.int32, device="cuda")

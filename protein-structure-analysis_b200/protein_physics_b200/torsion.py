@@ -208,9 +208,7 @@ class MALARunner:
             raise ValueError("temperature must be positive")
         st = np.zeros(batch.nsys, dtype=_lib.MALA_STATE_DTYPE)
         st["beta"] = 1.0 / T
-        # every bond moves at once: start the step scale at sqrt(100 / bonds)
-        # (the adaptation takes it from there)
-        st["scale"] = np.minimum(1.0, np.sqrt(100.0 / np.maximum(np.diff(batch.rb_off_h), 1)))
+        st["scale"] = 1.0
         self.states = torch.from_numpy(st.view(np.uint8).copy()).to("cuda")
         kind = batch.rb_kind_h
         sig = float(step) * batch.rb_scale_h * np.where(kind == 2, sidechain_mult, 1.0)

@@ -161,7 +161,7 @@ def test_mala_log_alpha_matches_host(oracle):
     R.step()
     st1 = R.state()
     delta = R.delta.cpu().numpy()[:flat.nrb]
-    sig = R.sigma.cpu().numpy()[:flat.nrb] * st0["scale"][0]  # the proposal's sigma
+    sig = R.sigma.cpu().numpy()[:flat.nrb] * st0["scale"][0]  # the proposal's sigma (scale 1 at the start)
     x1 = _sequential(x0, T, flat, delta)
     E0 = oracle.calculate_potential(x0, g["q"], g["r"], g["eps"], TopoArrays(flat))[4]
     E1 = oracle.calculate_potential(x1, g["q"], g["r"], g["eps"], TopoArrays(flat))[4]
