@@ -569,7 +569,7 @@ def run_replica(args):
     F = flatten(T)
     moveset = [k for k in range(F.nrb) if F.side_count[k] <= 0.25 * F.n]
     RE = ReplicaExchange((ch.xyz, ch.charge, ch.radius, ch.epsilon, F), geometric_ladder(300, 450, 16), seed=9,
-                         moveset=moveset, minimize_steps=100, mala_warmup=200)
+                         moveset=moveset, minimize_steps=500, mala_warmup=400)
     for _ in range(args.warmup):
         RE.interval(100)
     torch.cuda.synchronize()
