@@ -194,10 +194,15 @@ class DeviceBatch:
 
     @property
     def batch_s(self):
-        b = _lib.AlmaBatch()
-        b.nsys, b.natoms = self.nsys, self.natoms
-        b.atom_off, b.xyz, b.prm, b.prm64 = _ptr(self.atom_off), _ptr(self.xyz), _ptr(self.prm), _ptr(self.prm64)
-        b.born, b.status = _ptr(self.born), _ptr(self.status)
+        """The AlmaBatch of this batch (built once: its buffers never move;
+        the SASA cache pointer follows sasa_valid on every access)."""
+        b = getattr(self, "_batch_s", None)
+        if b is None:
+            b = _lib.AlmaBatch()
+            b.nsys, b.natoms = self.nsys, self.natoms
+            b.atom_off, b.xyz, b.prm, b.prm64 = _ptr(self.atom_off), _ptr(self.xyz), _ptr(self.prm), _ptr(self.prm64)
+            b.born, b.status = _ptr(self.born), _ptr(self.status)
+            self._batch_s = b
         b.sasa = _ptr(self.sasa) if self.sasa_valid else None
         return b
 
@@ -207,6 +212,7 @@ class DeviceBatch:
 
     # ---- neighbor list ---------------------------------------------------------
     def _alloc_nl(self, need):
+        self._nl_s = None
         sizes = np.diff(self.atom_off_h).astype(np.int64)
         if need is None:
             caps = [sizes * self.NL_FULL_PER_ATOM + 64, sizes * self.NL_HALF_PER_ATOM + 64,
@@ -244,6 +250,9 @@ class DeviceBatch:
 
     @property
     def nl_s(self):
+        """The AlmaNL of the list buffers (rebuilt after _alloc_nl moves them)."""
+        if getattr(self, "_nl_s", None) is not None:
+            return self._nl_s
         nl = _lib.AlmaNL()
         nl.full_ptr, nl.full_len, nl.full_cols, nl.full_base = (_ptr(self.full_ptr), _ptr(self.full_len),
                                                                 _ptr(self.full_cols), _ptr(self.full_base))
@@ -254,6 +263,7 @@ class DeviceBatch:
                                                                     _ptr(self.sfull_cols), _ptr(self.sfull_base))
         nl.shalf_ptr, nl.shalf_len, nl.shalf_cols, nl.shalf_base = (_ptr(self.shalf_ptr), _ptr(self.shalf_len),
                                                                     _ptr(self.shalf_cols), _ptr(self.shalf_base))
+        self._nl_s = nl
         return nl
 
     def _sp(self):
