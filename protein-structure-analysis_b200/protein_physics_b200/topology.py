@@ -118,12 +118,19 @@ class BondTopology:
         self.concerted_sidechain_pairs: list[tuple[int, int]] = []
         self.disulfide_pairs: list[tuple[int, int]] = []
         self.atomnames: list[str] = []
+        # Bumped by every method that changes the topology; ``flatten`` keys
+        # its cached arrays on it.  The reference exposes these attributes
+        # read-only (physics_engine.cpp:3732-3740), so the methods below are
+        # the only way its state changes.
+        self._version = 0
+        self._flat = None
 
     # ---- build (physics_engine.cpp:1341-1597) --------------------------------
     def build(self, resnames, atomnames, res_idx):
         n = len(resnames)
         if len(atomnames) != n or len(res_idx) != n:
             raise ValueError("resnames, atomnames and res_idx must have the same length")
+        self._version += 1
         self.N = n
         self.adj = [[] for _ in range(n)]
         self.bonds = []
@@ -238,6 +245,7 @@ class BondTopology:
             return
         if i > j:
             i, j = j, i
+        self._version += 1
         self.disulfide_pairs.append((i, j))
         row = self.excl[i]
         if j not in row:
@@ -247,6 +255,7 @@ class BondTopology:
     # ---- concerted sidechain pairs (:1640-1673) ------------------------------
     def identify_concerted_sidechain_pairs(self, init_coords, cutoff=6.0):
         xyz = _coords(init_coords)
+        self._version += 1
         self.concerted_sidechain_pairs = []
         cut2 = cutoff * cutoff
         sc = [k for k, rb in enumerate(self.rot_bonds) if rb.kind == BondKind.SIDECHAIN]
@@ -416,7 +425,26 @@ def _compact_from_lists(sides):
 
 
 def flatten(topo) -> FlatTopology:
-    """CSR arrays from this module's BondTopology or the reference's."""
+    """CSR arrays from this module's BondTopology or the reference's.
+
+    For this module's BondTopology the result is cached until one of its
+    mutating methods runs; the reference's objects are flattened each call.
+    The returned arrays are shared between calls and must not be written."""
+    ver = getattr(topo, "_version", None)
+    if ver is not None:
+        hit = getattr(topo, "_flat", None)
+        if hit is not None and hit[0] == ver:
+            return hit[1]
+        flat = _flatten(topo)
+        for a in vars(flat).values():
+            if isinstance(a, np.ndarray):
+                a.flags.writeable = False
+        topo._flat = (ver, flat)
+        return flat
+    return _flatten(topo)
+
+
+def _flatten(topo) -> FlatTopology:
     n = int(topo.num_atoms)
     excl_ptr, excl_cols = _csr(list(topo.excl))
     comp = getattr(topo, "_sides", None)

@@ -78,3 +78,22 @@ def test_reference_topology_flattens_identically(golden):
               "side_hi", "dih_abcd", "term_off", "term_v2", "term_n", "term_gamma", "ss", "conc_sc"):
         assert np.array_equal(getattr(A, k), getattr(B, k)), k
     assert sorted(map(tuple, A.crank)) == sorted(map(tuple, B.crank))
+
+
+def test_flatten_cache_follows_mutations(golden):
+    """flatten() reuses its arrays until build / add_disulfide /
+    identify_concerted_sidechain_pairs change the topology."""
+    from protein_physics_b200.topology import BondTopology, flatten
+    T = BondTopology()
+    T.build(golden.resnames, golden.atomnames, golden.res_idx)
+    a = flatten(T)
+    assert flatten(T) is a
+    assert not a.excl_cols.flags.writeable
+    T.add_disulfide(0, golden.n - 1)
+    b = flatten(T)
+    assert b is not a and len(b.ss) == len(a.ss) + 1
+    T.identify_concerted_sidechain_pairs(golden["xyz"])
+    c = flatten(T)
+    assert c is not b and len(c.conc_sc) == len(T.concerted_sidechain_pairs)
+    T.build(golden.resnames[:10], golden.atomnames[:10], golden.res_idx[:10])
+    assert flatten(T).n == 10
