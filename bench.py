@@ -94,7 +94,7 @@ def _coil_chain(n_res, seed):
     return synth.coil_chain(n_res, seed)
 
 
-def make_workload(kind, rank):
+def make_workload(kind, rank, n_chains=256):
     from protein_physics_b200 import synth
     from protein_physics_b200.dist import rank_seed
     from protein_physics_b200.topology import BondTopology, flatten
@@ -105,12 +105,12 @@ def make_workload(kind, rank):
         import multiprocessing as mp
         import numpy as np
         rng = np.random.default_rng(rank_seed(3, rank))
-        sizes = rng.integers(50, 601, size=256)
+        sizes = rng.integers(50, 601, size=256)[:n_chains]
         jobs = [(int(n), rank_seed(k, rank)) for k, n in enumerate(sizes)]
         # chain generation is host Python: spread it over the host cores
         with mp.get_context("spawn").Pool(min(32, os.cpu_count() or 1)) as pool:
             chains = pool.starmap(_coil_chain, jobs, chunksize=1)
-        temps = list(280.0 * (400.0 / 280.0) ** (np.arange(256) / 255.0) * KB)
+        temps = list(280.0 * (400.0 / 280.0) ** (np.arange(256) / 255.0) * KB)[:n_chains]
     systems, movesets, topos = [], [], []
     for ch in chains:
         T = BondTopology()
@@ -223,7 +223,7 @@ def run_ours(args, rank, world, local):
         value = prop_total / (ms_max * 1e-3)
         cpu = cpu_baseline(chains[0], topos[0], temps[0], args) if world == 1 else None
         plain = plain_gpu_baseline(chains[0], temps[0]) if (world == 1 and args.workload == "single") else None
-        ef = energy_force_rate(systems[0])
+        ef = energy_force_rate(systems[0], topos[0])
         out = {
             "metric": "Metropolis proposals/s", "value": value, "unit": "proposals/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
@@ -348,13 +348,24 @@ def plain_gpu_baseline(ch, T, budget_s=8.0):
     t0 = time.perf_counter()
     eng.generate_ensemble(P, R, 1, n, T, 0.12)
     dt = time.perf_counter() - t0
+    # its full-energy path (the reference has no forces): calculate_potential
+    eng.calculate_potential(P, R)
+    t0 = time.perf_counter()
+    ne = 0
+    while time.perf_counter() - t0 < 2.0 or ne < 3:
+        eng.calculate_potential(P, R)
+        ne += 1
+    de = time.perf_counter() - t0
     return {"value": n / dt, "unit": "proposals/s", "proposals": n, "seconds": dt,
             "what": "reference protein_physics_cuda.generate_ensemble(chain, 1 candidate) on this B200 "
                     "(physics_engine_cuda.cu built unmodified for sm_100a; host SASA and two H2D/D2H round "
-                    "trips per proposal)"}
+                    "trips per proposal)",
+            "energy": {"value": ne / de, "unit": "energy evals/s", "evals": ne, "seconds": de,
+                       "what": "reference protein_physics_cuda calculate_potential(particles, topology) on the "
+                               "same chain (energy only: the reference has no gradient)"}}
 
 
-def energy_force_rate(system, steps=20):
+def energy_force_rate(system, topo, steps=20):
     """Full energy + analytic gradient evaluations per second on one system:
     neighbor-list build, Born radii, energy terms and alma_forces per eval
     (device events, inputs resident)."""
@@ -376,6 +387,7 @@ def energy_force_rate(system, steps=20):
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for _ in range(steps):
         ev()
@@ -384,10 +396,29 @@ def energy_force_rate(system, steps=20):
     for _ in range(steps):
         b.forces(out=grad)
     f1.record()
+    g0.record()
+    for _ in range(steps):
+        b.nl_ready = False
+        b.build_nl(check=False)
+        b.energy_terms(recompute_born=True, out=terms)
+    g1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / steps
+    # the same energy through the public API, host particles in and a float out
+    from protein_physics_b200 import Particle, PhysicsEngine
+    xyz, q, r, eps, flat = system
+    P = [Particle(*map(float, x), float(qq), float(rr), float(ee)) for x, qq, rr, ee in zip(xyz, q, r, eps)]
+    eng = PhysicsEngine(precision="mixed")
+    eng.calculate_potential(P, topo)
+    t0 = time.perf_counter()
+    ne = 0
+    while time.perf_counter() - t0 < 1.0 or ne < 3:
+        eng.calculate_potential(P, topo)
+        ne += 1
+    api = ne / (time.perf_counter() - t0)
     return {"value": 1e3 / ms, "unit": "energy+force evals/s", "atoms": b.natoms, "ms_per_eval": ms,
-            "forces_ms": f0.elapsed_time(f1) / steps,
+            "forces_ms": f0.elapsed_time(f1) / steps, "energy_only_ms": g0.elapsed_time(g1) / steps,
+            "calculate_potential_per_s": api,
             "what": "neighbor list + Born radii + energy terms + analytic dE/dx (alma_forces), mixed precision"}
 
 
@@ -456,7 +487,7 @@ def run_globule(args):
     T = BondTopology()
     T.build(ch.resnames, ch.atomnames, ch.res_idx)
     system = (ch.xyz, ch.charge, ch.radius, ch.epsilon, flatten(T))
-    ef = energy_force_rate(system)
+    ef = energy_force_rate(system, T)
     b = DeviceBatch([system], precision="mixed")
     ts = TorsionSpace(b)
     torch.cuda.synchronize()
@@ -598,10 +629,22 @@ def run_profile_case(args):
     proposals, then exactly one mc launch of up to 200 proposals (it stops
     at the first drift flag); --config CL,NT[,K] picks the launch shape.
     "forces": the same chain, one energy evaluation and one alma_forces
-    call (4 gradient kernels)."""
+    call (4 gradient kernels).  "energy": the first 48 chains of the batched
+    workload (about 0.26M atoms, rows well above L2), one neighbor-list
+    build and one full energy evaluation."""
     import torch
     from protein_physics_b200.device import DeviceBatch
     from protein_physics_b200.mc import MCRunner
+    if args.profile == "energy":
+        chains, systems, _, _, _ = make_workload("batched", 0, n_chains=48)
+        batch = DeviceBatch(systems, precision="mixed")
+        batch.build_nl()
+        terms = batch.energy_terms()
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_case": "energy", "systems": len(chains), "atoms": batch.natoms,
+                          "half_entries": int(batch.half_len.sum()), "full_entries": int(batch.full_len.sum()),
+                          "total_energy": float(terms[:, 4].sum())}))
+        return
     chains, systems, movesets, temps, topos = make_workload("single", 0)
     batch = DeviceBatch(systems, precision="mixed")
     if args.profile == "forces":
@@ -625,8 +668,9 @@ def run_profile_case(args):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--profile", nargs="?", const="mc", default=None, choices=["mc", "forces"],
-                    help="a small case for ncu: one mc launch (mc) or one gradient evaluation (forces)")
+    ap.add_argument("--profile", nargs="?", const="mc", default=None, choices=["mc", "forces", "energy"],
+                    help="a small case for ncu: one mc launch (mc), one gradient evaluation (forces) "
+                         "or one batched list build + energy evaluation (energy)")
     ap.add_argument("--config", default="", help="CL,NT[,K]: cluster size, CTA size and speculative teams "
                                                  "instead of the autotuner")
     ap.add_argument("--cluster", type=int, default=16)

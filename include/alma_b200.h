@@ -152,6 +152,13 @@ typedef struct {
     int32_t *shalf_len;
     uint32_t *shalf_cols;
     const int64_t *shalf_base;
+    int32_t *full_span;       /* [natoms*2] optional (NULL: not kept): the
+                               * smallest and largest atom index in each full
+                               * row at the last build (INT32_MAX, -1 for an
+                               * empty row).  A moved atom whose span lies in
+                               * its side's atom range has no neighbour that
+                               * stays behind, so the move kernels skip its
+                               * cross-pair and SASA-mark scans. */
 } AlmaNL;
 
 /* ---- library ------------------------------------------------------------ */

@@ -396,7 +396,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) mc_kernel(MoveCtx C, MCConfigDev
         if (threadIdx.x == 0) accept = (r.dE < 0.0) || (u[3] < exp(-r.dE / S.temperature));
         __syncthreads();
         const int acc = accept;
-        move_finish<CL>(C, M, s, acc, parity, T);
+        move_finish<R, CL>(C, M, s, acc, parity, T);
         // commits and the drift flag visible to every CTA before the state
         // update and the next proposal's coordinate reads
         T.sync();
@@ -501,6 +501,7 @@ __device__ __forceinline__ MoveScratch scratch_at(const MoveScratch &w, size_t o
     t.hct_part = sh(w.hct_part);
     t.cross_part = sh(w.cross_part);
     t.affected = sh(w.affected);
+    t.edge = sh(w.edge);
     t.queue = sh(w.queue);
     t.drift = sh(w.drift);
     return t;  // work counters and phase timers stay shared (team 0's)
@@ -617,7 +618,7 @@ mc_spec_kernel(MoveCtx C, MCConfigDev cfg, AlmaChainState *__restrict__ states, 
         __syncthreads();
         const int a = a_sh;
         if (did_move) {
-            move_finish<CL>(Cq, M, s, q == a, parity, T);
+            move_finish<R, CL>(Cq, M, s, q == a, parity, T);
             T.sync();  // the commit and its drift flag, within the team
             if (q == a && T.rank == 0 && threadIdx.x == 0 && Cq.w.drift[2 * s + parity])
                 Rd->slot[rp][q].flags |= 8;

@@ -22,6 +22,7 @@ static size_t carve_scratch(MoveScratch *w, char *base, int32_t natoms) {
     t.born_new = (double *)take(sizeof(double) * (size_t)natoms);
     t.dE_atom = (double *)take(sizeof(double) * 2 * (size_t)natoms);
     t.affected = (int32_t *)take(sizeof(int32_t) * (size_t)natoms);
+    t.edge = (int32_t *)take(sizeof(int32_t) * (size_t)natoms);
     t.hct_part = (double *)take(sizeof(double) * MAX_WPR * (size_t)natoms);
     t.cross_part = (double *)take(sizeof(double) * MAX_WPR * (size_t)natoms);
     t.ctr = (unsigned long long *)take(sizeof(unsigned long long) * 4 * (size_t)(natoms + 1));
@@ -68,7 +69,7 @@ __global__ void __launch_bounds__(MOVE_THREADS) move_dE_kernel(MoveCtx C, const 
         dterms[4 * (size_t)s + 2] = r.ddih;
         dterms[4 * (size_t)s + 3] = r.dss;
     }
-    move_finish<1>(C, M, s, apply, 0, T);
+    move_finish<R, 1>(C, M, s, apply, 0, T);
 }
 
 }  // namespace alma

@@ -17,7 +17,12 @@
 //   * SASA is recomputed only for atoms whose half row holds an atom of a
 //     different group (moved atoms, plus fixed atoms that list a moved atom)
 //     — every other atom's SASA is unchanged bit for bit;
-//   * dihedral records are tested for a mixed group pattern.
+//   * dihedral records are tested for a mixed group pattern;
+//   * a moved atom whose full row lies inside its side's atom range (the
+//     row's index span, kept by the list build) has no partner that stays
+//     behind: it skips the cross-pair and SASA-mark scans, and its new Born
+//     radius (which no cross pair reads) is computed only when the move is
+//     accepted — a move of half the chain scans only the rows at the cut.
 // Per-atom contributions land in dE_atom[2*i] (cross) / dE_atom[2*i+1]
 // (SASA) and are summed in atom order, so the result is deterministic.
 #pragma once
@@ -128,13 +133,16 @@ struct MoveScratch {
     double *cross_part; // [natoms*MAX_WPR] per-segment cross-pair ΔE of moved atoms
     int32_t *affected;  // [natoms] atoms whose SASA is recomputed (per-system
                         // region), appended during the marking pass
+    int32_t *edge;      // [natoms] moved atoms with a neighbour outside their
+                        // rigid body (per-system region), appended in P1
     unsigned long long *ctr;  // [4*nsys] cumulative work counters: pair terms,
                               // hct terms, SASA neighbour visits, moved atoms
     unsigned long long *phase;  // [4*nsys] cumulative SM cycles of rank 0 in
                                 // the four phases of move_eval (+ finish)
-    int *queue;               // [8*nsys] per proposal parity: [2] = a trial
-                              // atom is beyond half the skin, [3] = affected
-                              // atoms (other slots reserved), two parities
+    int *queue;               // [8*nsys] per proposal parity: [1] = edge
+                              // atoms, [2] = a trial atom is beyond half the
+                              // skin, [3] = affected atoms (slot 0 reserved),
+                              // two parities
     int *drift;               // [2*nsys] drift flags, two proposals
 };
 
@@ -341,6 +349,31 @@ __device__ __forceinline__ int member(const MoveDesc &M, const int32_t *side_idx
     return side_atom(M.mem[g], side_idx, k);
 }
 
+// True when every neighbour in member m's full row lies in the atom range
+// of m's own rigid body, read from the row's index span: then the row holds
+// no cross pair (all partners move with m) and no pair whose distance
+// changes (no SASA mark), so the cross-pair and marking scans of m add
+// nothing and are skipped.  A torsion's body is its j-side range; a
+// crankshaft's psi-side atoms (body 2) need their span inside both sides'
+// ranges; the phi-only atoms of a crankshaft and the members of a concerted
+// pair (two groups) always scan.  Atoms of a side's explicit list are not in
+// its range, so a row that reaches one scans too.
+// Moves of fewer members scan every row: the skip would save little and
+// its edge-list reads sit on the phase's critical path.
+constexpr int INNER_MIN_MEMBERS = 128;
+
+// body < 0: not known to the caller (looked up for a crankshaft).
+__device__ __forceinline__ bool inner_member(const MoveCtx &C, const MoveDesc &M, int m, int body = -1) {
+    if (C.nl.full_span == nullptr || M.kind == 2 || n_members(M) < INNER_MIN_MEMBERS) return false;
+    const int2 sp = *reinterpret_cast<const int2 *>(C.nl.full_span + 2 * (size_t)m);
+    const SideRef &A = M.mem[0];
+    if (sp.x < A.lo || sp.y >= A.hi) return false;
+    if (M.kind == 0) return true;
+    const SideRef &B = M.rot[1].side;
+    if (sp.x < B.lo || sp.y >= B.hi) return false;
+    return body < 0 ? side_has(B, C.t.side_idx, m) : body == 2;
+}
+
 // Whole-CTA evaluation of a decoded, non-degenerate proposal of system s.
 // smem_d: >= 128 doubles; s_nAff: shared counter.  Leaves group/xyz_new/
 // born_new set for the members (the caller commits or discards, then calls
@@ -444,26 +477,43 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
     // P1: move groups, rigid bodies and the proposed coordinates — every
     // rotation applied in order (the crankshaft's second rotation turns its
     // psi side again, taking the axis from the post-phi positions).
-    for (int64_t k = tid; k < nm; k += nthr) {
-        int g;
-        const int m = member(M, t.side_idx, k, g);
-        double4 p = ld_xyz(b.xyz, m);
-        int body = g + 1;
-        if (M.kind == 2) {
-            rodrigues(p.x, p.y, p.z, M.rot[g]);
-        } else {
-            rodrigues(p.x, p.y, p.z, M.rot[0]);
-            if (M.kind == 1 && side_has(M.rot[1].side, t.side_idx, m)) {
-                rodrigues(p.x, p.y, p.z, M.rot[1]);
-                body = 2;
+    // Members whose rows reach outside their body go to the edge list (one
+    // atomic per warp); only these scan rows for cross pairs and SASA marks.
+    for (int64_t k0 = tid - lane; k0 < nm; k0 += nthr) {
+        const int64_t k = k0 + lane;
+        bool edge = false;
+        int m = 0;
+        if (k < nm) {
+            int g;
+            m = member(M, t.side_idx, k, g);
+            double4 p = ld_xyz(b.xyz, m);
+            int body = g + 1;
+            if (M.kind == 2) {
+                rodrigues(p.x, p.y, p.z, M.rot[g]);
+            } else {
+                rodrigues(p.x, p.y, p.z, M.rot[0]);
+                if (M.kind == 1 && side_has(M.rot[1].side, t.side_idx, m)) {
+                    rodrigues(p.x, p.y, p.z, M.rot[1]);
+                    body = 2;
+                }
             }
+            w.group[m] = (int8_t)(g + 1);
+            w.body[m] = (int8_t)body;
+            *reinterpret_cast<double4 *>(w.xyz_new + 4 * (size_t)m) = p;
+            if (rows_ok && d2_of(p, ld_xyz(C.nl.ref_xyz, m)) > C.P.half_skin2) q[2] = 1;
+            edge = !inner_member(C, M, m, body);
         }
-        w.group[m] = (int8_t)(g + 1);
-        w.body[m] = (int8_t)body;
-        *reinterpret_cast<double4 *>(w.xyz_new + 4 * (size_t)m) = p;
-        if (rows_ok && d2_of(p, ld_xyz(C.nl.ref_xyz, m)) > C.P.half_skin2) q[2] = 1;
+        const unsigned em = __ballot_sync(0xffffffffu, edge);
+        if (em) {
+            int base = 0;
+            if (lane == 0) base = atomicAdd(&q[1], __popc(em));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (edge) w.edge[a0 + base + __popc(em & ((1u << lane) - 1u))] = m;
+        }
     }
     T.sync();
+    const int64_t ne = q[1];
+    const bool by_edge = ne < nm;  // else every member scans: take them in member order
     const bool short_rows = rows_ok && q[2] == 0;
     if (timer) {
         const long long t1 = clock64();
@@ -479,23 +529,25 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
         w.drift[2 * s + (parity ^ 1)] = 0;
     }
 
-    // P2: half-list Born radii of the members at the new geometry (P4
-    // semantics) and SASA marks.  SASA reach: atoms i < j interact when j is
+    // P2: half-list Born radii of the edge members at the new geometry
+    // (update_born semantics) and SASA marks.  SASA reach: atoms i < j interact when j is
     // in i's half row and r < R*_i + R*_j + 2 probe; a pair whose distance
     // changes (rigid bodies differ) and is within reach before or after the
     // move changes the SASA of its lower atom only: mark that atom.
-    // Two task sets over the team's warps — Born segments of the moved rows,
+    // Two task sets over the team's warps — Born segments of the edge rows,
     // then mark segments — so the two kinds of work land on different warps.
+    // Only edge members take part in cross pairs, so only their new radii
+    // enter ΔE; the other members' radii are computed by the commit.
     const int wid = T.gwarp(), nw = T.gwarps();
-    const int wph = rows_wpr(2 * nm, nw);
-    const int64_t nhct = nm * wph;
+    const int wph = rows_wpr(2 * ne, nw);
+    const int64_t nhct = ne * wph;
     for (int64_t it = wid; it < 2 * nhct; it += nw) {
         const bool marking = it >= nhct;
         const int64_t i2 = marking ? it - nhct : it;
         const int64_t k = i2 / wph;
         const int seg = (int)(i2 % wph);
         int g;
-        const int m = member(M, t.side_idx, k, g);
+        const int m = by_edge ? w.edge[a0 + k] : member(M, t.side_idx, k, g);
         const double4 pm = ld_xyz(w.xyz_new, m);
         if (!marking) {
         R qm, rm, em;
@@ -548,8 +600,8 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
     // the rows allow), then the affected atoms' SASA, which wraps round onto
     // the warps: a short SASA row after a half row beats a full row.
     const int naff = q[3];
-    const int wpc = rows_wpr(nm, nw);
-    const int64_t ncross = nm * wpc;
+    const int wpc = rows_wpr(ne, nw);
+    const int64_t ncross = ne * wpc;
     const double pi4 = 4.0 * 3.14159265358979323846, pi2 = 2.0 * 3.14159265358979323846;
     unsigned long long nsasa = 0;
     for (int64_t it = wid; it < ncross + naff; it += nw) {
@@ -560,8 +612,8 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
         const int64_t k = it / wpc;
         const int seg = (int)(it % wpc);
         int g;
-        const int m = member(M, t.side_idx, k, g);
-        const int gm = g + 1;
+        const int m = by_edge ? w.edge[a0 + k] : member(M, t.side_idx, k, g);
+        const int gm = by_edge ? (int)w.group[m] : g + 1;
         const double4 pmo = ld_xyz(b.xyz, m), pmn = ld_xyz(w.xyz_new, m);
         R qm, rm, em;
         prm_of<R>(b.prm, b.prm64, m, qm, rm, em);
@@ -676,12 +728,14 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
         t0 = t1;
     }
 
-    // P4: deterministic sums — per-atom slots in atom order, then the CTA
-    // partials in rank order.
+    // P4: deterministic sums — per-atom slots in member / atom order (edge
+    // members only: the others have no cross pair), then the CTA partials in
+    // rank order.
     double c = 0.0, sa = 0.0;
     for (int64_t k = tid; k < nm; k += nthr) {
         int g;
         const int m = member(M, t.side_idx, k, g);
+        if (by_edge && inner_member(C, M, m, w.body[m])) continue;
         for (int sg = 0; sg < wpc; ++sg) c += w.cross_part[(size_t)m * MAX_WPR + sg];
     }
     for (int i = a0 + tid; i < a1; i += nthr) sa += w.dE_atom[2 * (size_t)i + 1];
@@ -701,13 +755,43 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
 // committed atom that drifted more than half the skin from its position at
 // the last list build in w.drift[2s + parity] (read after the caller's
 // next team barrier).
-template <int CL>
+//
+// An accepted move also gives its non-edge members their half-list Born
+// radii at the new geometry (update_born, physics_engine.cpp:2043-2051):
+// one warp per such member, whose half row holds members only, so every
+// position comes from xyz_new and nothing the commit writes is read.
+template <typename R, int CL>
 __device__ inline void move_finish(const MoveCtx &C, const MoveDesc &M, int s, int accept, int parity,
                                    const Team<CL> &T) {
     const MoveScratch &w = C.w;
     const int tid = T.gtid(), nthr = T.gthreads();
     const int a0 = C.b.atom_off[s];
     const int64_t nm = n_members(M);
+    if (accept && C.nl.full_span != nullptr && M.kind != 2 && nm >= INNER_MIN_MEMBERS) {
+        const int lane = threadIdx.x & 31, wid = T.gwarp(), nw = T.gwarps();
+        unsigned long long nh = 0;
+        for (int64_t k = wid; k < nm; k += nw) {
+            int g;
+            const int m = member(M, C.t.side_idx, k, g);
+            if (!inner_member(C, M, m)) continue;
+            R qm, rm, em;
+            prm_of<R>(C.b.prm, C.b.prm64, m, qm, rm, em);
+            const double4 pm = ld_xyz(w.xyz_new, m);
+            const int64_t hb = C.nl.half_ptr[m], he = hb + C.nl.half_len[m];
+            double sum = 0.0;
+            for (int64_t e = hb + lane; e < he; e += 32) {
+                const int j = (int)(C.nl.half_cols[e] & ALMA_IDX_MASK);
+                R qj, rj, ej;
+                prm_of<R>(C.b.prm, C.b.prm64, j, qj, rj, ej);
+                const R r2 = (R)d2_of(pm, ld_xyz(w.xyz_new, j));
+                sum += (double)hct_term<R>(m_sqrt(r2), r2, rm, rj);
+            }
+            sum = warp_sum(sum);
+            if (lane == 0) C.b.born[m] = 1.0 / fmax(1.0 / C.b.prm64[4 * (size_t)m + 1] - 0.5 * sum, 2.0);
+            nh += (unsigned long long)(he - hb);
+        }
+        if (lane == 0 && nh) atomicAdd(&w.ctr[4 * s + 1], nh);
+    }
     int drift = 0;
     for (int64_t k = tid; k < nm; k += nthr) {
         int g;
@@ -715,7 +799,7 @@ __device__ inline void move_finish(const MoveCtx &C, const MoveDesc &M, int s, i
         if (accept) {
             const double4 p = ld_xyz(w.xyz_new, m);
             *reinterpret_cast<double4 *>(C.b.xyz + 4 * (size_t)m) = p;
-            C.b.born[m] = w.born_new[m];
+            if (!inner_member(C, M, m, w.body[m])) C.b.born[m] = w.born_new[m];
             if (C.nl.ref_xyz && d2_of(p, ld_xyz(C.nl.ref_xyz, m)) > C.P.half_skin2) drift = 1;
         }
         w.group[m] = 0;

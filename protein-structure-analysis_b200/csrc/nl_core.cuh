@@ -79,6 +79,7 @@ __device__ __forceinline__ void nl_row_atom(int i, int lane, const SysGrid &g, c
         if (lane == 0) *reinterpret_cast<double4 *>(nl.ref_xyz + 4 * (size_t)i) = pi;
     }
     nfull = nhalf = nsfull = nshalf = 0;
+    int jmin = 0x7fffffff, jmax = -1;  // index span of the full row (PASS 1)
     for (int dz = -1; dz <= 1; ++dz) {
         const int cz2 = cz + dz;
         if (cz2 < 0 || cz2 >= g.nz) continue;
@@ -108,6 +109,8 @@ __device__ __forceinline__ void nl_row_atom(int i, int lane, const SysGrid &g, c
                     const unsigned msf = __ballot_sync(0xffffffffu, sh);
                     const unsigned msh = __ballot_sync(0xffffffffu, sh && j > i);
                     if (PASS == 1 && in) {
+                        jmin = min(jmin, j);
+                        jmax = max(jmax, j);
                         const unsigned lt = (1u << lane) - 1u;
                         const uint32_t e = (uint32_t)j | (excluded(excl_ptr, excl_cols, i, j) ? ALMA_EXCL_BIT : 0u);
                         nl.full_cols[fo + nfull + __popc(mf & lt)] = e;
@@ -123,6 +126,14 @@ __device__ __forceinline__ void nl_row_atom(int i, int lane, const SysGrid &g, c
                     nshalf += __popc(msh);
                 }
             }
+        }
+    }
+    if (PASS == 1 && nl.full_span != nullptr) {
+        jmin = __reduce_min_sync(0xffffffffu, jmin);
+        jmax = __reduce_max_sync(0xffffffffu, jmax);
+        if (lane == 0) {
+            nl.full_span[2 * (size_t)i] = jmin;
+            nl.full_span[2 * (size_t)i + 1] = jmax;
         }
     }
 }

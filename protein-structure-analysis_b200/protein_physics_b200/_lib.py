@@ -62,7 +62,8 @@ class AlmaNL(C.Structure):
                 ("half_ptr", _p), ("half_len", _p), ("half_cols", _p), ("half_base", _p),
                 ("ref_xyz", _p), ("need", _p),
                 ("sfull_ptr", _p), ("sfull_len", _p), ("sfull_cols", _p), ("sfull_base", _p),
-                ("shalf_ptr", _p), ("shalf_len", _p), ("shalf_cols", _p), ("shalf_base", _p)]
+                ("shalf_ptr", _p), ("shalf_len", _p), ("shalf_cols", _p), ("shalf_base", _p),
+                ("full_span", _p)]
 
 
 class AlmaMCConfig(C.Structure):

@@ -78,6 +78,7 @@ class DeviceBatch:
         self._build_topology([s[4] if s[4] is not None else _empty_topo(n) for s, n in zip(systems, sizes)])
         self.params = _lib.reference_params()
         self.nl_ready = False
+        self.keep_span = True  # AlmaNL.full_span: lets the move kernels skip rows that move whole
         self._alloc_nl(None)
         self.scratch = torch.zeros(max(1, self.L.alma_move_scratch_bytes(max(self.natoms, 1))),
                                    dtype=torch.uint8, device=_DEV)
@@ -243,6 +244,7 @@ class DeviceBatch:
         self.sfull_cols = torch.zeros(int(sfb[-1]) + 1, dtype=torch.int32, device=_DEV)
         self.shalf_cols = torch.zeros(int(shb[-1]) + 1, dtype=torch.int32, device=_DEV)
         self.ref_xyz = torch.zeros((n, 4), dtype=torch.float64, device=_DEV)
+        self.full_span = torch.zeros((n, 2), dtype=torch.int32, device=_DEV)
         self.need = torch.zeros((self.nsys, 4), dtype=torch.int64, device=_DEV)
         self.max_cells = int(max(4096, 8 * self.natoms + 4096 * self.nsys))
         self.nl_ws = torch.zeros(self.L.alma_nl_workspace_bytes(self.nsys, self.natoms, self.max_cells),
@@ -259,12 +261,21 @@ class DeviceBatch:
         nl.half_ptr, nl.half_len, nl.half_cols, nl.half_base = (_ptr(self.half_ptr), _ptr(self.half_len),
                                                                 _ptr(self.half_cols), _ptr(self.half_base))
         nl.ref_xyz, nl.need = _ptr(self.ref_xyz), _ptr(self.need)
+        nl.full_span = _ptr(self.full_span) if self.keep_span else None
         nl.sfull_ptr, nl.sfull_len, nl.sfull_cols, nl.sfull_base = (_ptr(self.sfull_ptr), _ptr(self.sfull_len),
                                                                     _ptr(self.sfull_cols), _ptr(self.sfull_base))
         nl.shalf_ptr, nl.shalf_len, nl.shalf_cols, nl.shalf_base = (_ptr(self.shalf_ptr), _ptr(self.shalf_len),
                                                                     _ptr(self.shalf_cols), _ptr(self.shalf_base))
         self._nl_s = nl
         return nl
+
+    def set_row_spans(self, on):
+        """Keep (default) or drop the per-row index spans (AlmaNL.full_span);
+        the move kernels give the same bits either way, only slower without.
+        The lists are rebuilt on the next use."""
+        self.keep_span = bool(on)
+        self._nl_s = None
+        self.nl_ready = False
 
     def _sp(self):
         return C.c_void_p((self.stream or torch.cuda.current_stream()).cuda_stream)

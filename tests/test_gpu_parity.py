@@ -210,3 +210,52 @@ def test_engine_reuses_batch_across_calls(golden):
     P3 = [Particle(*x, 0.5 * q, r, e) for x, q, r, e in zip(golden["xyz"], golden["q"], golden["r"], golden["eps"])]
     assert eng.calculate_potential(P3, T) == PhysicsEngine().calculate_potential(P3, T)
     assert len(eng._batches) == 2
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_row_spans_and_edge_skip(golden, precision):
+    """AlmaNL.full_span holds each full row's smallest and largest atom
+    index, and a move gives the same ΔE terms whether or not the kernels may
+    skip the rows that move whole (no cross pair, no SASA mark in them):
+    every torsion, crankshaft and concerted-pair move of the system."""
+    T = golden.topology()
+    on = _batch(golden, precision)
+    off = _batch(golden, precision)
+    off.set_row_spans(False)
+    for b in (on, off):
+        b.build_nl()
+        b.born_radii()
+    rp, cols, _ = on.nl_host(0, half=False)
+    span = on.full_span[:golden.n].cpu().numpy()
+    for i in range(golden.n):
+        row = cols[rp[i]:rp[i + 1]]
+        assert tuple(span[i]) == ((int(row.min()), int(row.max())) if row.size else (2 ** 31 - 1, -1))
+    moves = [(0, k) for k in range(len(T.rot_bonds))]
+    moves += [(1, k) for k in range(len(T.concerted_pairs))]
+    moves += [(2, k) for k in range(len(T.concerted_sidechain_pairs))]
+    rng = np.random.default_rng(5)
+    tol = 1e-11 if precision == "fp64" else 1e-9
+    inner = 0
+    for kind, a in moves:
+        d = rng.uniform(-0.3, 0.3, 2)
+        e1, t1 = on.move_dE([kind], [a], [d])
+        e0, t0 = off.move_dE([kind], [a], [d])
+        t1, t0 = t1[0].cpu().numpy(), t0[0].cpu().numpy()
+        np.testing.assert_allclose(t1, t0, rtol=tol, atol=1e-9, err_msg=str((kind, a)))
+        assert float(e1[0]) == pytest.approx(float(e0[0]), rel=tol, abs=1e-9)
+    # the skip engages: some torsion side holds atoms whose rows stay inside it
+    from protein_physics_b200.topology import flatten
+    F = flatten(T)
+    for k in range(F.nrb):
+        lo, hi = int(F.side_lo[k]), int(F.side_hi[k])
+        inner += int(np.sum((span[lo:hi, 0] >= lo) & (span[lo:hi, 1] < hi)))
+    assert inner > 0
+    # commits of the largest sides (their inner members' Born radii come from
+    # the commit pass): same coordinates, same radii
+    big = np.argsort(-F.side_count)[:4]
+    for kind, a in [(0, int(k)) for k in big] + [(1, 0)] * (len(T.concerted_pairs) > 0):
+        for b in (on, off):
+            b.move_dE([kind], [a], [[0.2, 0.0]], apply=True)
+        assert np.array_equal(on.coords(0), off.coords(0))
+        np.testing.assert_allclose(on.born[:golden.n].cpu().numpy(), off.born[:golden.n].cpu().numpy(),
+                                   rtol=1e-12 if precision == "fp64" else 1e-6)
