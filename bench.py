@@ -140,7 +140,7 @@ def run_ours(args, rank, world, local):
         tuned = tuple(int(v) for v in args.config.split(","))
     else:
         tuned = autotune(batch, temps, seed=777, policy=2, moveset=movesets,
-                         proposals=300 if args.workload == "single" else 30)
+                         proposals=1000 if args.workload == "single" else 30)
     tuned = (tuple(tuned) + (1,))[:3]
     runner = MCRunner(batch, temps, seed=12345 + rank, policy=2, cur_max0=0.12, moveset=movesets,
                       cluster_size=tuned[0], threads=tuned[1], spec_teams=tuned[2])

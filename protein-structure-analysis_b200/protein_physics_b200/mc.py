@@ -79,9 +79,9 @@ class MCRunner:
                     break
         self.cfg.cluster_size = int(cluster_size)
         self.cfg.threads_per_system = int(threads)
-        if spec_teams is None:  # a second team per system when the SMs are there
+        if spec_teams is None:  # up to four speculative teams per system when the SMs are there
             sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
-            spec_teams = 2 if 2 * batch.nsys * int(cluster_size) <= sms else 1
+            spec_teams = next(k for k in (4, 2, 1) if k == 1 or k * batch.nsys * int(cluster_size) <= sms)
         self.cfg.spec_teams = int(spec_teams)
         # device_rebuild: a drifted chain rebuilds its list, radii and energy
         # inside the persistent kernel (one-team launches) instead of
@@ -157,8 +157,10 @@ _TUNED = {}
 
 def autotune(batch, temperatures, seed, policy=0, moveset=None, proposals=200, candidates=None):
     """Picks (cluster_size, threads_per_system, spec_teams) for this batch shape by
-    timing `proposals` proposals per candidate on a scratch copy of the
-    batch state; cached per (systems, atom-count bucket, policy)."""
+    timing `proposals` proposals per candidate, after as many untimed ones
+    (the step scale and the acceptance rate, on which the speculative teams'
+    gain depends, settle first), on a scratch copy of the batch state;
+    cached per (systems, atom-count bucket, policy)."""
     import time
     sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
     key = (batch.nsys, int(np.log2(max(1, batch.natoms // max(1, batch.nsys)))), policy, moveset is not None)
@@ -174,7 +176,7 @@ def autotune(batch, temperatures, seed, policy=0, moveset=None, proposals=200, c
         try:
             R = MCRunner(batch, temperatures, seed, policy=policy, moveset=moveset, cluster_size=cl, threads=nt,
                          spec_teams=k)
-            R.run(max(10, proposals // 10))
+            R.run(max(10, proposals))
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             R.run(proposals)
