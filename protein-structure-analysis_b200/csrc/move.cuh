@@ -300,6 +300,16 @@ __device__ __forceinline__ double4 pos_new(const double *xyz, const double *xyz_
     return group[j] ? ld_xyz(xyz_new, j) : ld_xyz(xyz, j);
 }
 
+// The same, with the three loads issued together (one dependent L2 round
+// trip instead of two; the row scans are latency bound).  xyz_new of an
+// atom that does not move holds a stale value that is not used.
+__device__ __forceinline__ double4 pos_new_eager(const double *xyz, const double *xyz_new, const int8_t *group,
+                                                 int j) {
+    const int8_t g = group[j];
+    const double4 a = ld_xyz(xyz, j), n = ld_xyz(xyz_new, j);
+    return g ? n : a;
+}
+
 __device__ __forceinline__ double dih_angle4(double4 A, double4 B, double4 C, double4 D) {
     const double b1x = A.x - B.x, b1y = A.y - B.y, b1z = A.z - B.z;
     const double b2x = C.x - B.x, b2y = C.y - B.y, b2z = C.z - B.z;
@@ -407,20 +417,22 @@ __device__ __forceinline__ void sasa_row(const MoveCtx &C, int s, int k, bool sh
     const uint32_t *rc = short_rows ? C.nl.shalf_cols : C.nl.half_cols;
     const int64_t beg = short_rows ? C.nl.shalf_ptr[i] : C.nl.half_ptr[i];
     const int64_t end = beg + (short_rows ? C.nl.shalf_len[i] : C.nl.half_len[i]);
+    uint32_t nxt = beg + lane < end ? rc[beg + lane] : 0u;
     for (int64_t e0 = beg; e0 < end; e0 += 32) {
         const int64_t e = e0 + lane;
         double co = 0.0, cn = 0.0;
         bool ho = false, hn = false;
         if (e < end) {
-            const int j = (int)(rc[e] & ALMA_IDX_MASK);
+            const int j = (int)(nxt & ALMA_IDX_MASK);
+            if (e + 32 < end) nxt = rc[e + 32];  // next entry in flight
             const double rsj = b.prm64[4 * (size_t)j + 1] + C.P.probe_r;
             const double dc = rsi + rsj;
+            const double4 pjn = pos_new_eager(b.xyz, w.xyz_new, w.group, j);
             const double4 pjo = ld_xyz(b.xyz, j);
             if (!cached) {
                 const double ro = sqrt(d2_of(pio, pjo));
                 if (ro < dc) { ho = true; co = cs * ((dc - ro) / (2.0 * rsi)); }
             }
-            const double4 pjn = w.group[j] ? ld_xyz(w.xyz_new, j) : pjo;
             const double rn = sqrt(d2_of(pin, pjn));
             if (rn < dc) { hn = true; cn = cs * ((dc - rn) / (2.0 * rsi)); }
         }
@@ -554,11 +566,16 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
         prm_of<R>(b.prm, b.prm64, m, qm, rm, em);
         double sum = 0.0;
         const int64_t hb = C.nl.half_ptr[m], he = hb + C.nl.half_len[m];
-        for (int64_t e = hb + 32 * seg + lane; e < he; e += 32 * wph) {
-            const int j = (int)(C.nl.half_cols[e] & ALMA_IDX_MASK);
+        // the next entry of the row is fetched while this one is evaluated
+        const int64_t stp = 32 * wph;
+        int64_t e = hb + 32 * seg + lane;
+        uint32_t nxt = e < he ? C.nl.half_cols[e] : 0u;
+        for (; e < he; e += stp) {
+            const int j = (int)(nxt & ALMA_IDX_MASK);
+            if (e + stp < he) nxt = C.nl.half_cols[e + stp];
             R qj, rj, ej;
             prm_of<R>(b.prm, b.prm64, j, qj, rj, ej);
-            const double r2d = d2_of(pm, pos_new(b.xyz, w.xyz_new, w.group, j));
+            const double r2d = d2_of(pm, pos_new_eager(b.xyz, w.xyz_new, w.group, j));
             const R r2 = (R)r2d;
             sum += (double)hct_term<R>(m_sqrt(r2), r2, rm, rj);
         }
@@ -575,11 +592,20 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
         const uint32_t *rc = short_rows ? C.nl.sfull_cols : C.nl.full_cols;
         const int64_t fb = short_rows ? C.nl.sfull_ptr[m] : C.nl.full_ptr[m];
         const int64_t fe = fb + (short_rows ? C.nl.sfull_len[m] : C.nl.full_len[m]);
-        for (int64_t e = fb + 32 * seg + lane; e < fe; e += 32 * wph) {
-            const int j = (int)(rc[e] & ALMA_IDX_MASK);
-            if (w.body[j] == bm) continue;
-            const double dc = rsm + b.prm64[4 * (size_t)j + 1] + C.P.probe_r, dc2 = dc * dc;
-            const double4 pjo = ld_xyz(b.xyz, j), pjn = w.group[j] ? ld_xyz(w.xyz_new, j) : pjo;
+        const int64_t stp = 32 * wph;
+        int64_t e = fb + 32 * seg + lane;
+        uint32_t nxt = e < fe ? rc[e] : 0u;
+        for (; e < fe; e += stp) {
+            const int j = (int)(nxt & ALMA_IDX_MASK);
+            if (e + stp < fe) nxt = rc[e + stp];
+            // every load of the entry at once; most partners share m's body
+            const int bj = w.body[j];
+            const int8_t gj = w.group[j];
+            const double rj = b.prm64[4 * (size_t)j + 1];
+            const double4 pjo = ld_xyz(b.xyz, j), pjx = ld_xyz(w.xyz_new, j);
+            if (bj == bm) continue;
+            const double dc = rsm + rj + C.P.probe_r, dc2 = dc * dc;
+            const double4 pjn = gj ? pjx : pjo;
             if (d2_of(pmo, pjo) < dc2 || d2_of(pm, pjn) < dc2) {
                 const int a = j < m ? j : m;
                 if (atomicExch(&w.mark[a], 1) == 0) w.affected[a0 + atomicAdd(&q[3], 1)] = a;
@@ -657,17 +683,20 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
         };
         const unsigned below = (1u << lane) - 1u;
         int nq = 0;
-        for (int64_t e0 = fb + 32 * seg; e0 < fe; e0 += 32 * wpc) {
+        const int64_t stp = 32 * wpc;
+        uint32_t nxt = fb + 32 * seg + lane < fe ? C.nl.full_cols[fb + 32 * seg + lane] : 0u;
+        for (int64_t e0 = fb + 32 * seg; e0 < fe; e0 += stp) {
             const int64_t e = e0 + lane;
             bool pass = false;
             CrossCand c;
             if (e < fe) {
-                const uint32_t ent = C.nl.full_cols[e];
+                const uint32_t ent = nxt;
+                if (e + stp < fe) nxt = C.nl.full_cols[e + stp];  // next entry in flight
                 if (!(ent & ALMA_EXCL_BIT)) {
                     c.j = (int)(ent & ALMA_IDX_MASK);
                     c.gj = w.group[c.j];
+                    const double4 pjo = ld_xyz(b.xyz, c.j);  // with the group load
                     if (!(c.gj == gm || (c.gj != 0 && c.j < m))) {
-                        const double4 pjo = ld_xyz(b.xyz, c.j);
                         const double4 pjn = c.gj ? ld_xyz(w.xyz_new, c.j) : pjo;
                         c.r2o = d2_of(pmo, pjo);
                         c.r2n = d2_of(pmn, pjn);
