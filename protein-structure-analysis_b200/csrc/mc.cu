@@ -565,7 +565,7 @@ mc_spec_kernel(MoveCtx C, MCConfigDev cfg, AlmaChainState *__restrict__ states, 
     if (threadIdx.x == 0) {
         S = states[s];
         if (T.rank == 0) {
-            for (int k = 0; k < 8; ++k) Cq.w.queue[8 * s + k] = 0;  // this team's queues, both parities
+            for (int k = 0; k < QUEUE_PER_SYS; ++k) Cq.w.queue[QUEUE_PER_SYS * s + k] = 0;  // this team's queues, both parities
             Cq.w.drift[2 * s] = Cq.w.drift[2 * s + 1] = 0;
         }
     }

@@ -27,7 +27,7 @@ static size_t carve_scratch(MoveScratch *w, char *base, int32_t natoms) {
     t.cross_part = (double *)take(sizeof(double) * MAX_WPR * (size_t)natoms);
     t.ctr = (unsigned long long *)take(sizeof(unsigned long long) * 4 * (size_t)(natoms + 1));
     t.phase = (unsigned long long *)take(sizeof(unsigned long long) * 4 * (size_t)(natoms + 1));
-    t.queue = (int *)take(sizeof(int) * 8 * (size_t)(natoms + 1));
+    t.queue = (int *)take(sizeof(int) * QUEUE_PER_SYS * (size_t)(natoms + 1));
     t.drift = (int *)take(sizeof(int) * 2 * (size_t)(natoms + 1));
     if (w) *w = t;
     return off;
@@ -46,7 +46,7 @@ __global__ void __launch_bounds__(MOVE_THREADS) move_dE_kernel(MoveCtx C, const 
     const int s = blockIdx.x;
     const int k = kind[s];
     if (threadIdx.x == 0) {
-        for (int q = 0; q < 8; ++q) C.w.queue[8 * s + q] = 0;  // fresh queues: parity 0
+        for (int q = 0; q < QUEUE_PER_SYS; ++q) C.w.queue[QUEUE_PER_SYS * s + q] = 0;  // fresh queues: parity 0
         C.w.drift[2 * s] = C.w.drift[2 * s + 1] = 0;
         if (k >= 0) decode_move(M, C.t, C.b.xyz, s, k, a[s], delta + 2 * (size_t)s);
         else M.degenerate = 1;

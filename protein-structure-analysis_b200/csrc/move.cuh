@@ -139,12 +139,24 @@ struct MoveScratch {
                               // hct terms, SASA neighbour visits, moved atoms
     unsigned long long *phase;  // [4*nsys] cumulative SM cycles of rank 0 in
                                 // the four phases of move_eval (+ finish)
-    int *queue;               // [8*nsys] per proposal parity: [1] = edge
-                              // atoms, [2] = a trial atom is beyond half the
-                              // skin, [3] = affected atoms (slot 0 reserved),
-                              // two parities
+    int *queue;               // [QUEUE_PER_SYS*nsys] per proposal parity
+                              // (QUEUE_PER_PARITY ints): [0] = next P3 task,
+                              // [1] = edge atoms, [2] = a trial atom is
+                              // beyond half the skin, [3] = affected atoms,
+                              // [4] = next P2 task (others reserved)
     int *drift;               // [2*nsys] drift flags, two proposals
 };
+
+constexpr int QUEUE_PER_PARITY = 8;
+constexpr int QUEUE_PER_SYS = 2 * QUEUE_PER_PARITY;
+
+// Next task index of a dynamically scheduled phase for the calling warp
+// (lane 0 draws from the team's counter; every lane gets it).
+__device__ __forceinline__ int64_t draw_task(int *counter, int lane) {
+    int v = 0;
+    if (lane == 0) v = atomicAdd(counter, 1);
+    return __shfl_sync(0xffffffffu, v, 0);
+}
 
 // A j-side: sorted explicit atoms side_idx[eb, ee) plus the range [lo, hi).
 struct SideRef {
@@ -481,7 +493,7 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
     const int lane = threadIdx.x & 31;
     const int a0 = b.atom_off[s], a1 = b.atom_off[s + 1];
     const int64_t nm = n_members(M);
-    int *q = w.queue + 8 * s + 4 * parity;  // this proposal's queue counters
+    int *q = w.queue + QUEUE_PER_SYS * s + QUEUE_PER_PARITY * parity;  // this proposal's queue counters
     const bool timer = tid == 0;
     long long t0 = timer ? clock64() : 0;
     rows_ok = rows_ok && C.nl.sfull_cols != nullptr && C.nl.ref_xyz != nullptr;
@@ -536,8 +548,8 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
     // proposal, whose last readers finished before the barrier above: clear
     // them for the next proposal.
     if (tid == 0) {
-        int *qn = w.queue + 8 * s + 4 * (parity ^ 1);
-        qn[0] = qn[1] = qn[2] = qn[3] = 0;
+        int *qn = w.queue + QUEUE_PER_SYS * s + QUEUE_PER_PARITY * (parity ^ 1);
+        for (int k = 0; k < QUEUE_PER_PARITY; ++k) qn[k] = 0;
         w.drift[2 * s + (parity ^ 1)] = 0;
     }
 
@@ -546,14 +558,21 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
     // in i's half row and r < R*_i + R*_j + 2 probe; a pair whose distance
     // changes (rigid bodies differ) and is within reach before or after the
     // move changes the SASA of its lower atom only: mark that atom.
-    // Two task sets over the team's warps — Born segments of the edge rows,
-    // then mark segments — so the two kinds of work land on different warps.
+    // Two task sets — Born segments of the edge rows, then mark segments —
+    // drawn by the team's warps from a shared counter as each finishes a
+    // task (the row lengths vary, so a fixed striding leaves warps idle while
+    // others work through long rows); rows are cut into up to MAX_WPR
+    // segments so that there are about two tasks per warp.
     // Only edge members take part in cross pairs, so only their new radii
     // enter ΔE; the other members' radii are computed by the commit.
     const int wid = T.gwarp(), nw = T.gwarps();
-    const int wph = rows_wpr(2 * ne, nw);
+    (void)wid;
+    int wph = 1;
+    while (wph < MAX_WPR && 2 * ne * wph < 2 * (int64_t)nw) wph *= 2;
     const int64_t nhct = ne * wph;
-    for (int64_t it = wid; it < 2 * nhct; it += nw) {
+    int nx = 0;
+    for (int64_t it = draw_task(q + 4, lane); it < 2 * nhct; it = __shfl_sync(0xffffffffu, nx, 0)) {
+        if (lane == 0) nx = atomicAdd(q + 4, 1);  // the next draw, in flight during this task
         const bool marking = it >= nhct;
         const int64_t i2 = marking ? it - nhct : it;
         const int64_t k = i2 / wph;
@@ -625,18 +644,22 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
     // One task space: cross-pair segments first (every warp gets one when
     // the rows allow), then the affected atoms' SASA, which wraps round onto
     // the warps: a short SASA row after a half row beats a full row.
+    // Drawn from the team's counter like P2: the SASA rows first (each an
+    // ordered recurrence, the longest tasks), then the cross-pair segments.
     const int naff = q[3];
-    const int wpc = rows_wpr(ne, nw);
+    int wpc = 1;
+    while (wpc < MAX_WPR && ne * wpc + naff < 2 * (int64_t)nw) wpc *= 2;
     const int64_t ncross = ne * wpc;
     const double pi4 = 4.0 * 3.14159265358979323846, pi2 = 2.0 * 3.14159265358979323846;
     unsigned long long nsasa = 0;
-    for (int64_t it = wid; it < ncross + naff; it += nw) {
-        if (it >= ncross) {
-            sasa_row(C, s, (int)(it - ncross), short_rows, pi2, pi4, lane, nsasa);
+    for (int64_t it = draw_task(q + 0, lane); it < ncross + naff; it = __shfl_sync(0xffffffffu, nx, 0)) {
+        if (lane == 0) nx = atomicAdd(q + 0, 1);  // the next draw, in flight during this task
+        if (it < naff) {
+            sasa_row(C, s, (int)it, short_rows, pi2, pi4, lane, nsasa);
             continue;
         }
-        const int64_t k = it / wpc;
-        const int seg = (int)(it % wpc);
+        const int64_t k = (it - naff) / wpc;
+        const int seg = (int)((it - naff) % wpc);
         int g;
         const int m = by_edge ? w.edge[a0 + k] : member(M, t.side_idx, k, g);
         const int gm = by_edge ? (int)w.group[m] : g + 1;
@@ -834,7 +857,7 @@ __device__ inline void move_finish(const MoveCtx &C, const MoveDesc &M, int s, i
         w.group[m] = 0;
         w.body[m] = 0;
     }
-    const int naff = w.queue[8 * s + 4 * parity + 3];
+    const int naff = w.queue[QUEUE_PER_SYS * s + QUEUE_PER_PARITY * parity + 3];
     for (int k = tid; k < naff; k += nthr) {
         const int i = w.affected[a0 + k];
         if (accept && C.b.sasa) C.b.sasa[i] = w.dE_atom[2 * (size_t)i];  // the committed atoms' SASA terms
