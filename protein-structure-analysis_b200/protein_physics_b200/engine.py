@@ -29,19 +29,46 @@ class Particle:
                 f"{self.epsilon!r}, {self.is_water!r})")
 
 
+_FLAT_FIELDS = ("excl_ptr", "excl_cols", "rb_i", "rb_j", "rb_kind", "rb_scale", "side_ptr", "side_idx", "side_lo",
+                "side_hi", "dih_abcd", "term_off", "term_v2", "term_n", "term_gamma", "ss", "crank", "conc_sc")
+
+
+def _flat_digest(flat):
+    """Digest of a FlatTopology's arrays; kept on the object when its arrays
+    are read-only (the cached result of flatten, which never changes)."""
+    d = getattr(flat, "_digest", None)
+    if d is not None:
+        return d
+    import hashlib
+    h = hashlib.blake2b(digest_size=16)
+    for name in _FLAT_FIELDS:
+        h.update(np.ascontiguousarray(getattr(flat, name)).tobytes())
+    d = h.digest()
+    if not flat.excl_cols.flags.writeable:
+        flat._digest = d
+    return d
+
+
 def particle_arrays(particles):
     """(xyz [n,3], charge, radius, epsilon) from any objects with the
     Particle attributes (this module's or the reference's)."""
-    n = len(particles)
-    a = np.empty((n, 6), dtype=np.float64)
-    for k, p in enumerate(particles):
-        a[k] = (p.x, p.y, p.z, p.charge, p.radius, p.epsilon)
-    return a[:, :3].copy(), a[:, 3].copy(), a[:, 4].copy(), a[:, 5].copy()
+    ps = particles if isinstance(particles, list) else list(particles)
+    xyz = np.array([[p.x for p in ps], [p.y for p in ps], [p.z for p in ps]], dtype=np.float64).T.copy()
+    return (xyz.reshape(-1, 3), np.array([p.charge for p in ps], dtype=np.float64),
+            np.array([p.radius for p in ps], dtype=np.float64), np.array([p.epsilon for p in ps], dtype=np.float64))
 
 
 def particles_from(xyz, template):
-    """New Particle list with coordinates xyz and the other fields of template."""
-    return [Particle(x[0], x[1], x[2], p.charge, p.radius, p.epsilon, p.is_water) for x, p in zip(xyz, template)]
+    """New Particle list with coordinates xyz and the other fields of template
+    (built field by field: the values are floats already)."""
+    out = []
+    new = Particle.__new__
+    for (x, y, z), p in zip(np.asarray(xyz, dtype=np.float64).tolist(), template):
+        o = new(Particle)
+        o.x, o.y, o.z = x, y, z
+        o.charge, o.radius, o.epsilon, o.is_water = float(p.charge), float(p.radius), float(p.epsilon), bool(p.is_water)
+        out.append(o)
+    return out
 
 
 class PhysicsEngine:
@@ -70,10 +97,7 @@ class PhysicsEngine:
         for a in (q, r, e):
             h.update(np.ascontiguousarray(a, np.float64).tobytes())
         if flat is not None:
-            for name in ("excl_ptr", "excl_cols", "rb_i", "rb_j", "rb_kind", "rb_scale", "side_ptr", "side_idx",
-                         "side_lo", "side_hi", "dih_abcd", "term_off", "term_v2", "term_n", "term_gamma", "ss",
-                         "crank", "conc_sc"):
-                h.update(np.ascontiguousarray(getattr(flat, name)).tobytes())
+            h.update(_flat_digest(flat))
         key = (int(copies), len(q), flat is not None, h.hexdigest())
         b = self._batches.pop(key, None)
         X = np.tile(np.asarray(xyz, np.float64).reshape(-1, 3), (int(copies), 1))
