@@ -23,11 +23,16 @@ from .device import DeviceBatch
 
 class _Energy(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, xyz, batch):
+    def forward(ctx, xyz, batch, graph):
         n = batch.natoms
         if xyz.shape != (n, 3) or xyz.dtype != torch.float64 or not xyz.is_cuda:
             raise ValueError(f"xyz must be a CUDA float64 tensor of shape ({n}, 3)")
         batch.xyz[:n, :3].copy_(xyz.detach())
+        if graph:  # list, radii, energy and gradient as one replayed CUDA graph
+            terms, grad = batch.evaluate(graph=True)
+            if ctx.needs_input_grad[0]:
+                ctx.save_for_backward(grad[:n, :3].clone(), batch.atom_sys)
+            return terms[:, 4].clone()
         batch.nl_ready = False
         batch.invalidate_sasa()
         batch.build_nl()
@@ -40,24 +45,26 @@ class _Energy(torch.autograd.Function):
     @staticmethod
     def backward(ctx, gE):
         g, sys_of = ctx.saved_tensors
-        return g * gE[sys_of].unsqueeze(1), None
+        return g * gE[sys_of].unsqueeze(1), None, None
 
 
-def energy(xyz, batch: DeviceBatch):
-    """Per-system total energies [nsys] of coordinates xyz [natoms, 3]."""
-    return _Energy.apply(xyz, batch)
+def energy(xyz, batch: DeviceBatch, graph=False):
+    """Per-system total energies [nsys] of coordinates xyz [natoms, 3]
+    (graph=True: evaluated by replaying one captured CUDA graph)."""
+    return _Energy.apply(xyz, batch, bool(graph))
 
 
 class EnergyModel(torch.nn.Module):
     """A fixed set of systems (parameters and topology) whose energy is a
     differentiable function of the coordinates."""
 
-    def __init__(self, systems, precision="mixed"):
+    def __init__(self, systems, precision="mixed", graph=False):
         super().__init__()
         self.batch = DeviceBatch(systems, precision=precision)
+        self.graph = bool(graph)
 
     def coords(self):
         return self.batch.xyz[:self.batch.natoms, :3].clone()
 
     def forward(self, xyz):
-        return energy(xyz, self.batch)
+        return energy(xyz, self.batch, self.graph)

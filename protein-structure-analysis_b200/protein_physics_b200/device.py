@@ -371,6 +371,65 @@ class DeviceBatch:
                                       _ptr(g), self._sp()), "alma_forces")
         return g
 
+    def evaluate(self, graph=False):
+        """One full evaluation at the coordinates in self.xyz: fresh neighbor
+        list, Born radii, energy terms and dE/dx.  Returns (terms [nsys, 5],
+        grad [natoms, 4]); with graph=True both are buffers owned by the batch,
+        rewritten by every call.
+
+        graph=True replays one captured CUDA graph of the whole sequence (the
+        first call captures it): write new coordinates into self.xyz between
+        calls.  The list's overflow check runs after each replay (one status
+        read); on overflow the lists are regrown, the graph recaptured and the
+        evaluation repeated."""
+        if not graph:
+            self.nl_ready = False
+            self.invalidate_sasa()
+            self.build_nl()
+            terms = self.energy_terms(recompute_born=True)
+            return terms, self.forces()
+        for _ in range(3):
+            g = getattr(self, "_eval_graph", None)
+            if g is None:
+                g = self._capture_eval()
+            g.replay()
+            st = int(self.status.item())
+            if not st & (_lib.ST_NL_OVERFLOW | _lib.ST_CELL_OVERFLOW):
+                self.nl_ready = True
+                self.sasa_valid = True
+                return self._g_terms, self._g_grad
+            # regrow the lists eagerly; the graph holds the old buffers
+            self._eval_graph = None
+            self.status.zero_()
+            self.nl_ready = False
+            self.build_nl()
+        raise RuntimeError("evaluate: neighbor-list overflow persists")
+
+    def _capture_eval(self):
+        self._g_terms = torch.zeros((self.nsys, 5), dtype=torch.float64, device=_DEV)
+        self._g_grad = torch.zeros((max(self.natoms, 1), 4), dtype=torch.float64, device=_DEV)
+
+        def body():
+            self.nl_ready = False
+            self.build_nl(check=False)
+            self.energy_terms(recompute_born=True, out=self._g_terms)
+            self.forces(out=self._g_grad)
+
+        keep, self.stream = self.stream, None  # captured on torch's current stream
+        try:
+            side = torch.cuda.Stream()
+            side.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(side):  # warm-up: every workspace allocated outside the capture
+                body()
+            torch.cuda.current_stream().wait_stream(side)
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                body()
+        finally:
+            self.stream = keep
+        self._eval_graph = g
+        return g
+
     # ---- one proposal per system ---------------------------------------------
     def move_dE(self, kind, a, delta, apply=False):
         """kind/a: int per system; delta: [nsys, 2] radians.  Returns
