@@ -643,8 +643,8 @@ def run_profile_case(args):
     at the first drift flag); --config CL,NT[,K] picks the launch shape.
     "forces": the same chain, one energy evaluation and one alma_forces
     call (4 gradient kernels).  "energy": the first 48 chains of the batched
-    workload (about 0.26M atoms, rows well above L2), one neighbor-list
-    build and one full energy evaluation."""
+    workload (about 0.24M atoms, rows well above L2), one neighbor-list
+    build, one full energy evaluation and one gradient (alma_forces)."""
     import torch
     from protein_physics_b200.device import DeviceBatch
     from protein_physics_b200.mc import MCRunner
@@ -653,6 +653,7 @@ def run_profile_case(args):
         batch = DeviceBatch(systems, precision="mixed")
         batch.build_nl()
         terms = batch.energy_terms()
+        batch.forces()
         torch.cuda.synchronize()
         print(json.dumps({"profile_case": "energy", "systems": len(chains), "atoms": batch.natoms,
                           "half_entries": int(batch.half_len.sum()), "full_entries": int(batch.full_len.sum()),

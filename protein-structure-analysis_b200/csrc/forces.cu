@@ -109,8 +109,10 @@ __device__ __forceinline__ R hct_deriv(R r, R r2, R ri, R rj) {
     return -Lp / (L * L) + (R)1 / (U * U) + dT;
 }
 
+// Warp per atom, 256 threads, 4 blocks per SM (64 registers): the row
+// gathers are latency bound and the occupancy pays.
 template <typename R>
-__global__ void grad_pair_kernel(DevParams P, int natoms, const int32_t *__restrict__ atom_off, int nsys,
+__global__ void __launch_bounds__(256, 4) grad_pair_kernel(DevParams P, int natoms, const int32_t *__restrict__ atom_off, int nsys,
                                  const uint8_t *__restrict__ mask, const double *__restrict__ xyz,
                                  const float *__restrict__ prm, const double *__restrict__ prm64,
                                  const double *__restrict__ born, const int64_t *__restrict__ full_ptr,
@@ -159,7 +161,7 @@ __global__ void grad_pair_kernel(DevParams P, int natoms, const int32_t *__restr
 }
 
 // SASA adjoints over the ordered half row (FP64, as the forward).
-__global__ void grad_sasa_kernel(DevParams P, int natoms, const int32_t *__restrict__ atom_off, int nsys,
+__global__ void __launch_bounds__(256, 4) grad_sasa_kernel(DevParams P, int natoms, const int32_t *__restrict__ atom_off, int nsys,
                                  const uint8_t *__restrict__ mask, const double *__restrict__ xyz,
                                  const double *__restrict__ prm64, const int64_t *__restrict__ half_ptr,
                                  const int32_t *__restrict__ half_len, const uint32_t *__restrict__ half_cols,

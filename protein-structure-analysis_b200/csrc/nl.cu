@@ -240,9 +240,10 @@ __global__ void nl_rowscan_kernel(const int32_t *__restrict__ atom_off, const ui
     }
 }
 
-// Warp per atom.  PASS 0 counts, PASS 1 writes.
+// Warp per atom.  PASS 0 counts, PASS 1 writes.  256 threads, 4 blocks per
+// SM (at most 64 registers: the scan is latency bound, occupancy pays).
 template <int PASS>
-__global__ void nl_rows_kernel(const int32_t *__restrict__ atom_off, int nsys, int natoms, const uint8_t *__restrict__ mask,
+__global__ void __launch_bounds__(256, 4) nl_rows_kernel(const int32_t *__restrict__ atom_off, int nsys, int natoms, const uint8_t *__restrict__ mask,
                                const double *__restrict__ xyz, double rcut2, const SysGrid *__restrict__ grid,
                                const int32_t *__restrict__ ok, const int32_t *__restrict__ cell_of,
                                const int64_t *__restrict__ cell_start, const int32_t *__restrict__ cell_atoms,
