@@ -135,15 +135,35 @@ class MCRunner:
         target = int(self.state()["step"].max()) + int(nsteps) if nsteps > 0 else 0
         return self.run_to(target)
 
+    def _read_state(self):
+        """Chain states and the batch status word in one device-to-host
+        transfer (pinned buffer, one synchronisation)."""
+        n = self.states.numel()
+        if getattr(self, "_host", None) is None:
+            self._host = torch.empty(n + 4, dtype=torch.uint8, pin_memory=True)
+        s = self.b.stream or torch.cuda.current_stream()
+        with torch.cuda.stream(s):
+            self._host[:n].copy_(self.states, non_blocking=True)
+            self._host[n:].copy_(self.b.status.view(torch.uint8), non_blocking=True)
+        s.synchronize()
+        h = self._host.numpy()
+        return h[:n].view(_lib.STATE_DTYPE).copy(), int(h[n:].view(np.int32)[0])
+
+    def _need_mask(self):
+        """Device-side system mask of the chains whose need_rebuild is set."""
+        off = _lib.STATE_DTYPE.fields["need_rebuild"][1]
+        rows = self.states.view(self.b.nsys, _lib.STATE_DTYPE.itemsize)[:, off:off + 4]
+        return rows.view(torch.int32).reshape(self.b.nsys).ne(0).to(torch.uint8)
+
     def run_to(self, step_limit):
         while True:
             self.launch(step_limit)
-            st = self.state()
-            if self.cfg.spec_teams > 1 and int(self.b.status.item()) & _lib.ST_SPEC_ABORT:
+            st, status = self._read_state()
+            if self.cfg.spec_teams > 1 and status & _lib.ST_SPEC_ABORT:
                 raise RuntimeError("alma_mc_run: a speculative round timed out (teams not co-resident)")
             need = st["need_rebuild"] != 0
             if need.any():
-                mask = torch.from_numpy(need.astype(np.uint8)).to("cuda")
+                mask = self._need_mask()
                 self.b.build_nl(sys_mask=mask)
                 self.reset_energy(sys_mask=mask)
                 self.rebuilds += int(need.sum())
