@@ -105,15 +105,7 @@ struct CrossCand {
 };
 constexpr int CROSS_BUF = 64;  // per warp: < 32 waiting + one batch of 32
 constexpr int MAX_ROT = 2;
-constexpr int MAX_WPR = 4;  // warps per moved-atom row, at most
-
-// Warps per moved-atom row: as many as keep every warp of the team busy,
-// a power of two <= MAX_WPR.
-__device__ __forceinline__ int rows_wpr(int64_t nrows, int nwarps) {
-    int w = 1;
-    while (w < MAX_WPR && (int64_t)(2 * w) * nrows <= (int64_t)nwarps) w *= 2;
-    return w;
-}
+constexpr int MAX_WPR = 4;  // segments (tasks) per moved-atom row, at most
 
 // Global scratch for the move kernels; every array is all-zero between
 // proposals (each proposal clears what it set).
@@ -472,10 +464,12 @@ __device__ __forceinline__ void sasa_row(const MoveCtx &C, int s, int k, bool sh
 // counters, CTA partials and drift flag).  Leaves group/body/xyz_new/
 // born_new set for the members; move_finish commits or discards.
 //
-// Rows are strided over the team's warps.  Team barriers: (1) after the
-// proposal copy, (2) after the member Born radii and SASA marks (the marking
-// pass also builds the affected-atom list), (3) after the cross-pair and
-// SASA slots, (4) the CTA-partials exchange of team_sum.
+// Members are strided over the team's threads (P1, P4); row tasks (P2, P3)
+// are drawn from per-team counters.  Team barriers: (1) after the moved
+// coordinates and the edge list, (2) after the edge members' Born radii and
+// the SASA marks (the marking pass also builds the affected-atom list),
+// (3) after the cross-pair and SASA slots, (4) the CTA-partials exchange of
+// team_sum.
 //
 // rows_ok: every committed atom of system s is within half the skin of its
 // position at the last list build.  Then, when every trial position is too,
@@ -565,8 +559,7 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
     // segments so that there are about two tasks per warp.
     // Only edge members take part in cross pairs, so only their new radii
     // enter ΔE; the other members' radii are computed by the commit.
-    const int wid = T.gwarp(), nw = T.gwarps();
-    (void)wid;
+    const int nw = T.gwarps();
     int wph = 1;
     while (wph < MAX_WPR && 2 * ne * wph < 2 * (int64_t)nw) wph *= 2;
     const int64_t nhct = ne * wph;
