@@ -131,8 +131,10 @@ typedef struct {
  * skin of its build position no other pair can come within SASA reach, so
  * the move kernels walk these instead.  need[4*s + k] receives the entry
  * counts (k: full, half, short full, short half) of system s at its last
- * build; when a count exceeds its region, the rows of that system are not
- * written and ALMA_ST_NL_OVERFLOW is raised. */
+ * build; when a count exceeds its region, the rows of that system are
+ * incomplete and ALMA_ST_NL_OVERFLOW is raised (regrow the regions from
+ * need[] and build again).  Rows lie in their system's region in no
+ * particular order: read them through ptr/len. */
 typedef struct {
     int64_t *full_ptr;        /* [natoms] */
     int32_t *full_len;        /* [natoms] */

@@ -15,9 +15,10 @@
 //   bin    : atom -> cell, cell histogram
 //   scan   : cell starts
 //   scatter: atoms into cells, then a per-cell rank sort (ascending index)
-//   count  : warp per atom — row lengths
-//   rowscan: one CTA per system — row pointers inside the system's region
-//   fill   : warp per atom — rows, ballot-compacted in scan order
+//   rows   : warp per atom — one scan stages the row in shared memory,
+//            takes space from the system's cursors, writes the four rows
+//            ballot-compacted in scan order
+//   final  : per system — entry counts, overflow flag
 // Every stage honours an optional per-system mask, so systems can be
 // rebuilt independently (the MC driver rebuilds only chains that drifted).
 #include <cstdio>
@@ -35,14 +36,12 @@ struct NLWork {
     int32_t *cell_fill;   // [max_cells]
     int64_t *cell_start;  // [max_cells+1]
     int32_t *cell_atoms;  // [natoms]
-    int32_t *full_cnt;    // [natoms]
-    int32_t *half_cnt;    // [natoms]
-    int32_t *sfull_cnt;   // [natoms]
-    int32_t *shalf_cnt;   // [natoms]
+    int32_t *sort_spill;  // [natoms] rank-sort space for oversized cells
     int64_t *tile_sums;   // scan scratch
     int64_t *total_cells; // [1]
     int32_t *ok;          // [1] 1 when the grid fit
     int32_t *sys_ok;      // [nsys] 1 when the system's rows fit its region
+    int64_t *cursor;      // [4*nsys] next free entry of each row kind in the system's region
 };
 
 static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -63,14 +62,12 @@ static size_t carve(NLWork *w, char *base, int32_t nsys, int32_t natoms, int64_t
     t.cell_fill = (int32_t *)take(sizeof(int32_t) * (size_t)max_cells);
     t.cell_start = (int64_t *)take(sizeof(int64_t) * (size_t)(max_cells + 1));
     t.cell_atoms = (int32_t *)take(sizeof(int32_t) * (size_t)natoms);
-    t.full_cnt = (int32_t *)take(sizeof(int32_t) * (size_t)natoms);
-    t.half_cnt = (int32_t *)take(sizeof(int32_t) * (size_t)natoms);
-    t.sfull_cnt = (int32_t *)take(sizeof(int32_t) * (size_t)natoms);
-    t.shalf_cnt = (int32_t *)take(sizeof(int32_t) * (size_t)natoms);
+    t.sort_spill = (int32_t *)take(sizeof(int32_t) * (size_t)natoms);
     t.tile_sums = (int64_t *)take(sizeof(int64_t) * (size_t)ntiles);
     t.total_cells = (int64_t *)take(sizeof(int64_t));
     t.ok = (int32_t *)take(sizeof(int32_t));
     t.sys_ok = (int32_t *)take(sizeof(int32_t) * (size_t)(nsys > 0 ? nsys : 1));
+    t.cursor = (int64_t *)take(sizeof(int64_t) * 4 * (size_t)(nsys > 0 ? nsys : 1));
     if (w) *w = t;
     return off;
 }
@@ -196,79 +193,171 @@ __global__ void nl_cellsort_kernel(const int64_t *__restrict__ total_cells, cons
     }
 }
 
-// One CTA per system: row pointers inside the system's region, overflow
-// check, for the four row kinds (full, half, short full, short half; the
-// short ones only when the list carries them).
-__global__ void nl_rowscan_kernel(const int32_t *__restrict__ atom_off, const uint8_t *__restrict__ mask,
-                                  const int32_t *__restrict__ full_cnt, const int32_t *__restrict__ half_cnt,
-                                  const int32_t *__restrict__ sfull_cnt, const int32_t *__restrict__ shalf_cnt,
-                                  AlmaNL nl, int32_t *__restrict__ sys_ok, uint32_t *__restrict__ status) {
-    __shared__ int64_t sm[33];
-    const int s = blockIdx.x;
-    if (mask && !mask[s]) return;
-    const int a0 = atom_off[s], a1 = atom_off[s + 1];
-    const int nkind = nl.sfull_cols ? 4 : 2;
-    int fits = 1;
-    for (int kind = 0; kind < nkind; ++kind) {
-        const int32_t *cnt = kind == 0 ? full_cnt : kind == 1 ? half_cnt : kind == 2 ? sfull_cnt : shalf_cnt;
-        int64_t *ptr = kind == 0 ? nl.full_ptr : kind == 1 ? nl.half_ptr : kind == 2 ? nl.sfull_ptr : nl.shalf_ptr;
-        int32_t *len = kind == 0 ? nl.full_len : kind == 1 ? nl.half_len : kind == 2 ? nl.sfull_len : nl.shalf_len;
-        const int64_t *basev = kind == 0 ? nl.full_base : kind == 1 ? nl.half_base : kind == 2 ? nl.sfull_base
-                                                                                                : nl.shalf_base;
-        const int64_t base = basev[s], cap = basev[s + 1] - base;
-        int64_t carry = 0;
-        for (int b0 = a0; b0 < a1; b0 += blockDim.x) {
-            const int i = b0 + threadIdx.x;
-            const int64_t v = i < a1 ? cnt[i] : 0;
-            int64_t ex;
-            const int64_t tot = block_exclusive_scan(v, ex, sm);
-            if (i < a1) {
-                ptr[i] = base + carry + ex;
-                len[i] = (int32_t)v;
-            }
-            carry += tot;
-        }
-        if (threadIdx.x == 0) {
-            nl.need[4 * s + kind] = carry;
-            if (carry > cap) fits = 0;
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        sys_ok[s] = fits;
-        if (!fits) set_status(status, ALMA_ST_NL_OVERFLOW);
-    }
-}
+// Entries of one row staged per warp in shared memory by the one-pass
+// build (48 KB per 8-warp block); a longer row is scanned a second time.
+constexpr int NL_STAGE = 1536;
+constexpr uint32_t NL_SHORT_BIT = 0x40000000u;  // staging only: the pair is within SASA reach
 
-// Warp per atom.  PASS 0 counts, PASS 1 writes.  256 threads, 4 blocks per
-// SM (at most 64 registers: the scan is latency bound, occupancy pays).
-template <int PASS>
-__global__ void __launch_bounds__(256, 4) nl_rows_kernel(const int32_t *__restrict__ atom_off, int nsys, int natoms, const uint8_t *__restrict__ mask,
-                               const double *__restrict__ xyz, double rcut2, const SysGrid *__restrict__ grid,
-                               const int32_t *__restrict__ ok, const int32_t *__restrict__ cell_of,
-                               const int64_t *__restrict__ cell_start, const int32_t *__restrict__ cell_atoms,
-                               int32_t *__restrict__ full_cnt, int32_t *__restrict__ half_cnt,
-                               int32_t *__restrict__ sfull_cnt, int32_t *__restrict__ shalf_cnt,
-                               const double *__restrict__ prm64, double reach_pad,
-                               const int64_t *__restrict__ excl_ptr, const int32_t *__restrict__ excl_cols,
-                               AlmaNL nl, const int32_t *__restrict__ sys_ok) {
+// One-pass build, warp per atom: the 27-cell scan stages the row (exclusion
+// flag in bit 31, SASA-reach flag in bit 30) in shared memory in scan
+// order, lane 0 then takes space for the four rows from the system's
+// cursors (one atomic per row kind), and the warp writes the full row, the
+// half row (j > i) and the short rows from the staged entries — the same
+// rows, in the same order, as counting and filling in two scans.  Rows sit
+// in their system's region in the order the warps reach the cursors; every
+// reader goes through ptr/len.  A row that would overflow its region is not
+// written (nl_finalize_kernel raises the overflow); a row longer than the
+// stage is written by a second scan straight into its space.
+__global__ void __launch_bounds__(256, 4)
+nl_rows_onepass_kernel(const int32_t *__restrict__ atom_off, int nsys, int natoms, const uint8_t *__restrict__ mask,
+                       const double *__restrict__ xyz, double rcut2, const SysGrid *__restrict__ grid,
+                       const int32_t *__restrict__ ok, const int32_t *__restrict__ cell_of,
+                       const int64_t *__restrict__ cell_start, const int32_t *__restrict__ cell_atoms,
+                       const double *__restrict__ prm64, double reach_pad, const int64_t *__restrict__ excl_ptr,
+                       const int32_t *__restrict__ excl_cols, AlmaNL nl, int64_t *__restrict__ cursor) {
+    extern __shared__ uint32_t nl_stage_smem[];
     const int warps_per_block = blockDim.x >> 5;
     const int i = blockIdx.x * warps_per_block + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     if (i >= natoms || !*ok) return;
     const int s = sys_of_atom(atom_off, nsys, i);
     if (mask && !mask[s]) return;
-    if (PASS == 1 && !sys_ok[s]) return;
     const SysGrid g = grid[s];
-    int nfull, nhalf, nsfull, nshalf;
-    nl_row_atom<PASS>(i, lane, g, xyz, rcut2, cell_of, cell_start, cell_atoms, prm64, reach_pad, excl_ptr, excl_cols,
-                      nl, nfull, nhalf, nsfull, nshalf);
-    if (PASS == 0 && lane == 0) {
-        full_cnt[i] = nfull;
-        half_cnt[i] = nhalf;
-        sfull_cnt[i] = nsfull;
-        shalf_cnt[i] = nshalf;
+    uint32_t *stage = nl_stage_smem + (threadIdx.x >> 5) * NL_STAGE;
+    const bool shorts = nl.sfull_cols != nullptr;
+    const int c = cell_of[i];
+    const int cx = c % g.nx, cy = (c / g.nx) % g.ny, cz = c / (g.nx * g.ny);
+    const double4 pi = ld_xyz(xyz, i);
+    const double ri_pad = shorts ? prm64[4 * (size_t)i + 1] + reach_pad : 0.0;
+    int nfull = 0, nhalf = 0, nsfull = 0, nshalf = 0;
+    int jmin = 0x7fffffff, jmax = -1;
+    const unsigned lt = (1u << lane) - 1u;
+    for (int dz = -1; dz <= 1; ++dz) {
+        const int cz2 = cz + dz;
+        if (cz2 < 0 || cz2 >= g.nz) continue;
+        for (int dy = -1; dy <= 1; ++dy) {
+            const int cy2 = cy + dy;
+            if (cy2 < 0 || cy2 >= g.ny) continue;
+            for (int dx = -1; dx <= 1; ++dx) {
+                const int cx2 = cx + dx;
+                if (cx2 < 0 || cx2 >= g.nx) continue;
+                const int64_t cell = g.cell_off + cx2 + (int64_t)g.nx * (cy2 + (int64_t)g.ny * cz2);
+                const int64_t beg = cell_start[cell], end = cell_start[cell + 1];
+                for (int64_t k0 = beg; k0 < end; k0 += 32) {
+                    const int64_t k = k0 + lane;
+                    int j = -1;
+                    bool in = false, sh = false;
+                    if (k < end) {
+                        j = cell_atoms[k];
+                        const double r2 = d2_of(pi, ld_xyz(xyz, j));
+                        in = (j != i) && r2 < rcut2;
+                        if (in && shorts) {
+                            const double reach = ri_pad + prm64[4 * (size_t)j + 1];
+                            sh = r2 < reach * reach;
+                        }
+                    }
+                    const unsigned mf = __ballot_sync(0xffffffffu, in);
+                    if (in) {
+                        jmin = min(jmin, j);
+                        jmax = max(jmax, j);
+                        const int at = nfull + __popc(mf & lt);
+                        if (at < NL_STAGE)
+                            stage[at] = (uint32_t)j | (excluded(excl_ptr, excl_cols, i, j) ? ALMA_EXCL_BIT : 0u) |
+                                        (sh ? NL_SHORT_BIT : 0u);
+                    }
+                    nfull += __popc(mf);
+                    nhalf += __popc(__ballot_sync(0xffffffffu, in && j > i));
+                    nsfull += __popc(__ballot_sync(0xffffffffu, sh));
+                    nshalf += __popc(__ballot_sync(0xffffffffu, sh && j > i));
+                }
+            }
+        }
     }
+    // space in the system's regions (relative offsets; -1: does not fit)
+    int64_t off[4] = {0, 0, 0, 0};
+    const int nkind = shorts ? 4 : 2;
+    if (lane == 0) {
+        const int n[4] = {nfull, nhalf, nsfull, nshalf};
+        const int64_t *basev[4] = {nl.full_base, nl.half_base, nl.sfull_base, nl.shalf_base};
+        for (int kd = 0; kd < nkind; ++kd) {
+            const int64_t o = atomicAdd(reinterpret_cast<unsigned long long *>(cursor + 4 * s + kd),
+                                        (unsigned long long)n[kd]);
+            off[kd] = o + n[kd] <= basev[kd][s + 1] - basev[kd][s] ? basev[kd][s] + o : -1;
+        }
+    }
+    for (int kd = 0; kd < 4; ++kd) off[kd] = __shfl_sync(0xffffffffu, off[kd], 0);
+    bool fits = true;
+    for (int kd = 0; kd < nkind; ++kd) fits = fits && off[kd] >= 0;
+    if (!fits) return;  // the system overflows: nl_finalize_kernel flags it
+    if (lane == 0) {
+        nl.full_ptr[i] = off[0];
+        nl.full_len[i] = nfull;
+        nl.half_ptr[i] = off[1];
+        nl.half_len[i] = nhalf;
+        if (shorts) {
+            nl.sfull_ptr[i] = off[2];
+            nl.sfull_len[i] = nsfull;
+            nl.shalf_ptr[i] = off[3];
+            nl.shalf_len[i] = nshalf;
+        }
+    }
+    if (nfull > NL_STAGE) {  // too long to stage: scan again, writing at the pointers just set
+        __syncwarp();
+        int a, bb, cc, dd;
+        nl_row_atom<1>(i, lane, g, xyz, rcut2, cell_of, cell_start, cell_atoms, prm64, reach_pad, excl_ptr, excl_cols,
+                       nl, a, bb, cc, dd);
+        return;
+    }
+    __syncwarp();
+    if (lane == 0) *reinterpret_cast<double4 *>(nl.ref_xyz + 4 * (size_t)i) = pi;
+    int wf = 0, wh = 0, wsf = 0, wsh = 0;
+    for (int t0 = 0; t0 < nfull; t0 += 32) {
+        const int t = t0 + lane;
+        const bool v = t < nfull;
+        const uint32_t st = v ? stage[t] : 0u;
+        const uint32_t e = st & ~NL_SHORT_BIT;
+        const int j = (int)(st & ALMA_IDX_MASK & ~NL_SHORT_BIT);
+        const bool hf = v && j > i, sh = v && (st & NL_SHORT_BIT);
+        const unsigned mh = __ballot_sync(0xffffffffu, hf);
+        const unsigned msf = __ballot_sync(0xffffffffu, sh);
+        const unsigned msh = __ballot_sync(0xffffffffu, sh && hf);
+        if (v) nl.full_cols[off[0] + t] = e;
+        if (hf) nl.half_cols[off[1] + wh + __popc(mh & lt)] = e;
+        if (sh) {
+            nl.sfull_cols[off[2] + wsf + __popc(msf & lt)] = e;
+            if (hf) nl.shalf_cols[off[3] + wsh + __popc(msh & lt)] = e;
+        }
+        wf += 32;
+        wh += __popc(mh);
+        wsf += __popc(msf);
+        wsh += __popc(msh);
+    }
+    (void)wf;
+    if (nl.full_span != nullptr) {
+        jmin = __reduce_min_sync(0xffffffffu, jmin);
+        jmax = __reduce_max_sync(0xffffffffu, jmax);
+        if (lane == 0) {
+            nl.full_span[2 * (size_t)i] = jmin;
+            nl.full_span[2 * (size_t)i + 1] = jmax;
+        }
+    }
+}
+
+// Per system after the one-pass build: entry counts into need[], overflow
+// into the status word.
+__global__ void nl_finalize_kernel(int nsys, const uint8_t *__restrict__ mask, const int32_t *__restrict__ ok,
+                                   const int64_t *__restrict__ cursor, AlmaNL nl, uint32_t *__restrict__ status) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nsys || !*ok || (mask && !mask[s])) return;
+    const int nkind = nl.sfull_cols ? 4 : 2;
+    const int64_t *basev[4] = {nl.full_base, nl.half_base, nl.sfull_base, nl.shalf_base};
+    bool fits = true;
+    for (int kd = 0; kd < nkind; ++kd) {
+        const int64_t n = cursor[4 * s + kd];
+        nl.need[4 * s + kd] = n;
+        fits = fits && n <= basev[kd][s + 1] - basev[kd][s];
+    }
+    if (!fits) set_status(status, ALMA_ST_NL_OVERFLOW);
 }
 
 }  // namespace alma
@@ -283,6 +372,8 @@ extern "C" int alma_nl_build(const AlmaBatch *b, const AlmaTopo *t, AlmaNL *nl, 
                              const uint8_t *sys_mask, void *workspace, int64_t max_cells, void *stream) {
     if (!b || !nl || !workspace || b->nsys <= 0 || b->natoms < 0 || max_cells <= 0)
         return alma_set_error(ALMA_EINVAL, "alma_nl_build: bad arguments");
+    if (b->natoms >= (1 << 30))  // the build stages a flag in bit 30 of each entry
+        return alma_set_error(ALMA_EINVAL, "alma_nl_build: at most 2^30 - 1 atoms");
     if (!nl->full_ptr || !nl->full_len || !nl->half_ptr || !nl->half_len || !nl->full_base || !nl->half_base ||
         !nl->ref_xyz || !nl->need || !b->xyz || !b->atom_off)
         return alma_set_error(ALMA_EINVAL, "alma_nl_build: null buffer");
@@ -314,20 +405,16 @@ extern "C" int alma_nl_build(const AlmaBatch *b, const AlmaTopo *t, AlmaNL *nl, 
     exclusive_scan<int32_t>(w.cell_count, w.cell_start, max_cells, w.tile_sums, st);
     nl_scatter_kernel<<<nb, tb, 0, st>>>(b->atom_off, nsys, natoms, sys_mask, w.grid, w.ok, w.cell_of, w.cell_start,
                                          w.cell_fill, w.cell_atoms);
-    // Oversized cells (> SORT_SMEM atoms) sort through half_cnt as spill
-    // space: it holds natoms ints and is only written later by the count pass.
-    nl_cellsort_kernel<<<1184, 256, 0, st>>>(w.total_cells, w.ok, w.cell_start, w.cell_atoms, w.half_cnt);
+    // oversized cells (> SORT_SMEM atoms) sort through the spill space
+    nl_cellsort_kernel<<<1184, 256, 0, st>>>(w.total_cells, w.ok, w.cell_start, w.cell_atoms, w.sort_spill);
     const int wpb = 8, rb = (natoms + wpb - 1) / wpb;
     const int64_t *ep = t ? t->excl_ptr : nullptr;
     const int32_t *ec = t ? t->excl_cols : nullptr;
-    nl_rows_kernel<0><<<rb, wpb * 32, 0, st>>>(b->atom_off, nsys, natoms, sys_mask, b->xyz, rcut2, w.grid, w.ok,
-                                               w.cell_of, w.cell_start, w.cell_atoms, w.full_cnt, w.half_cnt,
-                                               w.sfull_cnt, w.shalf_cnt, b->prm64, reach_pad, ep, ec, *nl, w.sys_ok);
-    nl_rowscan_kernel<<<nsys, 1024, 0, st>>>(b->atom_off, sys_mask, w.full_cnt, w.half_cnt, w.sfull_cnt, w.shalf_cnt,
-                                             *nl, w.sys_ok, b->status);
-    nl_rows_kernel<1><<<rb, wpb * 32, 0, st>>>(b->atom_off, nsys, natoms, sys_mask, b->xyz, rcut2, w.grid, w.ok,
-                                               w.cell_of, w.cell_start, w.cell_atoms, w.full_cnt, w.half_cnt,
-                                               w.sfull_cnt, w.shalf_cnt, b->prm64, reach_pad, ep, ec, *nl, w.sys_ok);
-    ALMA_LAUNCH_CHECK_N("alma_nl_build", 11);
+    ALMA_CUDA_TRY(cudaMemsetAsync(w.cursor, 0, sizeof(int64_t) * 4 * (size_t)nsys, st));
+    nl_rows_onepass_kernel<<<rb, wpb * 32, sizeof(uint32_t) * NL_STAGE * wpb, st>>>(
+        b->atom_off, nsys, natoms, sys_mask, b->xyz, rcut2, w.grid, w.ok, w.cell_of, w.cell_start, w.cell_atoms,
+        b->prm64, reach_pad, ep, ec, *nl, w.cursor);
+    nl_finalize_kernel<<<(nsys + 255) / 256, 256, 0, st>>>(nsys, sys_mask, w.ok, w.cursor, *nl, b->status);
+    ALMA_LAUNCH_CHECK_N("alma_nl_build", 10);
     return ALMA_OK;
 }
