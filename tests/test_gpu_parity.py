@@ -259,3 +259,40 @@ def test_row_spans_and_edge_skip(golden, precision):
         assert np.array_equal(on.coords(0), off.coords(0))
         np.testing.assert_allclose(on.born[:golden.n].cpu().numpy(), off.born[:golden.n].cpu().numpy(),
                                    rtol=1e-12 if precision == "fp64" else 1e-6)
+
+
+def test_nl_overflow_regrows_and_rebuilds(oracle):
+    """Regions far too small for the rows: the build raises the overflow,
+    the batch regrows its regions from need[] and builds again; the rows are
+    then bit-exact, and a masked rebuild of one system after its atoms move
+    leaves the other system's rows as they were."""
+    from conftest import Golden
+    from protein_physics_b200.device import DeviceBatch
+    from protein_physics_b200.topology import flatten
+
+    class Tight(DeviceBatch):
+        NL_FULL_PER_ATOM = 1
+        NL_HALF_PER_ATOM = 1
+        NL_SHORT_PER_ATOM = 2
+
+    gs = [Golden("insulin"), Golden("xq8")]
+    systems = [(g["xyz"], g["q"], g["r"], g["eps"], flatten(g.topology())) for g in gs]
+    b = Tight(systems)
+    assert int(b.full_base[-1]) < 2 * b.natoms + 1000  # the initial regions cannot hold the rows
+    b.build_nl()
+    for s, g in enumerate(gs):
+        rp, cols, _ = b.nl_host(s, half=True)
+        ptr, ocols = oracle.nl_build(g["xyz"])
+        assert np.array_equal(rp, ptr) and np.array_equal(cols, ocols), s
+    before = b.nl_host(1, half=False)
+    x = b.xyz.clone()
+    a0, a1 = int(b.atom_off_h[0]), int(b.atom_off_h[1])
+    x[a0:a1, :3] += 0.3
+    b.xyz.copy_(x)
+    mask = torch.tensor([1, 0], dtype=torch.uint8, device="cuda")
+    b.build_nl(sys_mask=mask)
+    after = b.nl_host(1, half=False)
+    assert all(np.array_equal(u, v) for u, v in zip(before, after))
+    rp, cols, _ = b.nl_host(0, half=True)
+    ptr, ocols = oracle.nl_build(b.coords(0))
+    assert np.array_equal(rp, ptr) and np.array_equal(cols, ocols)
