@@ -94,6 +94,19 @@ def _coil_chain(n_res, seed):
     return synth.coil_chain(n_res, seed)
 
 
+def host_threads():
+    """Host threads available to this process (what the reference's OpenMP
+    engine uses: OMP_NUM_THREADS when set, else the CPUs this process may run
+    on)."""
+    env = os.environ.get("OMP_NUM_THREADS", "")
+    if env.strip().isdigit() and int(env) > 0:
+        return int(env)
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
 def make_workload(kind, rank, n_chains=256):
     from protein_physics_b200 import synth
     from protein_physics_b200.dist import rank_seed
@@ -200,22 +213,31 @@ def run_ours(args, rank, world, local):
     eng = PhysicsEngine(precision="mixed", seed=99 + rank)
     e2e_val = None
     h2d = d2h = 0
+    e2e_single = None
     if args.workload == "single":
         ch = chains[0]
-        P = [Particle(*x, q, r, e) for x, q, r, e in zip(ch.xyz, ch.charge, ch.radius, ch.epsilon)]
-        eng.generate_ensemble(P, topos[0], 1, 50)  # warm
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
+        P0 = [Particle(*x, q, r, e) for x, q, r, e in zip(ch.xyz, ch.charge, ch.radius, ch.epsilon)]
         n_e2e = max(1, args.steps // 2)
-        for _ in range(n_e2e):
-            P = eng.generate_ensemble(P, topos[0], 1, per_step)[0]
-        e1.record(stream)
-        torch.cuda.synchronize()
-        e2e_ms = e0.elapsed_time(e1)
-        e2e_val = n_e2e * per_step / (e2e_ms * 1e-3) * world
-        h2d = ch.n * 8 * 6
-        d2h = ch.n * 8 * 3
+
+        def e2e_rate(ncand):
+            P = P0
+            eng.generate_ensemble(P, topos[0], ncand, 50)  # warm
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(n_e2e):
+                P = eng.generate_ensemble(P, topos[0], ncand, per_step)[0]
+            e1.record(stream)
+            torch.cuda.synchronize()
+            return n_e2e * ncand * per_step / (e0.elapsed_time(e1) * 1e-3) * world
+
+        # the call the reference arm times: as many candidates as the host has
+        # threads (its OpenMP spans candidates), per_step proposals each
+        ncand = host_threads()
+        e2e_val = e2e_rate(ncand)
+        e2e_single = e2e_rate(1)
+        h2d = ncand * ch.n * 8 * 3 + ch.n * 8 * 3  # coordinates per candidate + charge, radius, epsilon
+        d2h = ncand * ch.n * 8 * 3
     clocks = sampler.summary()
     de_err = de_error_vs_fp64(systems[0], movesets[0], runner.state()["cur_max"][0]) if rank == 0 else None
     out = None
@@ -245,7 +267,11 @@ def run_ours(args, rank, world, local):
             "tuned": {"cluster_size": tuned[0], "threads_per_system": tuned[1], "spec_teams": tuned[2]},
             "wall_s": t_wall,
             "e2e": {"value": e2e_val, "unit": "proposals/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "api": "PhysicsEngine.generate_ensemble(host particles, topology, 1, 1000)",
+                    "candidates": host_threads() if args.workload == "single" else None,
+                    "single_candidate": e2e_single,
+                    "api": "PhysicsEngine.generate_ensemble(host particles, topology, n_candidates, 1000), "
+                           "n_candidates = the host threads, the call the reference arm times; single_candidate: "
+                           "the same with 1 candidate",
                     "workload": "the reference's own move policy (25 % crankshaft, every rotatable bond), as the "
                                 "reference arm runs it: heavier moves and more list rebuilds than the timed value"},
             "roofline": {"bound": "fp32", "kernel": ("mc_spec_kernel<float,%d,%d> x %d teams" % (tuned[1], tuned[0], tuned[2])
