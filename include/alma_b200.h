@@ -351,7 +351,7 @@ int alma_move_dE(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *nl, const 
  *
  * Same arguments and results as alma_move_dE, minus `scratch`.  The
  * scratch is a static area built into the library of
- * ALMA_NOALLOC_SCRATCH_BYTES (4 MiB), which every GPU that loads the
+ * ALMA_NOALLOC_SCRATCH_BYTES (5 MiB), which every GPU that loads the
  * library holds until the process exits; batches up to
  * ALMA_NOALLOC_MAX_ATOMS atoms fit, larger ones are rejected with
  * ALMA_EINVAL and a message.  No call allocates or frees device memory.
@@ -361,7 +361,7 @@ int alma_move_dE(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *nl, const 
  * the GPU (two streams, two host threads) race and corrupt each other's
  * results — serialise them.  Each call clears the part it uses before
  * running. */
-#define ALMA_NOALLOC_SCRATCH_BYTES (4u << 20)
+#define ALMA_NOALLOC_SCRATCH_BYTES (5u << 20)
 #define ALMA_NOALLOC_MAX_ATOMS 16384
 size_t alma_move_noalloc_capacity_bytes(void);
 int alma_move_dE_noalloc(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *nl, const AlmaParams *p,

@@ -72,6 +72,17 @@ def test_workspace_sizes_are_monotone():
     assert L.alma_move_scratch_bytes(100) < L.alma_move_scratch_bytes(1000)
 
 
+def test_noalloc_area_holds_its_documented_batch():
+    """The built-in scratch of alma_move_dE_noalloc holds the scratch of a
+    batch of ALMA_NOALLOC_MAX_ATOMS atoms (the header's promise), so a batch
+    within the documented limit is never turned away."""
+    from protein_physics_b200 import _lib
+    L = _lib.lib()
+    hdr = open(os.path.join(ROOT, "include", "alma_b200.h")).read()
+    max_atoms = int(re.search(r"#define ALMA_NOALLOC_MAX_ATOMS (\d+)", hdr).group(1))
+    assert L.alma_move_scratch_bytes(max_atoms) <= L.alma_move_noalloc_capacity_bytes()
+
+
 def test_engine_fails_loudly_without_gpu():
     import torch
     if torch.cuda.is_available():
