@@ -427,6 +427,13 @@ size_t alma_mc_scratch_bytes(int32_t natoms, int32_t nsys, int32_t teams);
 int alma_mc_run(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *nl, const AlmaParams *p, int prec,
                 void *scratch, const AlmaMCConfig *cfg, AlmaChainState *states, int64_t step_limit,
                 void *stream);
+/* Self-test of the speculative rounds' bounded cross-team wait: one CTA
+ * waits at a barrier that nothing else reaches; after its poll limit (about
+ * a second) it raises ALMA_ST_SPEC_ABORT in *status, writes 1 to *aborted
+ * and returns.  round_buf: alma_spec_round_bytes() bytes of device memory. */
+size_t alma_spec_round_bytes(void);
+int alma_spec_wait_selftest(void *round_buf, uint32_t *status, int32_t *aborted, void *stream);
+
 /* state.energy <- terms[5*s+4], need_rebuild <- 0 for masked systems. */
 int alma_mc_after_rebuild(AlmaChainState *states, const double *terms, const uint8_t *sys_mask,
                           int32_t nsys, void *stream);

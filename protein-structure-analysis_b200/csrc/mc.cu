@@ -545,6 +545,15 @@ __device__ __forceinline__ int spec_barrier(const Team<CL> &T, SpecRound *Rd, un
     return ab;
 }
 
+// One CTA alone at a barrier of two: its wait runs out (the timeout path of
+// spec_barrier, exercised without a second team that never arrives).
+__global__ void spec_wait_selftest_kernel(SpecRound *Rd, uint32_t *status, int32_t *aborted) {
+    __shared__ int abort_sh;
+    const Team<1> T;
+    const int ab = spec_barrier<1>(T, Rd, 2u, &abort_sh, status);
+    if (threadIdx.x == 0) *aborted = ab;
+}
+
 template <typename R, int NT, int CL>
 __global__ void __launch_bounds__(NT, 512 / NT)
 mc_spec_kernel(MoveCtx C, MCConfigDev cfg, AlmaChainState *__restrict__ states, int64_t step_limit, int teams,
@@ -739,6 +748,17 @@ static RebuildWS carve_rebuild(void *base, int32_t natoms, int32_t nsys) {
     RebuildWS t = {};
     if (base) rebuild_bytes(natoms, nsys, &t, base);
     return t;
+}
+
+extern "C" size_t alma_spec_round_bytes(void) { return sizeof(SpecRound); }
+
+extern "C" int alma_spec_wait_selftest(void *round_buf, uint32_t *status, int32_t *aborted, void *stream) {
+    if (!round_buf || !status || !aborted) return alma_set_error(ALMA_EINVAL, "alma_spec_wait_selftest: null buffer");
+    cudaStream_t st = (cudaStream_t)stream;
+    ALMA_CUDA_TRY(cudaMemsetAsync(round_buf, 0, sizeof(SpecRound), st));
+    spec_wait_selftest_kernel<<<1, 64, 0, st>>>((SpecRound *)round_buf, status, aborted);
+    ALMA_LAUNCH_CHECK("alma_spec_wait_selftest");
+    return ALMA_OK;
 }
 
 extern "C" size_t alma_mc_rebuild_bytes(int32_t natoms, int32_t nsys) {

@@ -136,6 +136,9 @@ def lib():
     L.alma_mc_scratch_bytes.argtypes = [_i32, _i32, _i32]
     L.alma_mc_rebuild_bytes.restype = C.c_size_t
     L.alma_mc_rebuild_bytes.argtypes = [_i32, _i32]
+    L.alma_spec_round_bytes.restype = C.c_size_t
+    L.alma_spec_round_bytes.argtypes = []
+    L.alma_spec_wait_selftest.argtypes = [_p, _p, _p, _p]
     L.alma_topo_sides.argtypes = [_i32, _p, _p, _i32, _p, _p, _p, _i64]
     L.alma_topo_sides_compact.argtypes = [_i32, _p, _p, _i32, _p, _p, _p, _p, _p, _p, _i64]
     L.alma_nl_build.argtypes = [_p, _p, _p, _p, _p, _p, _i64, _p]

@@ -182,3 +182,24 @@ def test_device_rebuild_batched_equals_host_rebuild():
         assert st1["n_accepted"][s] == st2["n_accepted"][s]
         assert np.array_equal(b1.coords(s), b2.coords(s))
         assert st1["energy"][s] == pytest.approx(st2["energy"][s], rel=1e-11)
+
+
+def test_spec_wait_runs_out_and_reports():
+    """The speculative rounds' cross-team wait is bounded: a team alone at a
+    barrier gives up after its poll limit, raises ALMA_ST_SPEC_ABORT and
+    returns; the context stays usable."""
+    import time
+    from protein_physics_b200 import _lib
+    L = _lib.lib()
+    buf = torch.zeros(L.alma_spec_round_bytes(), dtype=torch.uint8, device="cuda")
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    aborted = torch.zeros(1, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    t0 = time.perf_counter()
+    _lib.check(L.alma_spec_wait_selftest(buf.data_ptr(), status.data_ptr(), aborted.data_ptr(), stream),
+               "alma_spec_wait_selftest")
+    torch.cuda.synchronize()
+    assert int(aborted.item()) == 1
+    assert int(status.item()) & _lib.ST_SPEC_ABORT
+    assert time.perf_counter() - t0 < 30.0
+    assert float(torch.ones(4, device="cuda").sum()) == 4.0  # the context still works
