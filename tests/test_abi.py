@@ -90,3 +90,16 @@ def test_engine_fails_loudly_without_gpu():
     from protein_physics_b200 import Particle, PhysicsEngine
     with pytest.raises(RuntimeError):
         PhysicsEngine().calculate_potential([Particle(0, 0, 0, 1.0), Particle(3, 0, 0, -1.0)])
+
+
+def test_bench_host_threads_follows_omp_setting(monkeypatch):
+    """bench.py sizes the e2e call like the reference arm: one candidate per
+    host thread, OMP_NUM_THREADS first."""
+    import importlib
+    import sys
+    sys.path.insert(0, ROOT)
+    bench = importlib.import_module("bench")
+    monkeypatch.setenv("OMP_NUM_THREADS", "3")
+    assert bench.host_threads() == 3
+    monkeypatch.delenv("OMP_NUM_THREADS")
+    assert bench.host_threads() >= 1
