@@ -357,6 +357,10 @@ int alma_move_dE(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *nl, const 
  * ALMA_EINVAL and a message.  No call allocates or frees device memory.
  * The first call on each device looks up the area's device address (with
  * that device current); make that first call before any stream capture.
+ * The address is cached per device under the context it was looked up in;
+ * a call under another context (after cudaDeviceReset re-created the
+ * primary context) looks it up again.  A rejected call (bad size, null
+ * buffer) returns before touching the area.
  * All calls on a device share the one area: calls whose kernels overlap on
  * the GPU (two streams, two host threads) race and corrupt each other's
  * results — serialise them.  Each call clears the part it uses before

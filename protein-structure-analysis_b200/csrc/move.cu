@@ -1,4 +1,6 @@
 // Move ΔE entry points: one given proposal per system, one CTA per system.
+#include <cuda.h>
+
 #include <mutex>
 
 #include "move.cuh"
@@ -153,21 +155,53 @@ namespace {
 constexpr int kMaxDevices = 64;
 std::mutex g_scratch_mu;
 void *g_scratch_ptr[kMaxDevices] = {};
+unsigned long long g_scratch_ctx[kMaxDevices] = {};  // context the address was looked up under
+
+typedef CUresult (*CtxGetCurrentFn)(CUcontext *);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long *);
+
+// Unique ID of the calling thread's current context (0 when it cannot be
+// read).  A device reset or a re-created primary context gets a new ID,
+// and with it a new module load: the cached address is then stale.
+unsigned long long current_ctx_id() {
+    static CtxGetCurrentFn get_cur = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        cudaDriverEntryPointQueryResult q;
+        void *f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_cur = (CtxGetCurrentFn)f;
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = (CtxGetIdFn)f;
+    });
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (!get_cur || !get_id || get_cur(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
 }  // namespace
 
 // Device address of g_move_scratch on the current device.  In host code the
-// array's name is only a host-side handle, so the address is looked up once
-// per device (with that device current) and cached.
+// array's name is only a host-side handle, so the address is looked up with
+// the device current, on the first call on that device and again whenever
+// the current context is not the one it was looked up under (after a
+// device reset the module, and the array with it, is loaded anew).
 static int noalloc_scratch(void **out) {
     int dev = 0;
     ALMA_CUDA_TRY(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices) return alma_set_error(ALMA_EINVAL, "alma_move_dE_noalloc: device %d", dev);
+    const unsigned long long ctx = current_ctx_id();  // 0 before the runtime has made a context current
     std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (!g_scratch_ptr[dev]) {
+    if (!g_scratch_ptr[dev] || ctx == 0 || ctx != g_scratch_ctx[dev]) {
         void *p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_move_scratch);
         if (e != cudaSuccess) return alma_cuda_error(e, "alma_move_dE_noalloc: cudaGetSymbolAddress");
         g_scratch_ptr[dev] = p;
+        g_scratch_ctx[dev] = current_ctx_id();  // the lookup made the device's context current
     }
     *out = g_scratch_ptr[dev];
     return ALMA_OK;
@@ -186,8 +220,14 @@ extern "C" int alma_move_dE_noalloc(const AlmaBatch *b, const AlmaTopo *t, const
                               "(%d atoms, %zu bytes); use alma_move_dE with caller scratch",
                               b->natoms, ALMA_NOALLOC_MAX_ATOMS, (size_t)ALMA_NOALLOC_SCRATCH_BYTES);
     void *scratch = nullptr;
-    int rc = noalloc_scratch(&scratch);
+    int rc = noalloc_scratch(&scratch);  // looks the address up; touches nothing on the device
     if (rc) return rc;
+    // Validate everything before the clear: a rejected call leaves the shared
+    // area untouched (another call's kernel may still be using it).
+    rc = alma_check_move_args(b, t, nl, p, scratch, "alma_move_dE_noalloc");
+    if (rc) return rc;
+    if (!move_kind || !move_a || !move_delta || !dE || !dterms)
+        return alma_set_error(ALMA_EINVAL, "alma_move_dE_noalloc: null move buffer");
     // The area keeps whatever the previous call left: start from zero.
     ALMA_CUDA_TRY(cudaMemsetAsync(scratch, 0, need, (cudaStream_t)stream));
     return alma_move_dE(b, t, nl, p, prec, scratch, move_kind, move_a, move_delta, apply, dE, dterms, stream);

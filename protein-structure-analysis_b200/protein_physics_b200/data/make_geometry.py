@@ -200,7 +200,9 @@ def _approx_trp():
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("ALMA_REFERENCE", "")
+    if not ref or not os.path.isdir(ref):
+        sys.exit("usage: %s REFERENCE_TREE (or set ALMA_REFERENCE): the reference checkout" % sys.argv[0])
     tables = json.load(open(os.path.join(HERE, "residue_tables.json")))
     bt, rs = tables["bond_templates"], tables["rot_specs"]
     residues = read_pdb(os.path.join(ref, "data", "1XQ8.pdb"))

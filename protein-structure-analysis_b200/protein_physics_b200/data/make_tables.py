@@ -79,7 +79,9 @@ def extract_templates(ref_root):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("ALMA_REFERENCE", "")
+    if not ref or not os.path.isdir(ref):
+        sys.exit("usage: %s REFERENCE_TREE (or set ALMA_REFERENCE): the reference checkout" % sys.argv[0])
     here = os.path.dirname(os.path.abspath(__file__))
     bonds, rots = extract_templates(ref)
     for k, v in bonds.items():

@@ -95,7 +95,7 @@ class MCRunner:
         # of the GPU for the list's 27-cell scan, and on the bench workloads
         # the whole-GPU host rebuild of all flagged chains is faster.
         self.rebuild_ws = None
-        if device_rebuild:
+        if device_rebuild and int(spec_teams) == 1:  # only one-team launches rebuild in the kernel
             self.rebuild_ws = torch.empty(self.L.alma_mc_rebuild_bytes(batch.natoms, batch.nsys), dtype=torch.uint8,
                                           device="cuda")
             self.cfg.rebuild_ws = _ptr(self.rebuild_ws)
@@ -251,8 +251,8 @@ def generate_ensemble(engine, initial_state, topology, n_candidates, steps_per_c
     # instead of idling until the last chain of the launch has drifted too
     # (16 candidates of a 4,962-atom chain: 25.7k -> 32.6k proposals/s).
     cl, k = auto_shape(batch.nsys)
-    runner = MCRunner(batch, temperature, engine._next_seed(), policy=0, cur_max0=max_angle,
-                      device_rebuild=batch.nsys > 1 and k == 1 and cl >= 8)
+    runner = MCRunner(batch, temperature, engine._next_seed(), policy=0, cur_max0=max_angle, cluster_size=cl,
+                      spec_teams=k, device_rebuild=batch.nsys > 1 and k == 1 and cl >= 8)
     runner.run(steps_per_cand)
     X = batch.coords()
     return [particles_from(X[batch.atom_off_h[c]:batch.atom_off_h[c + 1]], initial_state)

@@ -166,7 +166,9 @@ def golden_system(name, sysd, R, pp, rng, n_torsion=24, n_crank=8, full_nl=False
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("ALMA_REFERENCE", "")
+    if not ref or not os.path.isdir(ref):
+        sys.exit("usage: %s REFERENCE_TREE (or set ALMA_REFERENCE): the reference checkout" % sys.argv[0])
     sys.path.insert(0, os.path.join(ref, "python"))
     import amber_params as ap
     from oracle import RefEngine, ref_so_path

@@ -5,7 +5,10 @@ results of alma_move_dE with caller scratch, call after call, although
 every call reuses the one built-in scratch area.
 
 This file sorts last so that a run stopping at the first failure has run
-every other test first; it also passes alone in a fresh process.
+every other test first; it also passes alone in a fresh process.  The
+tests check equality with the caller-scratch entry over calls in a row,
+that a call allocates no device memory, a batch just under the maximum,
+and the rejection of larger ones.
 """
 import ctypes as C
 
@@ -78,3 +81,49 @@ def test_noalloc_rejects_batches_beyond_its_area():
     assert b.natoms > 16384
     with pytest.raises(ValueError, match="exceeds the built-in scratch area"):
         _call(b, "alma_move_dE_noalloc", [0] * reps, [1] * reps, [[0.1, 0.0]] * reps, False)
+
+
+def test_noalloc_allocates_nothing_and_fills_its_area():
+    """Several calls on a batch just under the documented maximum (24
+    copies of insulin, 15,768 atoms): the GPU's free memory does not move
+    across them, and every call equals the caller-scratch entry."""
+    from conftest import Golden
+    from protein_physics_b200 import _lib
+    from protein_physics_b200.device import DeviceBatch, _ptr, _t
+    from protein_physics_b200.topology import flatten
+    L = _lib.lib()
+    L.alma_move_dE_noalloc.argtypes = [C.c_void_p] * 4 + [C.c_int] + [C.c_void_p] * 3 + [C.c_int] + [C.c_void_p] * 3
+    g = Golden("insulin")
+    F = flatten(g.topology())
+    reps = 16384 // g.n
+    b = DeviceBatch([(g["xyz"], g["q"], g["r"], g["eps"], F)] * reps, precision="mixed")
+    assert 16384 - g.n < b.natoms <= 16384
+    b.build_nl()
+    b.born_radii()
+    rng = np.random.default_rng(5)
+    kind = _t(np.zeros(reps, np.int32), torch.int32)
+    a = _t(rng.integers(0, F.nrb, size=reps).astype(np.int32), torch.int32)
+    delta = _t(np.stack([rng.uniform(-0.3, 0.3, reps), np.zeros(reps)], 1), torch.float64)
+    outs = [(torch.zeros(reps, dtype=torch.float64, device="cuda"),
+             torch.zeros((reps, 4), dtype=torch.float64, device="cuda")) for _ in range(2)]
+    common = [C.byref(b.batch_s), C.byref(b.topo_s), C.byref(b.nl_s), C.byref(b.params), b.prec]
+    move = [C.c_void_p(_ptr(kind)), C.c_void_p(_ptr(a)), C.c_void_p(_ptr(delta)), 0]
+
+    def noalloc():
+        dE, dt = outs[0]
+        _lib.check(L.alma_move_dE_noalloc(*common, *move, C.c_void_p(_ptr(dE)), C.c_void_p(_ptr(dt)), b._sp()),
+                   "alma_move_dE_noalloc")
+
+    noalloc()  # first call: the address lookup
+    dE, dt = outs[1]
+    _lib.check(L.alma_move_dE(*common, C.c_void_p(_ptr(b.scratch)), *move, C.c_void_p(_ptr(dE)),
+                              C.c_void_p(_ptr(dt)), b._sp()), "alma_move_dE")
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(4):
+        noalloc()
+        torch.cuda.synchronize()
+        np.testing.assert_allclose(outs[0][0].cpu().numpy(), outs[1][0].cpu().numpy(), rtol=1e-12, atol=1e-9)
+        np.testing.assert_allclose(outs[0][1].cpu().numpy(), outs[1][1].cpu().numpy(), rtol=1e-12, atol=1e-9)
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
