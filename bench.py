@@ -1,33 +1,40 @@
 """Benchmark: Metropolis proposals/s of the B200 engine (and of the reference).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload single|batched|globule|replica]
+                    [--workload batched|single|globule|replica]
 
-Workload "single" (default): one synthetic 300-residue compact chain
-(~4,700 atoms, all-atom with hydrogens, seeded), torsion moves restricted to
-bonds whose j-side holds <= 25 % of the atoms, 300 K (0.5962 kcal/mol), the
-reference's adaptive step (cur_max, lever scale, 2.5x sidechain), neighbor
-list 12 Å + 2 Å skin rebuilt on drift, FP32 pair terms with FP64 ΔE and
-Metropolis test.  One step = 1,000 proposals followed by a full energy
-recomputation (Born radii + energy).
-Workload "batched": 256 chains, 50-600 residues each (per-chain seeds),
-temperatures geometric over 280-400 K, one step = 100 proposals per chain.
-Workload "globule": a 1,000-residue chain: energy+force evals/s, 500
-torsion-space descent steps, then MALA proposals/s.
-Workload "replica": 16 replicas of a 4 x 1,000-residue chain, MALA:torsion
-1:3, replica exchange every 100 sweeps.
+Workload "batched" (default): 256 independent chains, 50-600 residues each
+(seeded, helix/coil phi/psi, ~1.36 M atoms), temperatures geometric over
+280-400 K, the reference generate_ensemble proposal policy (every rotatable
+bond, 25 % crankshaft, adaptive cur_max, 2.5x sidechain steps), FP32 pair
+terms with FP64 ΔE and Metropolis test; one step = 100 proposals per chain.
+The line also carries the single-chain drop-in ("single_chain": the
+300-residue compact chain below, with the reference's plain GPU path and
+CPU engine beside it).
+Workload "single": the 300-residue compact chain (4,962 atoms, Rg ~17 Å,
+workloads/c2_chain_300res.npz), torsion moves of bonds whose j-side holds
+<= 25 % of the atoms, 300 K; one step = 1,000 proposals + a full energy.
+Workload "globule": the 1,000-residue globule (workloads/c4_globule_1000res.npz):
+energy+force evals/s, 500 descent steps, then MALA proposals/s.
+Workload "replica": 16 replicas of the 4 x 1,000-residue chain
+(workloads/c5_multidomain_4x1000res.npz), MALA:torsion 1:3, replica
+exchange every 100 sweeps.
 
 value  = proposals/s of the whole job on the device (CUDA events, inputs
          resident), max over ranks;
-e2e    = the same metric through the public API (PhysicsEngine.
-         generate_ensemble with host particle lists: host->device copy, list
-         build, MC, device->host copy of the final coordinates every step).
-Multi-GPU: every rank runs its own independent chain(s) (replicas; no
+e2e    = the same metric through the public API with host buffers every
+         step (batched: BatchedEnsemble.run, coordinates in and out;
+         single: PhysicsEngine.generate_ensemble with particle lists).
+--impl reference runs the reference engine (oracle/_ref, compiled from the
+reference sources) on the host cores on the same inputs and prints the
+same config; it loads nothing of this package (the chain generator
+synth.py is loaded by path: numpy and scipy only).
+Multi-GPU: every rank runs its own independent chains (replicas; no
 data-path collective); value sums the proposals of all ranks.
 """
 import argparse
+import importlib.util
 import json
-import math
 import os
 import statistics
 import subprocess
@@ -36,16 +43,23 @@ import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
-sys.path.insert(0, os.path.join(ROOT, "protein-structure-analysis_b200"))
-sys.path.insert(0, os.path.join(ROOT, "oracle"))
+PKG = os.path.join(ROOT, "protein-structure-analysis_b200")
+WORKLOADS = os.path.join(ROOT, "workloads")
 
 KB = 0.0019872  # kcal/mol/K
 FP32_PEAK_NOMINAL = 148 * 128 * 2 * 1.965e9  # ops/s: SMs x FP32 lanes x FMA x max SM clock
 OPS_PAIR, OPS_HCT, OPS_SASA = 47.0, 21.0, 11.0  # algorithmic ops per unit (FP32 + MUFU)
+C3_CHAINS, C3_PER_STEP, C2_PER_STEP = 256, 100, 1000
+L2_NOTE = "inputs larger than L2 (lists of 1.36 M atoms) and a 256 MiB L2 flush between GPU steps"
 
 
 def rank_info():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def seed_of(base, rank):
+    """Seed of rank `rank`'s inputs (disjoint streams per rank)."""
+    return int(base) + 1000 * int(rank)
 
 
 class ClockSampler:
@@ -88,12 +102,6 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-def _coil_chain(n_res, seed):
-    sys.path.insert(0, os.path.join(ROOT, "protein-structure-analysis_b200"))
-    from protein_physics_b200 import synth
-    return synth.coil_chain(n_res, seed)
-
-
 def host_threads():
     """Host threads available to this process (what the reference's OpenMP
     engine uses: OMP_NUM_THREADS when set, else the CPUs this process may run
@@ -107,67 +115,108 @@ def host_threads():
         return os.cpu_count() or 1
 
 
-def make_workload(kind, rank, n_chains=256):
-    from protein_physics_b200 import synth
-    from protein_physics_b200.dist import rank_seed
+# ---- inputs (numpy only: both arms build them the same way) --------------------------
+def load_synth():
+    """The chain generator, loaded by path (numpy + scipy; no package import)."""
+    if "alma_synth" in sys.modules:
+        return sys.modules["alma_synth"]
+    spec = importlib.util.spec_from_file_location(
+        "alma_synth", os.path.join(PKG, "protein_physics_b200", "synth.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["alma_synth"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def _chain_dict(ch):
+    return dict(xyz=ch.xyz, charge=ch.charge, radius=ch.radius, epsilon=ch.epsilon, resnames=list(ch.resnames),
+                atomnames=list(ch.atomnames), res_idx=[int(v) for v in ch.res_idx])
+
+
+def _coil_chain_job(n_res, seed):
+    return _chain_dict(load_synth().coil_chain(n_res, seed))
+
+
+def fixture(fname):
+    """A chain written by workloads/make_workloads.py (plain arrays)."""
+    import numpy as np
+    d = np.load(os.path.join(WORKLOADS, fname), allow_pickle=False)
+    return dict(xyz=d["xyz"].astype(np.float64), charge=d["charge"], radius=d["radius"], epsilon=d["epsilon"],
+                resnames=[str(v) for v in d["resnames"]], atomnames=[str(v) for v in d["atomnames"]],
+                res_idx=[int(v) for v in d["res_idx"]])
+
+
+def rg_of(xyz):
+    import numpy as np
+    c = xyz - xyz.mean(0)
+    return float(np.sqrt((c * c).sum(1).mean()))
+
+
+def c3_inputs(rank, n_chains=C3_CHAINS):
+    """The batched workload: chain sizes U{50..600} residues and per-chain
+    seeds, helix/coil chains (synth.coil_chain), temperatures geometric over
+    280-400 K (kcal/mol)."""
+    import multiprocessing as mp
+    import numpy as np
+    rng = np.random.default_rng(seed_of(3, rank))
+    sizes = rng.integers(50, 601, size=C3_CHAINS)[:n_chains]
+    jobs = [(int(n), seed_of(k, rank)) for k, n in enumerate(sizes)]
+    with mp.get_context("spawn").Pool(max(1, min(32, os.cpu_count() or 1))) as pool:  # host Python: all cores
+        chains = pool.starmap(_coil_chain_job, jobs, chunksize=1)
+    temps = list(280.0 * (400.0 / 280.0) ** (np.arange(C3_CHAINS) / (C3_CHAINS - 1)) * KB)[:n_chains]
+    return chains, temps
+
+
+def config_of(kind, chains):
+    """The workload description both arms print (the same dict)."""
+    atoms = int(sum(len(c["xyz"]) for c in chains))
+    if kind == "batched":
+        return {"workload": "batched MC: %d independent chains of 50-600 residues (seeded helix/coil, all-atom), "
+                            "T 280-400 K geometric, the reference generate_ensemble proposal policy, "
+                            "%d proposals per chain per step" % (len(chains), C3_PER_STEP),
+                "chains": len(chains), "atoms": atoms, "proposals_per_chain_per_step": C3_PER_STEP,
+                "moves": "every rotatable bond, 25 % crankshaft, cur_max adapted per 200 proposals",
+                "l2": L2_NOTE, "parallelism": "replicas"}
+    return {"workload": "single chain: 300-residue compact chain (%d atoms, Rg %.1f A), torsion moves of bonds "
+                        "whose j-side holds <= 25 %% of the atoms, 300 K, %d proposals + a full energy per step"
+                        % (atoms, rg_of(chains[0]["xyz"]), C2_PER_STEP),
+            "chains": 1, "atoms": atoms, "rg_A": round(rg_of(chains[0]["xyz"]), 2),
+            "l2": "a 256 MiB L2 flush between steps", "parallelism": "replicas"}
+
+
+# ---- our arm --------------------------------------------------------------------------
+def _our_systems(chains):
+    sys.path.insert(0, PKG)
     from protein_physics_b200.topology import BondTopology, flatten
-    if kind == "single":
-        chains = [synth.compact_chain(300, seed=rank_seed(2, rank))]
-        temps = [300.0 * KB]
-    else:
-        import multiprocessing as mp
-        import numpy as np
-        rng = np.random.default_rng(rank_seed(3, rank))
-        sizes = rng.integers(50, 601, size=256)[:n_chains]
-        jobs = [(int(n), rank_seed(k, rank)) for k, n in enumerate(sizes)]
-        # chain generation is host Python: spread it over the host cores
-        with mp.get_context("spawn").Pool(min(32, os.cpu_count() or 1)) as pool:
-            chains = pool.starmap(_coil_chain, jobs, chunksize=1)
-        temps = list(280.0 * (400.0 / 280.0) ** (np.arange(256) / 255.0) * KB)[:n_chains]
-    systems, movesets, topos = [], [], []
-    for ch in chains:
+    systems, topos = [], []
+    for c in chains:
         T = BondTopology()
-        T.build(ch.resnames, ch.atomnames, ch.res_idx)
-        F = flatten(T)
-        systems.append((ch.xyz, ch.charge, ch.radius, ch.epsilon, F))
-        movesets.append([k for k in range(F.nrb) if F.side_count[k] <= 0.25 * F.n])
+        T.build(c["resnames"], c["atomnames"], c["res_idx"])
+        systems.append((c["xyz"], c["charge"], c["radius"], c["epsilon"], flatten(T)))
         topos.append(T)
-    return chains, systems, movesets, temps, topos
+    return systems, topos
 
 
-def run_ours(args, rank, world, local):
+def _moveset(F):
+    return [k for k in range(F.nrb) if F.side_count[k] <= 0.25 * F.n]
+
+
+def _timed_mc(runner, batch, args, per_step, full_energy, world, local, flush):
+    """W untimed steps, then K timed steps between events on the launching
+    stream (L2 flushed between steps); returns the measurements."""
     import numpy as np
     import torch
     from protein_physics_b200 import _lib
-    from protein_physics_b200.device import DeviceBatch
-    from protein_physics_b200.mc import MCRunner
-    torch.cuda.set_device(local)
-    if world > 1:
-        from protein_physics_b200.dist import init
-        init("nccl", timeout_s=120)
-    chains, systems, movesets, temps, topos = make_workload(args.workload, rank)
-    per_step = 1000 if args.workload == "single" else 100
-    batch = DeviceBatch(systems, precision="mixed")
-    from protein_physics_b200.mc import autotune
-    if args.config:
-        tuned = tuple(int(v) for v in args.config.split(","))
-    else:
-        tuned = autotune(batch, temps, seed=777, policy=2, moveset=movesets,
-                         proposals=1000 if args.workload == "single" else 30)
-    tuned = (tuple(tuned) + (1,))[:3]
-    runner = MCRunner(batch, temps, seed=12345 + rank, policy=2, cur_max0=0.12, moveset=movesets,
-                      cluster_size=tuned[0], threads=tuned[1], spec_teams=tuned[2])
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     stream = torch.cuda.current_stream()
 
     def step():
         runner.run(per_step)
-        runner.reset_energy()  # full energy recomputation every per_step proposals
+        if full_energy:
+            runner.reset_energy()  # the full energy recomputation of every step
 
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
-    ctr0 = batch.move_counters().astype(np.float64)
     st0 = runner.state()
     launches0 = _lib.lib().alma_launch_count()
     rebuild0 = runner.rebuilds
@@ -176,123 +225,240 @@ def run_ours(args, rank, world, local):
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
-    t_wall0 = time.perf_counter()
     with sampler:
         ev0.record(stream)
         for _ in range(args.steps):
-            flush.fill_(1.0)  # L2 flush between steps (256 MiB write)
+            flush.fill_(1.0)
             step()
         ev1.record(stream)
         torch.cuda.synchronize()
-    t_wall = time.perf_counter() - t_wall0
     ms = ev0.elapsed_time(ev1)
     st1 = runner.state()
-    ctr1 = batch.move_counters().astype(np.float64)
-    launches = _lib.lib().alma_launch_count() - launches0 + args.steps  # + the flush fills
-    proposals = float(np.sum(st1["step"] - st0["step"]))
-    accepted = float(np.sum(st1["n_accepted"] - st0["n_accepted"]))
-    # mc kernel time alone (roofline): time one extra chunk without rebuilds
-    dctr = (ctr1 - ctr0).sum(axis=0)
-    ops = dctr[0] * OPS_PAIR + dctr[1] * OPS_HCT + dctr[2] * OPS_SASA
-    from protein_physics_b200.dist import reduce_timing
-    ms_max, prop_total = reduce_timing(ms, proposals, device="cuda")
-    # isolated MC-kernel timing for the roofline: chunk without host rebuild logic
+    return dict(ms=ms, proposals=float(np.sum(st1["step"] - st0["step"])),
+                accepted=float(np.sum(st1["n_accepted"] - st0["n_accepted"])),
+                launches=_lib.lib().alma_launch_count() - launches0 + args.steps,  # + the flush fills
+                rebuilds=runner.rebuilds - rebuild0, clocks=sampler.summary())
+
+
+def _kernel_roofline(runner, batch, tuned, proposals_per_launch):
+    """One extra MC launch alone (no host rebuild step), timed with events
+    on its stream; algorithmic ops from the kernel's own work counters."""
+    import numpy as np
+    import torch
+    stream = torch.cuda.current_stream()
     ke0, ke1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    st0 = runner.state()
     c0 = batch.move_counters().astype(np.float64).sum(axis=0)
-    lim = int(runner.state()["step"].max()) + 200
+    lim = int(st0["step"].max()) + proposals_per_launch
     ke0.record(stream)
     runner.launch(lim)
     ke1.record(stream)
     torch.cuda.synchronize()
     k_ms = ke0.elapsed_time(ke1)
     c1 = batch.move_counters().astype(np.float64).sum(axis=0)
-    k_ops = (c1 - c0)[0] * OPS_PAIR + (c1 - c0)[1] * OPS_HCT + (c1 - c0)[2] * OPS_SASA
-    achieved = k_ops / (k_ms * 1e-3)
-    # e2e through the public API: generate_ensemble from host particle lists
-    from protein_physics_b200 import Particle, PhysicsEngine
-    eng = PhysicsEngine(precision="mixed", seed=99 + rank)
-    e2e_val = None
-    h2d = d2h = 0
-    e2e_single = None
-    if args.workload == "single":
-        ch = chains[0]
-        P0 = [Particle(*x, q, r, e) for x, q, r, e in zip(ch.xyz, ch.charge, ch.radius, ch.epsilon)]
-        n_e2e = max(1, args.steps // 2)
+    st1 = runner.state()
+    d = c1 - c0
+    ops = d[0] * OPS_PAIR + d[1] * OPS_HCT + d[2] * OPS_SASA
+    achieved = ops / (k_ms * 1e-3)
+    name = ("mc_spec_kernel<float,%d,%d> x %d teams" % (tuned[1], tuned[0], tuned[2]) if tuned[2] > 1 else
+            "mc_kernel<float,%d,%d>" % (tuned[1] or 512, tuned[0]))
+    return {"bound": "fp32", "kernel": name, "achieved": achieved / 1e12, "peak": FP32_PEAK_NOMINAL / 1e12,
+            "unit": "TOP/s (FP32+MUFU ops)", "frac": achieved / FP32_PEAK_NOMINAL,
+            "peak_source": "nominal 148 SM x 128 FP32 lanes x 2 x 1965 MHz (no measured FP32 peak in "
+                           "MEASURED_PEAKS.json; the kernel is neither HBM- nor tensor-bound)",
+            "work_per_launch": {"pair_terms": float(d[0]), "hct": float(d[1]), "sasa_visits": float(d[2]),
+                                "moved_atoms": float(d[3]), "proposals": float(np.sum(st1["step"] - st0["step"]))},
+            "kernel_ms": k_ms, "traffic": None}
 
-        def e2e_rate(ncand):
-            P = P0
-            eng.generate_ensemble(P, topos[0], ncand, 50)  # warm
-            torch.cuda.synchronize()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            for _ in range(n_e2e):
-                P = eng.generate_ensemble(P, topos[0], ncand, per_step)[0]
-            e1.record(stream)
-            torch.cuda.synchronize()
-            return n_e2e * ncand * per_step / (e0.elapsed_time(e1) * 1e-3) * world
 
-        # the call the reference arm times: as many candidates as the host has
-        # threads (its OpenMP spans candidates), per_step proposals each
-        ncand = host_threads()
-        e2e_val = e2e_rate(ncand)
-        e2e_single = e2e_rate(1)
-        h2d = ncand * ch.n * 8 * 3 + ch.n * 8 * 3  # coordinates per candidate + charge, radius, epsilon
-        d2h = ncand * ch.n * 8 * 3
-    clocks = sampler.summary()
-    de_err = de_error_vs_fp64(systems[0], movesets[0], runner.state()["cur_max"][0]) if rank == 0 else None
+def run_ours(args, rank, world, local):
+    import numpy as np
+    import torch
+    sys.path.insert(0, PKG)
+    from protein_physics_b200.device import DeviceBatch
+    from protein_physics_b200.mc import BatchedEnsemble, MCRunner, autotune
+    torch.cuda.set_device(local)
+    if world > 1:
+        from protein_physics_b200.dist import init
+        init("nccl", timeout_s=120)
+    if args.workload == "batched":
+        chains, temps = c3_inputs(rank)
+        policy, per_step, full_energy = 0, C3_PER_STEP, False
+    else:
+        chains, temps = [fixture("c2_chain_300res.npz")], [300.0 * KB]
+        policy, per_step, full_energy = 2, C2_PER_STEP, True
+    config = config_of(args.workload, chains)
+    systems, topos = _our_systems(chains)
+    movesets = None if policy == 0 else [_moveset(s[4]) for s in systems]
+    batch = DeviceBatch(systems, precision="mixed")
+    if args.config:
+        tuned = tuple(int(v) for v in args.config.split(","))
+    else:
+        tuned = autotune(batch, temps, seed=777, policy=policy, moveset=movesets,
+                         proposals=1000 if policy == 2 else 30)
+    tuned = (tuple(tuned) + (1,))[:3]
+    runner = MCRunner(batch, temps, seed=12345 + rank, policy=policy, cur_max0=0.12, moveset=movesets,
+                      cluster_size=tuned[0], threads=tuned[1], spec_teams=tuned[2])
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    t = _timed_mc(runner, batch, args, per_step, full_energy, world, local, flush)
+    from protein_physics_b200.dist import reduce_timing
+    ms_max, prop_total = reduce_timing(t["ms"], t["proposals"], device="cuda")
+    roof = _kernel_roofline(runner, batch, tuned, 200 if policy == 2 else 50)
+    # e2e through the public API, host buffers in and out every step
+    if args.workload == "batched":
+        e2e = e2e_batched(systems, temps, tuned, args, world)
+    else:
+        e2e = e2e_single(chains[0], topos[0], args, world)
     out = None
     if rank == 0:
-        value = prop_total / (ms_max * 1e-3)
-        cpu = cpu_baseline(chains[0], topos[0], temps[0], args) if world == 1 else None
-        plain = plain_gpu_baseline(chains[0], temps[0]) if (world == 1 and args.workload == "single") else None
-        ef = energy_force_rate(systems[0], topos[0])
+        stats = {"accept_rate": t["accepted"] / max(1.0, t["proposals"]), "nl_rebuilds": t["rebuilds"],
+                 "rg_A_mean": float(np.mean([rg_of(c["xyz"]) for c in chains])),
+                 "full_row_mean": float(batch.full_len[:batch.natoms].double().mean()),
+                 "half_row_mean": float(batch.half_len[:batch.natoms].double().mean())}
         out = {
-            "metric": "Metropolis proposals/s", "value": value, "unit": "proposals/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "metric": "Metropolis proposals/s", "value": prop_total / (ms_max * 1e-3), "unit": "proposals/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 pair terms, f64 dE",
             "data": "synthetic (seeded NeRF chains, ff14SB parameters from the reference tables)",
-            "config": {"workload": ("single chain, 300 residues compact, %d atoms, torsion moves with j-side <= 25%%"
-                                    " of atoms, T=300 K, 1000 proposals + full energy per step" % chains[0].n)
-                       if args.workload == "single" else
-                       "256 chains x 50-600 residues (%d atoms), T 280-400 K, 100 proposals/chain per step"
-                       % sum(c.n for c in chains),
-                       "atoms": sum(c.n for c in chains),
-                       "rg_A": round(__import__("protein_physics_b200.synth", fromlist=["x"]).radius_of_gyration(
-                           chains[0].xyz), 1),
-                       "accept_rate": accepted / max(1.0, proposals), "nl_rebuilds": runner.rebuilds - rebuild0,
-                       "l2": "flushed between steps (256 MiB write)", "parallelism": "replicas" if world > 1 else "1 GPU"},
-            "clocks": clocks,
-            "gpu_launches": int(launches),
-            "dE_error_vs_fp64": de_err,
+            "config": config, "workload_stats": stats, "clocks": t["clocks"], "gpu_launches": int(t["launches"]),
             "tuned": {"cluster_size": tuned[0], "threads_per_system": tuned[1], "spec_teams": tuned[2]},
-            "wall_s": t_wall,
-            "e2e": {"value": e2e_val, "unit": "proposals/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "candidates": host_threads() if args.workload == "single" else None,
-                    "single_candidate": e2e_single,
-                    "api": "PhysicsEngine.generate_ensemble(host particles, topology, n_candidates, 1000), "
-                           "n_candidates = the host threads, the call the reference arm times; single_candidate: "
-                           "the same with 1 candidate",
-                    "workload": "the reference's own move policy (25 % crankshaft, every rotatable bond), as the "
-                                "reference arm runs it: heavier moves and more list rebuilds than the timed value"},
-            "roofline": {"bound": "fp32", "kernel": ("mc_spec_kernel<float,%d,%d> x %d teams" % (tuned[1], tuned[0], tuned[2])
-                                                    if tuned[2] > 1 else "mc_kernel<float,%d,%d>" % (tuned[1], tuned[0])),
-                         "achieved": achieved / 1e12,
-                         "peak": FP32_PEAK_NOMINAL / 1e12, "unit": "TOP/s (FP32+MUFU ops)",
-                         "frac": achieved / FP32_PEAK_NOMINAL,
-                         "peak_source": "nominal 148 SM x 128 FP32 lanes x 2 x 1965 MHz (no measured FP32 peak "
-                                        "in MEASURED_PEAKS.json; the kernel is neither HBM- nor tensor-bound)",
-                         "work_per_launch": {"pair_terms": float((c1 - c0)[0]), "hct": float((c1 - c0)[1]),
-                                             "sasa_visits": float((c1 - c0)[2]), "proposals": 200},
-                         "kernel_ms": k_ms, "traffic": None},
-            "cpu_baseline": cpu,
-            "plain_gpu_path": plain,
-            "energy_force": ef,
+            "e2e": e2e, "roofline": roof,
         }
+        if world == 1:
+            out["cpu_baseline"] = cpu_baseline(args.workload, chains, temps)
+            if args.workload == "batched":
+                out["single_chain"] = single_chain_section(args)
+            else:
+                out.update(single_extras(chains[0], topos[0], systems[0], movesets[0], runner))
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
         dist.destroy_process_group()
     return out
+
+
+def e2e_batched(systems, temps, tuned, args, world):
+    """BatchedEnsemble.run(100, xyz=host coordinates) per step: host->device
+    copy of every chain's coordinates, the device MC, device->host copy of
+    the final coordinates."""
+    import torch
+    from protein_physics_b200.mc import BatchedEnsemble
+    ens = BatchedEnsemble(systems, temps, seed=4242, shape=tuned)
+    X = ens.run(5).copy()
+    n = max(3, args.steps // 2)
+    p0 = ens.state()["step"].sum()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(n):
+        X = ens.run(C3_PER_STEP, xyz=X)
+    dt = time.perf_counter() - t0
+    props = float(ens.state()["step"].sum() - p0)
+    nbytes = int(X.nbytes)
+    return {"value": props / dt * world, "unit": "proposals/s", "h2d_bytes_per_step": nbytes,
+            "d2h_bytes_per_step": nbytes, "steps": n,
+            "api": "BatchedEnsemble(systems, temperatures).run(100, xyz=host coordinates of all chains): "
+                   "host->device copy, fresh lists and energies, the MC, device->host copy (wall clock)"}
+
+
+def e2e_single(ch, topo, args, world):
+    """PhysicsEngine.generate_ensemble(host particle lists, n candidates,
+    1,000 proposals) with n = the host threads (the call the reference arm
+    times for one chain), and with one candidate."""
+    import torch
+    from protein_physics_b200 import Particle, PhysicsEngine
+    eng = PhysicsEngine(precision="mixed", seed=99)
+    P0 = [Particle(*x, q, r, e) for x, q, r, e in zip(ch["xyz"], ch["charge"], ch["radius"], ch["epsilon"])]
+    n_e2e = max(1, args.steps // 2)
+    stream = torch.cuda.current_stream()
+
+    def rate(ncand):
+        P = P0
+        eng.generate_ensemble(P, topo, ncand, 50)  # warm
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(n_e2e):
+            P = eng.generate_ensemble(P, topo, ncand, C2_PER_STEP)[0]
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return n_e2e * ncand * C2_PER_STEP / (e0.elapsed_time(e1) * 1e-3) * world
+
+    pp = _ref_module()  # one candidate per thread of the reference engine, as its arm runs
+    ref_threads = pp.PhysicsEngine().num_threads() if pp is not None else None
+    ncand = ref_threads or host_threads()
+    n = len(P0)
+    return {"value": rate(ncand), "unit": "proposals/s", "h2d_bytes_per_step": ncand * n * 24 + n * 24,
+            "d2h_bytes_per_step": ncand * n * 24, "candidates": ncand, "reference_threads": ref_threads,
+            "host_threads": host_threads(), "single_candidate": rate(1),
+            "api": "PhysicsEngine.generate_ensemble(host particles, topology, n_candidates, 1000), n_candidates = "
+                   "the host threads; single_candidate: the same with 1 candidate",
+            "workload": "the reference's own move policy (every rotatable bond, 25 % crankshaft), as the reference "
+                        "times it"}
+
+
+def single_extras(ch, topo, system, moveset, runner):
+    """Beside the single-chain number: the reference's plain GPU path, FP64
+    proposals/s, the ΔE error against FP64 and energy+force evals/s."""
+    return {"plain_gpu_path": plain_gpu_baseline(ch, 300.0 * KB),
+            "fp64": fp64_rate(system, moveset),
+            "dE_error_vs_fp64": de_error_vs_fp64(system, moveset, runner.state()["cur_max"][0]),
+            "energy_force": energy_force_rate(system, topo)}
+
+
+def single_chain_section(args):
+    """The single-chain drop-in on the 300-residue compact chain: device
+    rate, its kernel roofline, e2e through generate_ensemble, and the
+    comparators (reference plain GPU path and CPU engine, FP64 rate)."""
+    import torch
+    from protein_physics_b200.device import DeviceBatch
+    from protein_physics_b200.mc import MCRunner, autotune
+
+    class A:
+        steps, warmup = max(3, args.steps // 2), 3
+    ch = fixture("c2_chain_300res.npz")
+    systems, topos = _our_systems([ch])
+    ms = [_moveset(systems[0][4])]
+    temps = [300.0 * KB]
+    batch = DeviceBatch(systems, precision="mixed")
+    tuned = (tuple(autotune(batch, temps, seed=777, policy=2, moveset=ms, proposals=1000)) + (1,))[:3]
+    runner = MCRunner(batch, temps, seed=12345, policy=2, cur_max0=0.12, moveset=ms, cluster_size=tuned[0],
+                      threads=tuned[1], spec_teams=tuned[2])
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    t = _timed_mc(runner, batch, A, C2_PER_STEP, True, 1, torch.cuda.current_device(), flush)
+    out = {"value": t["proposals"] / (t["ms"] * 1e-3), "unit": "proposals/s", "steps": A.steps,
+           "config": config_of("single", [ch]),
+           "workload_stats": {"accept_rate": t["accepted"] / max(1.0, t["proposals"]), "nl_rebuilds": t["rebuilds"],
+                              "full_row_mean": float(batch.full_len[:batch.natoms].double().mean()),
+                              "half_row_mean": float(batch.half_len[:batch.natoms].double().mean())},
+           "tuned": {"cluster_size": tuned[0], "threads_per_system": tuned[1], "spec_teams": tuned[2]},
+           "clocks": t["clocks"], "roofline": _kernel_roofline(runner, batch, tuned, 200),
+           "e2e": e2e_single(ch, topos[0], A, 1),
+           "cpu_baseline": cpu_baseline("single", [ch], temps)}
+    out.update(single_extras(ch, topos[0], systems[0], ms[0], runner))
+    return out
+
+
+def fp64_rate(system, moveset, steps=3):
+    """Proposals/s of the same single-chain workload with FP64 pair terms
+    (the reference's own precision), same launch shape rules."""
+    import torch
+    from protein_physics_b200.device import DeviceBatch
+    from protein_physics_b200.mc import MCRunner
+    b = DeviceBatch([system], precision="fp64")
+    R = MCRunner(b, [300.0 * KB], seed=54321, policy=2, moveset=[moveset])
+    R.run(C2_PER_STEP)
+    torch.cuda.synchronize()
+    st0 = R.state()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        R.run(C2_PER_STEP)
+        R.reset_energy()
+    e1.record()
+    torch.cuda.synchronize()
+    n = float((R.state()["step"] - st0["step"]).sum())
+    return {"value": n / (e0.elapsed_time(e1) * 1e-3), "unit": "proposals/s", "precision": "fp64 pair terms",
+            "steps": steps, "spec_teams": int(R.cfg.spec_teams), "cluster_size": int(R.cfg.cluster_size)}
 
 
 def de_error_vs_fp64(system, moveset, cur_max, n=256):
@@ -323,31 +489,122 @@ def de_error_vs_fp64(system, moveset, cur_max, n=256):
             "n_moves": n, "median_abs_dE": float(np.median(mags)), "unit": "kcal/mol"}
 
 
-def cpu_baseline(ch, topo, T, args, budget_s=12.0):
-    """The reference engine (oracle/_ref, compiled from the reference sources)
-    timed on the host: generate_ensemble on the same chain, one candidate."""
+# ---- the reference engine (oracle/_ref) -------------------------------------------------
+def _ref_module():
     import glob
-    hits = glob.glob(os.path.join(ROOT, "oracle", "_ref", "protein_physics*.so"))
+    hits = glob.glob(os.path.join(ROOT, "oracle", "_ref", "protein_physics.*so"))
     if not hits:
-        return {"value": None, "unit": "proposals/s", "cores": 0, "kind": "reference",
-                "sample": "unavailable: oracle/_ref not built"}
+        return None
     sys.path.insert(0, os.path.dirname(hits[0]))
     import protein_physics as pp
+    return pp
+
+
+def _ref_inputs(pp, c):
     R = pp.BondTopology()
-    R.build(ch.resnames, ch.atomnames, ch.res_idx)
+    R.build(c["resnames"], c["atomnames"], c["res_idx"])
     P = [pp.Particle(*map(float, x), float(q), float(r), float(e)) for x, q, r, e in
-         zip(ch.xyz, ch.charge, ch.radius, ch.epsilon)]
+         zip(c["xyz"], c["charge"], c["radius"], c["epsilon"])]
+    return P, R
+
+
+def stratified(chains, k, offset=0.5):
+    """k chain indices spread evenly over the size order."""
+    import numpy as np
+    order = np.argsort([len(c["xyz"]) for c in chains], kind="stable")
+    return [int(order[min(len(order) - 1, int((s + offset) / k * len(order)))]) for s in range(k)]
+
+
+def ref_batched_rate(pp, chains, temps, picks, n_props, ncand):
+    """The reference on the batched workload: for each picked chain,
+    generate_ensemble(chain, ncand candidates, n_props proposals, its own
+    temperature) — one OpenMP thread per candidate — timed as a whole."""
     eng = pp.PhysicsEngine()
+    inputs = [_ref_inputs(pp, chains[k]) for k in picks]
     t0 = time.perf_counter()
-    eng.generate_ensemble(P, R, 1, 5, T, 0.12)
+    for (P, R), k in zip(inputs, picks):
+        eng.generate_ensemble(P, R, ncand, n_props, temps[k], 0.12)
+    return len(picks) * ncand * n_props, time.perf_counter() - t0
+
+
+def cpu_baseline(kind, chains, temps, budget_s=12.0):
+    """The reference engine (oracle/_ref) on the host cores, a bounded sample
+    of the same workload."""
+    pp = _ref_module()
+    if pp is None:
+        return {"value": None, "unit": "proposals/s", "cores": 0, "kind": "reference",
+                "sample": "unavailable: oracle/_ref not built"}
+    eng = pp.PhysicsEngine()
+    if kind == "batched":
+        ncand = eng.num_threads()
+        picks = stratified(chains, 8)
+        props, dt = ref_batched_rate(pp, chains, temps, picks[:1], 5, ncand)
+        n = max(5, int(budget_s / max(dt, 1e-3) * 5 / len(picks)))
+        props, dt = ref_batched_rate(pp, chains, temps, picks, n, ncand)
+        return {"value": props / dt, "unit": "proposals/s", "cores": ncand, "kind": "reference",
+                "sample": "reference generate_ensemble on 8 chains spread over the size range, %d candidates x %d "
+                          "proposals each, %d proposals in %.1f s" % (ncand, n, props, dt)}
+    P, R = _ref_inputs(pp, chains[0])
+    t0 = time.perf_counter()
+    eng.generate_ensemble(P, R, 1, 5, temps[0], 0.12)
     dt5 = max(1e-3, time.perf_counter() - t0)
     n = max(10, int(budget_s / dt5 * 5))
     t0 = time.perf_counter()
-    eng.generate_ensemble(P, R, 1, n, T, 0.12)
+    eng.generate_ensemble(P, R, 1, n, temps[0], 0.12)
     dt = time.perf_counter() - t0
     return {"value": n / dt, "unit": "proposals/s", "cores": 1, "kind": "reference",
-            "sample": f"reference generate_ensemble(chain of {ch.n} atoms, 1 candidate, {n} proposals) in "
+            "sample": f"reference generate_ensemble(chain of {len(P)} atoms, 1 candidate, {n} proposals) in "
                       f"{dt:.1f} s; one chain runs on one thread (OpenMP spans candidates)"}
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference CPU engine (oracle/_ref) on all host
+    threads, on the same inputs, printing the same config."""
+    if rank != 0:
+        return None
+    pp = _ref_module()
+    if pp is None:
+        return {"impl": "reference", "unavailable": "reference engine not built (oracle/_ref)"}
+    eng = pp.PhysicsEngine()
+    ncand = eng.num_threads()
+    if args.workload == "batched":
+        chains, temps = c3_inputs(0)
+        picks_w = stratified(chains, max(1, args.warmup), offset=0.25)
+        picks = stratified(chains, args.steps)
+        _, dt = ref_batched_rate(pp, chains, temps, picks_w[:1], 5, ncand)
+        n = max(5, int(20.0 / max(1, args.steps + args.warmup) / max(dt, 1e-3) * 5))
+        ref_batched_rate(pp, chains, temps, picks_w, n, ncand)
+        props, dt = ref_batched_rate(pp, chains, temps, picks, n, ncand)
+        sample = ("one chain per step, %d chains spread over the size range (of %d), generate_ensemble with %d "
+                  "candidates x %d proposals each at the chain's temperature" % (args.steps, len(chains), ncand, n))
+    elif args.workload == "single":
+        chains, temps = [fixture("c2_chain_300res.npz")], [300.0 * KB]
+        P, R = _ref_inputs(pp, chains[0])
+        t0 = time.perf_counter()
+        eng.generate_ensemble(P, R, ncand, 3, temps[0], 0.12)
+        per = max(1e-3, time.perf_counter() - t0) / 3
+        n = max(5, int(20.0 / max(1, args.steps + args.warmup) / per))
+        for _ in range(args.warmup):
+            eng.generate_ensemble(P, R, ncand, n, temps[0], 0.12)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            eng.generate_ensemble(P, R, ncand, n, temps[0], 0.12)
+        dt = time.perf_counter() - t0
+        props = args.steps * n * ncand
+        sample = "%d x generate_ensemble(%d candidates x %d proposals), every rotatable bond (the reference " \
+                 "cannot restrict its moves)" % (args.steps, ncand, n)
+    else:
+        return {"impl": "reference", "unavailable": "the reference has no %s workload (no gradient, no MALA)"
+                % args.workload}
+    value = props / dt
+    return {"impl": "reference", "metric": "Metropolis proposals/s", "value": value, "unit": "proposals/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded NeRF chains, ff14SB parameters from the reference tables)",
+            "config": config_of(args.workload, chains),
+            "cpu_baseline": {"value": value, "unit": "proposals/s", "cores": ncand, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "proposals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
 def plain_gpu_baseline(ch, T, budget_s=8.0):
@@ -356,16 +613,15 @@ def plain_gpu_baseline(ch, T, budget_s=8.0):
     chain, one candidate, on this GPU."""
     import glob
     hits = glob.glob(os.path.join(ROOT, "oracle", "_ref", "protein_physics_cuda*.so"))
-    cpu = glob.glob(os.path.join(ROOT, "oracle", "_ref", "protein_physics.*so"))
-    if not hits or not cpu:
+    pp = _ref_module()
+    if not hits or pp is None:
         return {"value": None, "unit": "proposals/s", "unavailable": "oracle/_ref/protein_physics_cuda not built"}
     sys.path.insert(0, os.path.dirname(hits[0]))
-    import protein_physics as pp
     import protein_physics_cuda as pc
     R = pp.BondTopology()
-    R.build(ch.resnames, ch.atomnames, ch.res_idx)
+    R.build(ch["resnames"], ch["atomnames"], ch["res_idx"])
     P = [pc.Particle(*map(float, x), float(q), float(r), float(e)) for x, q, r, e in
-         zip(ch.xyz, ch.charge, ch.radius, ch.epsilon)]
+         zip(ch["xyz"], ch["charge"], ch["radius"], ch["epsilon"])]
     eng = pc.PhysicsEngine()
     t0 = time.perf_counter()
     eng.generate_ensemble(P, R, 1, 5, T, 0.12)
@@ -374,8 +630,7 @@ def plain_gpu_baseline(ch, T, budget_s=8.0):
     t0 = time.perf_counter()
     eng.generate_ensemble(P, R, 1, n, T, 0.12)
     dt = time.perf_counter() - t0
-    # its full-energy path (the reference has no forces): calculate_potential
-    eng.calculate_potential(P, R)
+    eng.calculate_potential(P, R)  # its full-energy path (the reference has no forces)
     t0 = time.perf_counter()
     ne = 0
     while time.perf_counter() - t0 < 2.0 or ne < 3:
@@ -461,46 +716,6 @@ def energy_force_rate(system, topo, steps=20):
             "what": "neighbor list + Born radii + energy terms + analytic dE/dx (alma_forces), mixed precision"}
 
 
-def run_reference(args, rank, world):
-    """--impl reference: the reference CPU engine on all host threads."""
-    if rank != 0:
-        return None
-    import glob
-    hits = glob.glob(os.path.join(ROOT, "oracle", "_ref", "protein_physics*.so"))
-    if not hits:
-        return {"impl": "reference", "unavailable": "reference engine not built (oracle/_ref)"}
-    sys.path.insert(0, os.path.dirname(hits[0]))
-    import protein_physics as pp
-    chains, systems, movesets, temps, topos = make_workload(args.workload, 0)
-    ch = chains[0]
-    R = pp.BondTopology()
-    R.build(ch.resnames, ch.atomnames, ch.res_idx)
-    P = [pp.Particle(*map(float, x), float(q), float(r), float(e)) for x, q, r, e in
-         zip(ch.xyz, ch.charge, ch.radius, ch.epsilon)]
-    eng = pp.PhysicsEngine()
-    ncand = eng.num_threads()
-    t0 = time.perf_counter()
-    eng.generate_ensemble(P, R, ncand, 3, temps[0], 0.12)
-    per = max(1e-3, time.perf_counter() - t0) / 3
-    n = max(5, int(20.0 / max(1, args.steps + args.warmup) / per))
-    for _ in range(args.warmup):
-        eng.generate_ensemble(P, R, ncand, n, temps[0], 0.12)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        eng.generate_ensemble(P, R, ncand, n, temps[0], 0.12)
-    dt = time.perf_counter() - t0
-    value = args.steps * n * ncand / dt
-    return {"impl": "reference", "metric": "Metropolis proposals/s", "value": value, "unit": "proposals/s",
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (same seeded chain)",
-            "config": {"workload": f"reference generate_ensemble on the {ch.n}-atom chain, {ncand} candidates x "
-                                   f"{n} proposals per step (one chain per OpenMP thread)"},
-            "cpu_baseline": {"value": value, "unit": "proposals/s", "cores": ncand, "kind": "reference",
-                             "sample": f"{args.steps} x {ncand} chains x {n} proposals"},
-            "e2e": {"value": value, "unit": "proposals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-
-
 def _line(metric, value, unit, args, ms_per_step, config, clocks, launches, **extra):
     out = {"metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -518,14 +733,13 @@ def run_globule(args):
     gradient, Metropolis-Hastings)."""
     import numpy as np
     import torch
-    from protein_physics_b200 import _lib, synth
+    sys.path.insert(0, PKG)
+    from protein_physics_b200 import _lib
     from protein_physics_b200.device import DeviceBatch
-    from protein_physics_b200.topology import BondTopology, flatten
     from protein_physics_b200.torsion import MALARunner, TorsionSpace, minimize
-    ch = synth.compact_chain(1000, seed=4)
-    T = BondTopology()
-    T.build(ch.resnames, ch.atomnames, ch.res_idx)
-    system = (ch.xyz, ch.charge, ch.radius, ch.epsilon, flatten(T))
+    ch = fixture("c4_globule_1000res.npz")
+    systems, topos = _our_systems([ch])
+    system, T = systems[0], topos[0]
     ef = energy_force_rate(system, T)
     b = DeviceBatch([system], precision="mixed")
     ts = TorsionSpace(b)
@@ -567,10 +781,10 @@ def run_globule(args):
     n = int(st1["n_proposed"][0] - st0["n_proposed"][0])
     acc = int(st1["n_accepted"][0] - st0["n_accepted"][0])
     return _line("MALA torsion proposals/s", n / (ms * 1e-3), "proposals/s", args, ms / args.steps,
-                 {"workload": "1,000-residue collapsed chain, %d atoms, Rg %.1f A; 500 descent steps, then MALA "
+                 {"workload": "1,000-residue globule, %d atoms, Rg %.1f A; 500 descent steps, then MALA "
                               "(all %d rotatable bonds per proposal, step 0.5 deg, truncated drift), 300 K, "
-                              "10 proposals per step" % (ch.n, synth.radius_of_gyration(ch.xyz), ts.nrb),
-                  "atoms": ch.n, "mala_accept_rate": acc / max(1, n), "mala_step_scale": float(st1["scale"][0]),
+                              "10 proposals per step" % (len(ch["xyz"]), rg_of(ch["xyz"]), ts.nrb),
+                  "atoms": len(ch["xyz"]), "mala_accept_rate": acc / max(1, n), "mala_step_scale": float(st1["scale"][0]),
                   "launch": "one CUDA graph per proposal (%.0f proposals/s when launched from the host)" % eager_rate,
                   "l2": "inputs > L2 (16k atoms x lists)"},
                  sampler.summary(), _lib.lib().alma_launch_count() - l0,
@@ -630,16 +844,13 @@ def run_replica(args):
     torsion proposals 1:3, replica exchange every 100 sweeps.  One bench
     step = one exchange interval (100 proposals per replica)."""
     import torch
-    from protein_physics_b200 import _lib, synth
+    sys.path.insert(0, PKG)
+    from protein_physics_b200 import _lib
     from protein_physics_b200.replica import ReplicaExchange, geometric_ladder
-    from protein_physics_b200.topology import BondTopology, flatten
-    ch = synth.multidomain_chain(4, 1000, 10, seed=11)
-    T = BondTopology()
-    T.build(ch.resnames, ch.atomnames, ch.res_idx)
-    F = flatten(T)
-    moveset = [k for k in range(F.nrb) if F.side_count[k] <= 0.25 * F.n]
-    RE = ReplicaExchange((ch.xyz, ch.charge, ch.radius, ch.epsilon, F), geometric_ladder(300, 450, 16), seed=9,
-                         moveset=moveset, minimize_steps=500, mala_warmup=400)
+    ch = fixture("c5_multidomain_4x1000res.npz")
+    systems, _ = _our_systems([ch])
+    RE = ReplicaExchange(systems[0], geometric_ladder(300, 450, 16), seed=9, moveset=_moveset(systems[0][4]),
+                         minimize_steps=500, mala_warmup=400)
     for _ in range(args.warmup):
         RE.interval(100)
     torch.cuda.synchronize()
@@ -658,8 +869,8 @@ def run_replica(args):
     return _line("Metropolis proposals/s (replica exchange)", (RE.proposals - p0) / (ms * 1e-3), "proposals/s", args,
                  ms / args.steps,
                  {"workload": "16 replicas x %d-atom 4-domain chain (%d atoms), T 300-450 K geometric, "
-                              "MALA:torsion 1:3, exchange every 100 sweeps" % (ch.n, 16 * ch.n),
-                  "atoms": 16 * ch.n, "l2": "inputs > L2"},
+                              "MALA:torsion 1:3, exchange every 100 sweeps" % (len(ch["xyz"]), 16 * len(ch["xyz"])),
+                  "atoms": 16 * len(ch["xyz"]), "l2": "inputs > L2"},
                  sampler.summary(), _lib.lib().alma_launch_count() - l0, exchange=st)
 
 
@@ -667,16 +878,30 @@ def run_profile_case(args):
     """Small cases for ncu.  "mc": the single-chain workload, 100 warm-up
     proposals, then exactly one mc launch of up to 200 proposals (it stops
     at the first drift flag); --config CL,NT[,K] picks the launch shape.
-    "forces": the same chain, one energy evaluation and one alma_forces
-    call (4 gradient kernels).  "energy": the first 48 chains of the batched
-    workload (about 0.24M atoms, rows well above L2), one neighbor-list
-    build, one full energy evaluation and one gradient (alma_forces)."""
+    "mc-batched": the first 48 chains of the batched workload (~0.25 M
+    atoms), 20 warm-up proposals per chain, then one mc launch of up to 20
+    proposals per chain.  "forces": the single chain, one energy evaluation
+    and one alma_forces call (4 gradient kernels).  "energy": the first 48
+    chains of the batched workload, one neighbor-list build, one full energy
+    evaluation and one gradient (alma_forces)."""
     import torch
+    sys.path.insert(0, PKG)
     from protein_physics_b200.device import DeviceBatch
     from protein_physics_b200.mc import MCRunner
-    if args.profile == "energy":
-        chains, systems, _, _, _ = make_workload("batched", 0, n_chains=48)
+    if args.profile in ("energy", "mc-batched"):
+        chains, temps = c3_inputs(0, n_chains=48)
+        systems, _ = _our_systems(chains)
         batch = DeviceBatch(systems, precision="mixed")
+        if args.profile == "mc-batched":
+            runner = MCRunner(batch, temps, seed=12345, policy=0, cluster_size=1, threads=args.threads,
+                              spec_teams=1)
+            runner.run(20)
+            lim = int(runner.state()["step"].max()) + 20
+            runner.launch(lim)
+            torch.cuda.synchronize()
+            print(json.dumps({"profile_case": "mc-batched", "systems": len(chains), "atoms": batch.natoms,
+                              "proposals": int(runner.state()["step"].sum())}))
+            return
         batch.build_nl()
         terms = batch.energy_terms()
         batch.forces()
@@ -685,32 +910,35 @@ def run_profile_case(args):
                           "half_entries": int(batch.half_len.sum()), "full_entries": int(batch.full_len.sum()),
                           "total_energy": float(terms[:, 4].sum())}))
         return
-    chains, systems, movesets, temps, topos = make_workload("single", 0)
+    ch = fixture("c2_chain_300res.npz")
+    systems, _ = _our_systems([ch])
+    temps = [300.0 * KB]
     batch = DeviceBatch(systems, precision="mixed")
     if args.profile == "forces":
         batch.energy_terms()
         g = batch.forces()
         torch.cuda.synchronize()
-        print(json.dumps({"profile_case": "forces", "atoms": chains[0].n, "grad_norm": float(g.norm())}))
+        print(json.dumps({"profile_case": "forces", "atoms": batch.natoms, "grad_norm": float(g.norm())}))
         return
     cl, nt, k = (tuple(int(v) for v in args.config.split(",")) + (1,))[:3] if args.config else \
         (args.cluster, args.threads, 1)
-    runner = MCRunner(batch, temps, seed=12345, policy=2, moveset=movesets, cluster_size=cl, threads=nt,
-                      spec_teams=k)
+    runner = MCRunner(batch, temps, seed=12345, policy=2, moveset=[_moveset(systems[0][4])], cluster_size=cl,
+                      threads=nt, spec_teams=k)
     runner.run(100)
     lim = int(runner.state()["step"].max()) + 200
     runner.launch(lim)
     torch.cuda.synchronize()
     st = runner.state()
-    print(json.dumps({"profile_case": "single chain", "atoms": chains[0].n, "steps_done": int(st["step"][0]),
+    print(json.dumps({"profile_case": "single chain", "atoms": batch.natoms, "steps_done": int(st["step"][0]),
                       "cluster": cl, "threads": nt, "spec_teams": k}))
 
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--profile", nargs="?", const="mc", default=None, choices=["mc", "forces", "energy"],
-                    help="a small case for ncu: one mc launch (mc), one gradient evaluation (forces) "
-                         "or one batched list build + energy evaluation (energy)")
+    ap.add_argument("--profile", nargs="?", const="mc", default=None,
+                    choices=["mc", "mc-batched", "forces", "energy"],
+                    help="a small case for ncu: one mc launch (mc: single chain; mc-batched: 48 chains), one "
+                         "gradient evaluation (forces) or one batched list build + energy evaluation (energy)")
     ap.add_argument("--config", default="", help="CL,NT[,K]: cluster size, CTA size and speculative teams "
                                                  "instead of the autotuner")
     ap.add_argument("--cluster", type=int, default=16)
@@ -719,7 +947,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="single", choices=["single", "batched", "globule", "replica"])
+    ap.add_argument("--workload", default="batched", choices=["batched", "single", "globule", "replica"])
     args = ap.parse_args()
     rank, world, local = rank_info()
     if args.profile:

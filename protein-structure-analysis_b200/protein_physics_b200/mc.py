@@ -281,3 +281,82 @@ def run_landscape(engine, initial_state, topology, n_snapshots, steps_per_snapsh
         energies.append(float(shot.energy_terms()[0, 4].item()))
     cur_max = float(runner.state()["cur_max"][0])
     return snaps, energies, cur_max
+
+
+class BatchedEnsemble:
+    """Many independent chains — each its own atoms, topology and
+    temperature — advanced together by the device MC: the batched form of
+    generate_ensemble with one candidate per chain (the reference runs
+    such chains one call, or one OpenMP thread, at a time).
+
+    systems: [(xyz [n,3], charge, radius, epsilon, topology), ...] with a
+    BondTopology (or its flatten()) per chain; temperatures in kcal/mol
+    (scalar broadcast); policy 0 is generate_ensemble's proposal policy.
+    The device batch, neighbor lists and launch shape are set up once;
+    each run() is one host round trip: coordinates in (optional), steps
+    proposals per chain, coordinates out."""
+
+    def __init__(self, systems, temperatures, seed=0, precision="mixed", max_angle=0.12, policy=0, moveset=None,
+                 shape=None):
+        sys_flat = []
+        for x, q, r, e, topo in systems:
+            flat = topo if hasattr(topo, "excl_ptr") else flatten(topo)
+            if flat.nrb == 0:
+                raise ValueError("a chain has no rotatable bonds")
+            sys_flat.append((np.asarray(x, np.float64).reshape(-1, 3), q, r, e, flat))
+        self.batch = DeviceBatch(sys_flat, precision=precision)
+        self.temperatures = np.broadcast_to(np.asarray(temperatures, np.float64), (self.batch.nsys,)).copy()
+        self.max_angle = float(max_angle)
+        self.policy, self.moveset = int(policy), moveset
+        if shape is None:
+            cl, k = auto_shape(self.batch.nsys)
+            shape = (cl, 0, k)
+        self.shape = tuple(shape)
+        self.runner = MCRunner(self.batch, self.temperatures, seed, policy=self.policy, cur_max0=self.max_angle,
+                               moveset=moveset, cluster_size=self.shape[0], threads=self.shape[1],
+                               spec_teams=self.shape[2])
+        n = self.batch.natoms
+        self._host_in = torch.empty((n, 3), dtype=torch.float64, pin_memory=True)
+        self._host_out = torch.empty((n, 3), dtype=torch.float64, pin_memory=True)
+        self._dev = torch.empty((n, 3), dtype=torch.float64, device="cuda")
+
+    @property
+    def atom_offsets(self):
+        return self.batch.atom_off_h.copy()
+
+    def restart(self, xyz):
+        """New starting coordinates [natoms, 3] (all chains, concatenated):
+        a fresh list, radii and energy per chain, cur_max back to max_angle
+        (as every generate_ensemble call starts); the random stream goes on."""
+        b = self.batch
+        src = xyz if isinstance(xyz, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(xyz, np.float64))
+        if src.device.type == "cpu" and not src.is_pinned():
+            self._host_in.copy_(src.reshape(b.natoms, 3))
+            src = self._host_in
+        self._dev.copy_(src.reshape(b.natoms, 3), non_blocking=True)
+        b.xyz[:b.natoms, :3].copy_(self._dev)
+        b.nl_ready = False
+        b.invalidate_sasa()
+        b.status.zero_()
+        st = self.runner.state()
+        st["cur_max"] = self.max_angle
+        st["acc_win"] = st["tot_win"] = st["need_rebuild"] = 0
+        self.runner.states.copy_(torch.from_numpy(st.view(np.uint8).copy()))
+        b.build_nl()
+        self.runner.reset_energy()
+
+    def run(self, steps, xyz=None):
+        """steps proposals per chain (from xyz when given, else from where
+        the last run left the chains); returns the final coordinates
+        [natoms, 3] as a host array (split with atom_offsets)."""
+        if steps <= 0:
+            raise ValueError("steps must be positive")
+        if xyz is not None:
+            self.restart(xyz)
+        self.runner.run(int(steps))
+        self._host_out.copy_(self.batch.xyz[:self.batch.natoms, :3], non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        return self._host_out.numpy()
+
+    def state(self):
+        return self.runner.state()

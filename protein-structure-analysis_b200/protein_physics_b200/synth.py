@@ -8,13 +8,16 @@ reference's residue bond templates, so BondTopology.build gives the
 reference exclusions / rotatable bonds.  Charges, R* and epsilon come from
 data/ff_params.json (the reference's amber_params ff14SB lookup).
 
+This module needs numpy and scipy only (no package-relative imports), so
+a benchmark can load it by path to build inputs for another engine.
+
 Workloads (residue counts and shapes of the reference's benchmark
 configurations, all seeded):
   * ``chain(n_res, seed)``      — phi ~ N(-60, 15), psi ~ N(-45, 15) deg,
                                   chi from the wells {60, 180, 300} +- U(10)
-  * ``compact_chain(...)``      — the same, then collapsed by seeded torsion
-                                  Monte Carlo on a radius-of-gyration restraint
-                                  plus a soft heavy-atom clash penalty
+  * ``compact_chain(...)``      — a coil chain collapsed in torsion space
+                                  (L-BFGS over phi / psi of a soft-sphere bead
+                                  model on a radius-of-gyration restraint)
   * ``coil_chain(...)``         — helix/coil phi-psi mixture
 """
 from __future__ import annotations
@@ -31,6 +34,8 @@ with open(os.path.join(_DATA, "residue_ic.json")) as _f:
     _IC = json.load(_f)
 with open(os.path.join(_DATA, "ff_params.json")) as _f:
     _FF = json.load(_f)
+with open(os.path.join(_DATA, "residue_tables.json")) as _f:
+    _BOND_TEMPLATES = json.load(_f)["bond_templates"]
 
 RESIDUES = ["ALA", "ARG", "ASN", "ASP", "CYS", "GLN", "GLU", "GLY", "HID", "ILE",
             "LEU", "LYS", "MET", "PHE", "PRO", "SER", "THR", "TRP", "TYR", "VAL"]
@@ -214,9 +219,8 @@ def _intra_pairs(res, order):
     """(i, j) index pairs of one residue's atoms >= 4 bonds apart (may clash)."""
     if res in _INTRA:
         return _INTRA[res]
-    from .topology import BOND_TEMPLATES
     adj = {}
-    for a, b in BOND_TEMPLATES[res]:
+    for a, b in _BOND_TEMPLATES[res]:
         adj.setdefault(a, []).append(b)
         adj.setdefault(b, []).append(a)
     idx = {nm: k for k, nm in enumerate(order)}
@@ -468,57 +472,140 @@ def _torsion(a, b, c, d):
     return math.degrees(math.atan2(np.linalg.norm(b2) * np.dot(b1, n2), np.dot(n1, n2)))
 
 
-def collapse(ch: Chain, seed, rg_target, moves=4000, k_rg=1.0, ca_clash=5.0, k_clash=50.0, temp=1.0, domains=None):
-    """Seeded backbone collapse: torsion Monte Carlo on the C-alpha trace
-    (phi/psi pivots) with the energy k_rg (Rg_CA - rg_target)^2 +
-    k_clash sum (ca_clash - d)^2 over C-alpha pairs >= 3 residues apart, then
-    a rebuild from the resulting phi/psi and a sidechain repack.  Rg is
-    measured on C-alpha atoms; with domains = [(r0, r1), ...] the Rg term is
-    summed over those residue ranges instead (multi-domain chains)."""
-    from scipy.spatial import cKDTree
+# Heavy sidechain atoms per residue: size of the sidechain bead of the
+# collapse model.
+_N_SIDECHAIN = {"GLY": 0, "ALA": 1, "SER": 2, "CYS": 2, "VAL": 3, "THR": 3, "PRO": 3, "ILE": 4, "LEU": 4, "ASP": 4,
+                "ASN": 4, "MET": 4, "GLU": 5, "GLN": 5, "LYS": 5, "HID": 6, "PHE": 7, "ARG": 7, "TYR": 8, "TRP": 10}
 
+
+class _BeadChain:
+    """Collapse model of a built chain: per residue N, CA, a sidechain bead
+    and C (in that order, so every torsion moves a suffix of the points),
+    each a soft sphere; the backbone phi / psi are the degrees of freedom
+    (omega and the bond geometry stay as built)."""
+
+    def __init__(self, ch, radius_scale):
+        n_res = len(ch.sequence)
+        ridx = np.asarray(ch.res_idx)
+        first = np.searchsorted(ridx, np.arange(n_res + 1))[:-1]
+        N, CA, C = ch.xyz[first], ch.xyz[first + 1], ch.xyz[first + 2]
+        nsc = np.array([_N_SIDECHAIN[r] for r in ch.sequence])
+        # bead on the ideal C-beta direction, further out for larger sidechains
+        b, c = CA - N, C - CA
+        d = -0.58273431 * np.cross(b, c) + 0.56802827 * b - 0.54067466 * c
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        B = CA + np.minimum(1.53 + 0.45 * np.maximum(nsc - 1, 0), 4.0)[:, None] * d
+        self.X0 = np.stack([N, CA, B, C], 1).reshape(-1, 3)
+        self.rad = radius_scale * np.stack([np.full(n_res, 1.6), np.full(n_res, 1.9),
+                                            np.where(nsc > 0, 1.9 + 0.35 * np.sqrt(nsc), 0.0),
+                                            np.full(n_res, 1.7)], 1).reshape(-1)
+        self.res = np.repeat(np.arange(n_res), 4)
+        self.bead = np.tile(np.arange(4) == 2, n_res)
+        self.real = np.flatnonzero(self.rad > 0)
+        tors = []
+        for r in range(n_res):
+            if r > 0 and ch.sequence[r] != "PRO":
+                tors.append((4 * r, 4 * r + 1, 4 * r + 2))  # phi about N-CA: moves the bead, C and beyond
+            if r < n_res - 1:
+                tors.append((4 * r + 1, 4 * r + 3, 4 * r + 4))  # psi about CA-C: moves the next residue on
+        self.tors = np.array(tors, dtype=np.int64).reshape(-1, 3)
+        self.owner = np.searchsorted(self.tors[:, 2], np.arange(self.X0.shape[0]), side="right") - 1
+
+    def coords(self, theta):
+        """Points after turning torsion k by theta[k] (radians), axes as built:
+        x -> T_1 o ... o T_k(p) (x), k(p) the last torsion moving point p."""
+        X0, t = self.X0, self.tors
+        u = X0[t[:, 1]] - X0[t[:, 0]]
+        u /= np.linalg.norm(u, axis=1, keepdims=True)
+        A = X0[t[:, 0]]
+        c, s = np.cos(theta), np.sin(theta)
+        ux, uy, uz = u[:, 0], u[:, 1], u[:, 2]
+        k1 = 1.0 - c
+        R = np.empty((len(theta), 3, 3))
+        R[:, 0, 0], R[:, 0, 1], R[:, 0, 2] = c + ux * ux * k1, ux * uy * k1 - uz * s, ux * uz * k1 + uy * s
+        R[:, 1, 0], R[:, 1, 1], R[:, 1, 2] = uy * ux * k1 + uz * s, c + uy * uy * k1, uy * uz * k1 - ux * s
+        R[:, 2, 0], R[:, 2, 1], R[:, 2, 2] = uz * ux * k1 - uy * s, uz * uy * k1 + ux * s, c + uz * uz * k1
+        tk = A - np.einsum("kij,kj->ki", R, A)
+        Ms = np.empty_like(R)
+        ts = np.empty_like(A)
+        M, tt = np.eye(3), np.zeros(3)
+        for k in range(len(theta)):  # cumulative composition, outermost torsion first
+            tt = M @ tk[k] + tt
+            M = M @ R[k]
+            Ms[k], ts[k] = M, tt
+        X = X0.copy()
+        sel = self.owner >= 0
+        w = self.owner[sel]
+        X[sel] = np.einsum("pij,pj->pi", Ms[w], X0[sel]) + ts[w]
+        return X
+
+    def energy(self, X, groups, rg_target, k_rg, k_rep):
+        """k_rg sum_g (Rg_g - target)^2 over the point groups + k_rep sum
+        (r_i + r_j - d)^2 over overlapping pairs two or more residues apart
+        (bead pairs of neighbouring residues too); returns (E, dE/dX)."""
+        from scipy.spatial import cKDTree
+        g = np.zeros_like(X)
+        E = 0.0
+        for idx in groups:
+            d = X[idx] - X[idx].mean(0)
+            rg = math.sqrt((d * d).sum(1).mean())
+            E += k_rg * (rg - rg_target) ** 2
+            g[idx] += 2.0 * k_rg * (rg - rg_target) * d / (len(idx) * rg)
+        P = X[self.real]
+        pr = cKDTree(P).query_pairs(2.0 * self.rad.max(), output_type="ndarray")
+        i, j = self.real[pr[:, 0]], self.real[pr[:, 1]]
+        dr = np.abs(self.res[i] - self.res[j])
+        keep = (dr >= 2) | ((dr == 1) & self.bead[i] & self.bead[j])
+        i, j = i[keep], j[keep]
+        v = X[i] - X[j]
+        dist = np.sqrt((v * v).sum(1))
+        d0 = self.rad[i] + self.rad[j]
+        m = dist < d0
+        i, j, v, dist, d0 = i[m], j[m], v[m], dist[m], d0[m]
+        E += k_rep * float(((d0 - dist) ** 2).sum())
+        f = (-2.0 * k_rep * (d0 - dist) / np.maximum(dist, 1e-9))[:, None] * v
+        np.add.at(g, i, f)
+        np.add.at(g, j, -f)
+        return E, g
+
+    def torsion_grad(self, X, g):
+        """dE/dtheta_k = u_k . sum over the moved suffix of (x - a_k) x g."""
+        xg = np.cross(X, g)
+        Sxg = np.concatenate([np.cumsum(xg[::-1], 0)[::-1], np.zeros((1, 3))])
+        Sg = np.concatenate([np.cumsum(g[::-1], 0)[::-1], np.zeros((1, 3))])
+        t = self.tors
+        u = X[t[:, 1]] - X[t[:, 0]]
+        u /= np.linalg.norm(u, axis=1, keepdims=True)
+        return (u * (Sxg[t[:, 2]] - np.cross(X[t[:, 0]], Sg[t[:, 2]]))).sum(1)
+
+
+def collapse(ch: Chain, seed, rg_target, iters=6000, k_rg=5.0, k_rep=10.0, radius_scale=0.85, domains=None):
+    """Seeded backbone collapse: L-BFGS over every backbone phi / psi of a
+    soft-sphere bead model (N, CA, C and one sidechain bead per residue) on
+    k_rg (Rg - rg_target)^2 plus the overlap penalty, then a rebuild from
+    the resulting phi / psi and a seeded sidechain packing.  The restraint
+    target sits below the Rg wanted: the overlap penalty holds the chain
+    out at about the density of packed beads.  With domains = [(r0, r1),
+    ...] the Rg term is one per residue range (multi-domain chains)."""
+    from scipy.optimize import minimize
     rng = np.random.default_rng(seed)
+    model = _BeadChain(ch, radius_scale)
+    if domains:
+        groups = [np.intersect1d(model.real, np.arange(4 * r0, 4 * r1)) for r0, r1 in domains]
+    else:
+        groups = [model.real]
+
+    def f(theta):
+        X = model.coords(theta)
+        E, g = model.energy(X, groups, rg_target, k_rg, k_rep)
+        return E, model.torsion_grad(X, g)
+
+    res = minimize(f, np.zeros(len(model.tors)), jac=True, method="L-BFGS-B",
+                   options={"maxiter": int(iters), "maxfun": 2 * int(iters)})
+    X = model.coords(res.x).reshape(-1, 4, 3)
+    N, CA, C = X[:, 0], X[:, 1], X[:, 3]
     n_res = len(ch.sequence)
-    ridx = np.asarray(ch.res_idx)
-    first = np.searchsorted(ridx, np.arange(n_res + 1))
-    bbn = np.stack([ch.xyz[first[r]:first[r] + 3] for r in range(n_res)])  # [n_res, 3(N,CA,C), 3]
-    X = bbn.reshape(-1, 3).copy()
-
-    def energy(X):
-        ca = X[1::3]
-        if domains:
-            e = k_rg * sum((radius_of_gyration(ca[r0:r1]) - rg_target) ** 2 for r0, r1 in domains)
-        else:
-            e = k_rg * (radius_of_gyration(ca) - rg_target) ** 2
-        pairs = cKDTree(ca).query_pairs(ca_clash, output_type="ndarray")
-        if len(pairs):
-            far = np.abs(pairs[:, 0] - pairs[:, 1]) >= 3
-            d = np.linalg.norm(ca[pairs[far, 0]] - ca[pairs[far, 1]], axis=1)
-            e += k_clash * float(((ca_clash - d) ** 2).sum())
-        return e
-
-    E = energy(X)
-    for _ in range(moves):
-        r = int(rng.integers(1, n_res - 1))
-        is_phi = rng.random() < 0.5 and ch.sequence[r] != "PRO"
-        a, b = (3 * r, 3 * r + 1) if is_phi else (3 * r + 1, 3 * r + 2)
-        side = np.arange(b + 1, X.shape[0])
-        if side.size > X.shape[0] // 2:
-            side = np.arange(0, a)
-        delta = math.radians(rng.uniform(-90.0, 90.0))
-        o = X[a]
-        u = X[b] - o
-        u /= np.linalg.norm(u)
-        v = X[side] - o
-        c, s = math.cos(delta), math.sin(delta)
-        trial = X.copy()
-        trial[side] = o + v * c + np.cross(u, v) * s + np.outer(v @ u, u) * (1 - c)
-        Et = energy(trial)
-        if Et < E or rng.random() < math.exp(-(Et - E) / temp):
-            X, E = trial, Et
-    N, CA, C = X[0::3], X[1::3], X[2::3]
-    phi = ch.phi.copy()
-    psi = ch.psi.copy()
+    phi, psi = ch.phi.copy(), ch.psi.copy()
     for r in range(n_res):
         if r > 0 and ch.sequence[r] != "PRO":
             phi[r] = _torsion(C[r - 1], N[r], CA[r], C[r])
@@ -529,21 +616,22 @@ def collapse(ch: Chain, seed, rg_target, moves=4000, k_rg=1.0, ca_clash=5.0, k_c
     return pack_sidechains(ch.sequence, phi, psi, frames, bbpos, rng)
 
 
-def compact_chain(n_res, seed, rg_target=None, moves=4000):
-    """A collapsed chain (default C-alpha Rg target 2.2 * n_res^0.38 Å).
-    The pivot collapse reaches the target near 300 residues; longer chains
-    stay well above it (1,000 residues: Rg ~58 Å for a 30 Å target)."""
+def compact_chain(n_res, seed, rg_target=None, iters=6000):
+    """A coil chain collapsed by the bead model (collapse).  The default
+    restraint target 0.7 * 2.2 * n_res^0.38 Å ends near the Rg of a packed
+    globular protein of that length (300 residues: ~18 Å all-atom); the
+    device relaxation of workloads.py then clears the remaining clashes."""
     ch = coil_chain(n_res, seed)
     if rg_target is None:
-        rg_target = 2.2 * n_res ** 0.38
-    return collapse(ch, seed + 7919, rg_target, moves=moves)
+        rg_target = 0.7 * 2.2 * n_res ** 0.38
+    return collapse(ch, seed + 7919, rg_target, iters=iters)
 
 
-def multidomain_chain(n_domains, domain_res, linker_res, seed, moves=None):
+def multidomain_chain(n_domains, domain_res, linker_res, seed, iters=None):
     """n_domains compact domains of domain_res residues joined by coil
-    linkers of linker_res residues: one coil chain collapsed with a per-domain
-    Rg restraint (target 2.2 * domain_res^0.38 Å each)."""
+    linkers of linker_res residues: one coil chain collapsed with one Rg
+    restraint per domain."""
     n_res = n_domains * domain_res + (n_domains - 1) * linker_res
     ch = coil_chain(n_res, seed)
     doms = [(d * (domain_res + linker_res), d * (domain_res + linker_res) + domain_res) for d in range(n_domains)]
-    return collapse(ch, seed + 7919, 2.2 * domain_res ** 0.38, moves=moves or 4 * n_res, domains=doms)
+    return collapse(ch, seed + 7919, 0.7 * 2.2 * domain_res ** 0.38, iters=iters or 6000, domains=doms)

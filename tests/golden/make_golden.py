@@ -1,6 +1,7 @@
 """Generates the golden vectors in tests/golden/ from the reference itself.
 
     python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py --workloads [wl_c2 wl_c4 wl_c5]
 
 Needs the reference tree (ALMA sources + data) and its compiled engine
 (oracle/_ref, `make -C oracle ref`).  Every number stored here is produced
@@ -14,6 +15,9 @@ from its python/amber_params.py.  Inputs:
   insulin    data/SM_P01308.pdb, heavy atoms, 3 disulfides, H charges
              folded onto heavy atoms (amber_params.missing_hydrogen_charge)
   synth64    the seeded synthetic 64-residue chain (protein_physics_b200.synth)
+  wl_c2/4/5  the benchmark chains in workloads/ (300-residue compact chain,
+             1,000-residue globule, 4 x 1,000-residue multi-domain chain);
+             inputs stay in workloads/, the golden keeps their SHA-256
 
 PDB reading mirrors the reference parser's rules (python/gui_main.py:281-605):
 first model only, water and nucleotide residues dropped, non-finite
@@ -105,13 +109,17 @@ def topo_record(pp, sysd):
     excl_rows = [list(e) for e in T.excl]
     excl_cnt = np.array([len(e) for e in excl_rows], np.int64)
     excl_flat = np.array([j for e in excl_rows for j in e], np.int32)
-    sides = [list(s) for s in T.rot_bond_sides]
-    side_cnt = np.array([len(s) for s in sides], np.int64)
-    side_flat = np.array([j for s in sides for j in s], np.int32)
+    if len(sysd["xyz"]) < 20000:
+        sides = [list(s) for s in T.rot_bond_sides]
+        side_cnt = np.array([len(s) for s in sides], np.int64)
+        side_flat = np.array([j for s in sides for j in s], np.int32)
+    else:  # ~10^8 side entries: counts only (the DFS lists would not fit in Python lists)
+        side_cnt = np.array([T.j_side(rb.i, rb.j).__len__() for rb in T.rot_bonds], np.int64)
+        side_flat = None
     return T, dict(
         excl_cnt=excl_cnt, excl_sha=sha(excl_flat),
         rb=np.array([(rb.i, rb.j, int(rb.kind)) for rb in T.rot_bonds], np.int32).reshape(-1, 3),
-        side_cnt=side_cnt, side_sha=sha(side_flat),
+        side_cnt=side_cnt, side_sha=sha(side_flat) if side_flat is not None else "",
         rot_bond_scale=np.array(list(T.rot_bond_scale)),
         dih=np.stack([T.dih_a, T.dih_b, T.dih_c, T.dih_d], 1).astype(np.int32) if T.num_dihedrals else
         np.zeros((0, 4), np.int32),
@@ -122,7 +130,7 @@ def topo_record(pp, sysd):
         ss=np.array(list(T.disulfide_pairs), np.int32).reshape(-1, 2))
 
 
-def golden_system(name, sysd, R, pp, rng, n_torsion=24, n_crank=8, full_nl=False):
+def golden_system(name, sysd, R, pp, rng, n_torsion=24, n_crank=8, full_nl=False, inputs=True, fixture=None):
     from oracle import RefEngine  # noqa: F401
     out = {}
     T, trec = topo_record(pp, sysd)
@@ -155,8 +163,14 @@ def golden_system(name, sysd, R, pp, rng, n_torsion=24, n_crank=8, full_nl=False
         phi_k, psi_k = ref_crank[kref]
         moves.append((1, phi_k * 100000 + psi_k, d, dE, *terms))
     out["moves"] = np.array(moves, dtype=np.float64).reshape(-1, 8)
-    out["xyz"], out["q"], out["r"], out["eps"] = x, q, r, e
     out["ss_in"] = np.array(sysd["ss"], np.int32).reshape(-1, 2)
+    if not inputs:
+        out["fixture"] = np.array(fixture)
+        out["xyz_sha"] = np.array(sha(np.asarray(x, np.float64)))
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+        print(name, "atoms", x.shape[0], "pairs", int(out["nl_row_cnt"].sum()), "E", out["energy_topo"][4])
+        return
+    out["xyz"], out["q"], out["r"], out["eps"] = x, q, r, e
     meta = dict(resnames=list(sysd["resnames"]), atomnames=list(sysd["atomnames"]),
                 res_idx=[int(v) for v in sysd["res_idx"]])
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
@@ -165,7 +179,37 @@ def golden_system(name, sysd, R, pp, rng, n_torsion=24, n_crank=8, full_nl=False
     print(name, "atoms", x.shape[0], "pairs", len(cols), "E", out["energy_topo"][4])
 
 
+WORKLOAD_FIXTURES = {"wl_c2": "c2_chain_300res.npz", "wl_c4": "c4_globule_1000res.npz",
+                     "wl_c5": "c5_multidomain_4x1000res.npz"}
+
+
+def workload_goldens(R, pp, names=None):
+    """Goldens of the benchmark chains (workloads/*.npz, written by
+    workloads/make_workloads.py): the same reference outputs as for the
+    other systems, without a copy of the inputs (the tests read them from
+    the fixture) and with 16 torsion + 8 crankshaft replays."""
+    rng = np.random.default_rng(20261204)
+    for name, fname in WORKLOAD_FIXTURES.items():
+        if names and name not in names:
+            continue
+        path = os.path.join(ROOT, "workloads", fname)
+        if not os.path.exists(path):
+            print("skip", name, "(no", fname + ")")
+            continue
+        d = np.load(path, allow_pickle=False)
+        sysd = dict(xyz=d["xyz"].astype(np.float64), q=d["charge"], r=d["radius"], eps=d["epsilon"],
+                    resnames=[str(v) for v in d["resnames"]], atomnames=[str(v) for v in d["atomnames"]],
+                    res_idx=[int(v) for v in d["res_idx"]], ss=[])
+        golden_system(name, sysd, R, pp, rng, n_torsion=16, n_crank=8, inputs=False, fixture=fname)
+
+
 def main():
+    if len(sys.argv) > 1 and sys.argv[1] == "--workloads":
+        from oracle import RefEngine, ref_so_path
+        sys.path.insert(0, os.path.dirname(ref_so_path()))
+        import protein_physics as pp
+        workload_goldens(RefEngine(), pp, sys.argv[2:])
+        return
     ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("ALMA_REFERENCE", "")
     if not ref or not os.path.isdir(ref):
         sys.exit("usage: %s REFERENCE_TREE (or set ALMA_REFERENCE): the reference checkout" % sys.argv[0])

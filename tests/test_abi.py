@@ -103,3 +103,19 @@ def test_bench_host_threads_follows_omp_setting(monkeypatch):
     assert bench.host_threads() == 3
     monkeypatch.delenv("OMP_NUM_THREADS")
     assert bench.host_threads() >= 1
+
+
+def test_bench_reference_inputs_load_nothing_of_the_package():
+    """The reference arm builds its inputs with the chain generator loaded
+    by path: protein_physics_b200 (and its native library) stay unloaded,
+    and both arms describe the workload with the same config."""
+    import subprocess
+    import sys
+    code = ("import sys; sys.path.insert(0, %r); import bench; "
+            "chains, temps = bench.c3_inputs(0, n_chains=2); "
+            "assert not [m for m in sys.modules if m.startswith('protein_physics_b200')], sorted(sys.modules); "
+            "c = bench.config_of('batched', chains); assert c == bench.config_of('batched', chains); "
+            "assert c['chains'] == 2 and c['atoms'] == sum(len(x['xyz']) for x in chains); "
+            "assert len(temps) == 2 and abs(temps[0] - 280 * 0.0019872) < 1e-12; print('ok')" % ROOT)
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stderr[-2000:]
