@@ -79,12 +79,47 @@ __device__ __forceinline__ double m_sqrt(double x) { return sqrt(x); }
 __device__ __forceinline__ float m_abs(float x) { return fabsf(x); }
 __device__ __forceinline__ double m_abs(double x) { return fabs(x); }
 
+// Fast FP32 forms for the pair passes (the FP64 passes keep the exact
+// forms).  Error budget per call, relative: rsqrtf <= 2 ulp; __fdividef
+// <= 2 ulp (denominators here are far inside [2^-126, 2^126]); __expf
+// 2 + floor(1.16 |x|) ulp — 3 ulp for the Debye-Hückel factor (kappa r <=
+// 1.51 inside the cutoff) and for the GB factor wherever it is not
+// negligible against r^2.  Logarithms stay logf (the HCT log of L/U near 1
+// needs its relative accuracy) and so do expm1f / log1pf of the ΔE
+// differences.  Summed over ~10^6 pairs these stay well inside the 1e-6
+// relative bar on the total energy and the 1e-4 kcal/mol bar on ΔE.
+__device__ __forceinline__ float f_sqrt(float x) { return x > 0.0f ? x * rsqrtf(x) : 0.0f; }
+__device__ __forceinline__ double f_sqrt(double x) { return sqrt(x); }
+
 // One nonbonded pair: Debye-Hückel + GB + LJ 12-6 + smooth capped hard core.
-// r2 is the FP64 squared distance (rounded to R); q = qi*qj product; the
-// caller has already applied the exclusion and 12 Å tests.
+// r2d is the FP64 squared distance; q = qi*qj product; the caller has
+// already applied the exclusion and 12 Å tests.  FP32: the fast forms
+// above, and LJ + hard core in FP64 inside sigma (the steep terms).
 template <typename R>
-__device__ __forceinline__ R pair_energy(const DevParams &P, R r2, R qp, R sig, R eps_prod,
+__device__ __forceinline__ R pair_energy(const DevParams &P, double r2d, R qp, R sig, R eps_prod,
                                          R ai, R aj) {
+    if constexpr (sizeof(R) == 4) {
+        const float r2 = (float)r2d;
+        const float rinv = rsqrtf(r2), r = r2 * rinv;
+        const float edh = (float)P.coulomb_over_epsw * qp * rinv * __expf(-(float)P.kappa * r);
+        const float aa = ai * aj;
+        const float f2 = r2 + aa * __expf(-0.25f * __fdividef(r2, aa));
+        const float egb = (float)P.gb_coef * qp * rsqrtf(f2);
+        const double sig2 = (double)sig * (double)sig;
+        if (r2d < sig2) {
+            const double s2 = sig2 / r2d, s6 = s2 * s2 * s2;
+            double lj = 4.0 * sqrt((double)eps_prod) * (s6 * s6 - s6);
+            const double rc = (double)sig * P.hard_frac, rc2 = rc * rc;
+            if (r2d < rc2) {
+                const double t2 = rc2 / r2d, t6 = t2 * t2 * t2, x = t6 * t6 - 1.0;
+                lj += fmin(P.hard_scale * x * x, P.hard_cap);
+            }
+            return (float)((double)(edh + egb) + lj);
+        }
+        const float sr = sig * rinv, s2 = sr * sr, s6 = s2 * s2 * s2;
+        return edh + egb + 4.0f * f_sqrt(eps_prod) * (s6 * s6 - s6);
+    }
+    const R r2 = (R)r2d;
     const R r = m_sqrt(r2);
     const R edh = (R)P.coulomb_over_epsw * qp / r * m_exp(-(R)P.kappa * r);
     const R aa = ai * aj;
@@ -145,6 +180,24 @@ __device__ __forceinline__ double lj_hard(const DevParams &P, double r2, R sig, 
 template <typename R>
 __device__ __forceinline__ double pair_delta(const DevParams &P, double r2o, double r2n, R qp, R sig, R eps_prod,
                                              R aao, R aan, double sig64, double eps64) {
+    if constexpr (sizeof(R) == 4) {
+        const double d2 = r2n - r2o;
+        const float ro2 = (float)r2o, rn2 = (float)r2n;
+        const float rio = rsqrtf(ro2), rin = rsqrtf(rn2);
+        const float ro = ro2 * rio, rn = rn2 * rin;
+        const float dr = __fdividef((float)d2, ro + rn);
+        const float kap = (float)P.kappa;
+        const float gdo = (float)P.coulomb_over_epsw * qp * rio * __expf(-kap * ro);
+        const float ddh = gdo * expm1f(-kap * dr - log1pf(dr * rio));
+        const float xo = aao * __expf(-0.25f * __fdividef(ro2, aao));
+        const float xn = aan * __expf(-0.25f * __fdividef(rn2, aan));
+        const float fo2 = ro2 + xo, fn2 = rn2 + xn;
+        const float fo = fo2 * rsqrtf(fo2), fn = fn2 * rsqrtf(fn2);
+        const float num = (float)(-d2) + (xo - xn);
+        const float dgb = (float)P.gb_coef * qp * __fdividef(num, fo * fn * (fo + fn));
+        return (double)ddh + (double)dgb +
+               (lj_hard<float>(P, r2n, sig, eps_prod, sig64, eps64) - lj_hard<float>(P, r2o, sig, eps_prod, sig64, eps64));
+    }
     const double d2 = r2n - r2o;
     const R ro2 = (R)r2o, rn2 = (R)r2n;
     const R ro = m_sqrt(ro2), rn = m_sqrt(rn2);
@@ -163,6 +216,15 @@ __device__ __forceinline__ double pair_delta(const DevParams &P, double r2o, dou
 // HCT descreening integral of atom j (radius rj) on atom i (radius ri).
 template <typename R>
 __device__ __forceinline__ R hct_term(R r, R r2, R ri, R rj) {
+    if constexpr (sizeof(R) == 4) {
+        const float d = fabsf(r - rj);
+        const float L = d > ri ? d : ri;
+        const float U = r + rj;
+        if (ri >= U) return 0.0f;
+        const float rU = __fdividef(1.0f, U);
+        return __fdividef(1.0f, L) - rU +
+               (r2 - rj * rj + ri * ri) * __fdividef(0.25f, r2 * ri * ri) * logf(L * rU);
+    }
     const R d = m_abs(r - rj);
     const R L = d > ri ? d : ri;
     const R U = r + rj;
@@ -199,6 +261,55 @@ __device__ __forceinline__ double warp_max(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
     return v;
+}
+
+// ---------------------------------------------------------------------------
+// SASA cap recurrence (physics_engine.cpp:2068-2083) over a 32-entry chunk
+// of a row: sa -= min(0.85 sa, c_l) for every lane l set in `hits`, in lane
+// (= row) order.  The hit values are first packed into lanes 0..n-1 (one
+// shuffle from the position of each lane's set bit), then read back by
+// index in groups of four: those shuffles do not depend on sa, so they
+// issue ahead of the dependent FP64 chain instead of one round trip per
+// entry.  The arithmetic and its order are those of the entry-by-entry
+// loop, so the result is the same to the bit.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double sasa_pack(unsigned hits, double c, int lane) {
+    const int src = lane < __popc(hits) ? (int)__fns(hits, 0, lane + 1) : lane;
+    return __shfl_sync(0xffffffffu, c, src);
+}
+
+__device__ __forceinline__ double sasa_step(double sa, double c) { return sa - fmin(sa * 0.85, c); }
+
+__device__ __forceinline__ double sasa_chunk(double sa, unsigned hits, double c, int lane) {
+    const int n = __popc(hits);
+    if (n == 0) return sa;
+    const double packed = sasa_pack(hits, c, lane);
+    int k = 0;
+    for (; k + 4 <= n; k += 4) {
+        const double c0 = __shfl_sync(0xffffffffu, packed, k), c1 = __shfl_sync(0xffffffffu, packed, k + 1);
+        const double c2 = __shfl_sync(0xffffffffu, packed, k + 2), c3 = __shfl_sync(0xffffffffu, packed, k + 3);
+        sa = sasa_step(sasa_step(sasa_step(sasa_step(sa, c0), c1), c2), c3);
+    }
+    for (; k < n; ++k) sa = sasa_step(sa, __shfl_sync(0xffffffffu, packed, k));
+    return sa;
+}
+
+// Two independent recurrences (old and new geometry) over the same chunk,
+// interleaved.
+__device__ __forceinline__ void sasa_chunk2(double &sa_a, unsigned hits_a, double c_a, double &sa_b,
+                                            unsigned hits_b, double c_b, int lane) {
+    const int na = __popc(hits_a), nb = __popc(hits_b);
+    const double pa = sasa_pack(hits_a, c_a, lane), pb = sasa_pack(hits_b, c_b, lane);
+    const int n = na < nb ? na : nb;
+    int k = 0;
+    for (; k + 2 <= n; k += 2) {
+        const double a0 = __shfl_sync(0xffffffffu, pa, k), a1 = __shfl_sync(0xffffffffu, pa, k + 1);
+        const double b0 = __shfl_sync(0xffffffffu, pb, k), b1 = __shfl_sync(0xffffffffu, pb, k + 1);
+        sa_a = sasa_step(sasa_step(sa_a, a0), a1);
+        sa_b = sasa_step(sasa_step(sa_b, b0), b1);
+    }
+    for (int q = k; q < na; ++q) sa_a = sasa_step(sa_a, __shfl_sync(0xffffffffu, pa, q));
+    for (int q = k; q < nb; ++q) sa_b = sasa_step(sa_b, __shfl_sync(0xffffffffu, pb, q));
 }
 
 // Block-wide sum; every thread gets the result.  smem: >= 32 doubles.

@@ -35,7 +35,7 @@ __device__ __forceinline__ void born_atom(int i, int lane, const double *__restr
         load_prm<R>(prm, prm64, j, qj, rj, ej);
         const double r2d = d2_of(pi, ld_xyz(xyz, j));
         const R r2 = (R)r2d;
-        sum += (double)hct_term<R>(m_sqrt(r2), r2, ri, rj);
+        sum += (double)hct_term<R>(f_sqrt(r2), r2, ri, rj);
     }
     sum = warp_sum(sum);
     if (lane == 0) {
@@ -81,16 +81,10 @@ __device__ __forceinline__ void pair_sasa_atom(const DevParams &P, int i, int la
             if (!(use_excl && (ent & ALMA_EXCL_BIT)) && r2d <= P.pair_cut2) {
                 R qj, rj, ej;
                 load_prm<R>(prm, prm64, j, qj, rj, ej);
-                e += (double)pair_energy<R>(P, (R)r2d, qi * qj, ri + rj, ei * ej, ai, (R)born[j]);
+                e += (double)pair_energy<R>(P, r2d, qi * qj, ri + rj, ei * ej, ai, (R)born[j]);
             }
         }
-        unsigned m = __ballot_sync(0xffffffffu, hit);
-        while (m) {  // the order-dependent recurrence, entry by entry
-            const int l = __ffs(m) - 1;
-            m &= m - 1;
-            const double c = __shfl_sync(0xffffffffu, cap, l);
-            sa -= fmin(sa * 0.85, c);
-        }
+        sa = sasa_chunk(sa, __ballot_sync(0xffffffffu, hit), cap, lane);  // in row order
     }
     e = warp_sum(e);
     if (lane == 0) {

@@ -58,16 +58,32 @@ template <typename R>
 __device__ __forceinline__ void pair_grad(const DevParams &P, double r2d, R qp, R sig, R eps_prod, R ai, R aj,
                                           double sig64, double eps64, double &fr, double &dEdA) {
     const R r2 = (R)r2d;
-    const R r = m_sqrt(r2);
-    const R kap = (R)P.kappa;
-    const R edh = (R)P.coulomb_over_epsw * qp / r * m_exp(-kap * r);
-    const R f_dh = -edh * ((R)1 / r + kap) / r;
-    const R A = ai * aj;
-    const R D = m_exp(-r2 / ((R)4 * A));
-    const R f2 = r2 + A * D;
-    const R egb = (R)P.gb_coef * qp / m_sqrt(f2);
-    const R f_gb = -egb * ((R)2 - (R)0.5 * D) / ((R)2 * f2);
-    dEdA = (double)(-egb * D * ((R)1 + r2 / ((R)4 * A)) / ((R)2 * f2));
+    R f_dh, f_gb;
+    if constexpr (sizeof(R) == 4) {  // the fast FP32 forms of pair_energy (same error budget)
+        const float rinv = rsqrtf(r2), r = r2 * rinv;
+        const float kap = (float)P.kappa;
+        const float edh = (float)P.coulomb_over_epsw * qp * rinv * __expf(-kap * r);
+        f_dh = -edh * (rinv + kap) * rinv;
+        const float A = ai * aj;
+        const float r2_4A = 0.25f * __fdividef(r2, A);
+        const float D = __expf(-r2_4A);
+        const float f2 = r2 + A * D;
+        const float rf2 = __fdividef(1.0f, f2);
+        const float egb = (float)P.gb_coef * qp * rsqrtf(f2);
+        f_gb = -egb * (2.0f - 0.5f * D) * 0.5f * rf2;
+        dEdA = (double)(-egb * D * (1.0f + r2_4A) * 0.5f * rf2);
+    } else {
+        const R r = m_sqrt(r2);
+        const R kap = (R)P.kappa;
+        const R edh = (R)P.coulomb_over_epsw * qp / r * m_exp(-kap * r);
+        f_dh = -edh * ((R)1 / r + kap) / r;
+        const R A = ai * aj;
+        const R D = m_exp(-r2 / ((R)4 * A));
+        const R f2 = r2 + A * D;
+        const R egb = (R)P.gb_coef * qp / m_sqrt(f2);
+        f_gb = -egb * ((R)2 - (R)0.5 * D) / ((R)2 * f2);
+        dEdA = (double)(-egb * D * ((R)1 + r2 / ((R)4 * A)) / ((R)2 * f2));
+    }
     double f_lj;
     const double sig2 = sig64 * sig64;
     if (r2d < sig2) {  // steep: FP64 with FP64 sigma / epsilon
@@ -81,7 +97,10 @@ __device__ __forceinline__ void pair_grad(const DevParams &P, double r2d, R qp, 
     } else {
         const R s2 = (R)(sig2 / r2d);
         const R s6 = s2 * s2 * s2;
-        f_lj = (double)((R)4 * m_sqrt(eps_prod) * ((R)6 * s6 - (R)12 * s6 * s6) / r2);
+        if constexpr (sizeof(R) == 4)
+            f_lj = (double)(4.0f * f_sqrt(eps_prod) * (6.0f * s6 - 12.0f * s6 * s6) * __fdividef(1.0f, r2));
+        else
+            f_lj = (double)((R)4 * m_sqrt(eps_prod) * ((R)6 * s6 - (R)12 * s6 * s6) / r2);
     }
     fr = (double)f_dh + (double)f_gb + f_lj;
 }
@@ -92,6 +111,24 @@ template <typename R>
 __device__ __forceinline__ R hct_deriv(R r, R r2, R ri, R rj) {
     const R U = r + rj;
     if (ri >= U) return (R)0;
+    if constexpr (sizeof(R) == 4) {  // fast reciprocals, logf kept (see hct_term)
+        const float d = fabsf(r - rj);
+        float L, Lp;
+        if (d > ri) {
+            L = d;
+            Lp = r > rj ? 1.0f : -1.0f;
+        } else {
+            L = ri;
+            Lp = 0.0f;
+        }
+        const float rL = __fdividef(1.0f, L), rU = __fdividef(1.0f, U), rr = __fdividef(1.0f, r);
+        const float Pp = r2 - rj * rj + ri * ri;
+        const float Q = logf(L * rU);
+        const float rden = __fdividef(0.25f, ri * ri * r2);
+        const float T = Pp * Q * rden;
+        const float dT = (2.0f * r * Q + Pp * (Lp * rL - rU)) * rden - 2.0f * T * rr;
+        return -Lp * rL * rL + rU * rU + dT;
+    }
     const R d = m_abs(r - rj);
     R L, Lp;
     if (d > ri) {
@@ -191,11 +228,11 @@ __global__ void __launch_bounds__(256, 4) grad_sasa_kernel(DevParams P, int nato
                 cap = cap_scale * ((dc - r) / (2.0 * rsi));
             }
         }
-        unsigned m = __ballot_sync(0xffffffffu, hit);
-        while (m) {
-            const int l = __ffs(m) - 1;
-            m &= m - 1;
-            const double c = __shfl_sync(0xffffffffu, cap, l);
+        const unsigned m = __ballot_sync(0xffffffffu, hit);
+        const int n = __popc(m);
+        const double packed = sasa_pack(m, cap, lane);
+        for (int q = 0; q < n; ++q) {  // row order; the shuffles do not wait for sa
+            const double c = __shfl_sync(0xffffffffu, packed, q);
             if (c <= sa * 0.85) {
                 sa -= c;
             } else {
@@ -228,21 +265,24 @@ __global__ void __launch_bounds__(256, 4) grad_sasa_kernel(DevParams P, int nato
                 cap = cap_scale * ((dc - r) / (2.0 * rsi));
             }
         }
-        double coef = 0.0;
-        unsigned m = __ballot_sync(0xffffffffu, hit);
-        while (m) {
-            const int l = __ffs(m) - 1;
-            m &= m - 1;
-            const double c = __shfl_sync(0xffffffffu, cap, l);
+        // the recurrence over the packed hits: packed lane q holds the q-th
+        // hit; its cap-branch adjoint goes back to the hit's own lane
+        const unsigned m = __ballot_sync(0xffffffffu, hit);
+        const int n = __popc(m);
+        const double packed = sasa_pack(m, cap, lane);
+        double pcoef = 0.0;
+        for (int q = 0; q < n; ++q) {
+            const double c = __shfl_sync(0xffffffffu, packed, q);
             if (c <= sa * 0.85) {
                 sa -= c;
-                if (lane == l) coef = base * pow(0.15, (double)(n_frac - seen));
+                if (lane == q) pcoef = base * pow(0.15, (double)(n_frac - seen));
             } else {
                 sa -= sa * 0.85;
                 ++seen;
             }
         }
-        if (coef != 0.0) {
+        const double coef = __shfl_sync(0xffffffffu, pcoef, __popc(m & ((1u << lane) - 1u)));
+        if (hit && coef != 0.0) {
             const double s = coef / r;
             gx += s * dx;
             gy += s * dy;
@@ -360,7 +400,7 @@ __global__ void grad_born_kernel(int natoms, const int32_t *__restrict__ atom_of
         const double4 pj = ld_xyz(xyz, j);
         const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
         const R r2 = (R)(dx * dx + dy * dy + dz * dz);
-        const R r = m_sqrt(r2);
+        const R r = f_sqrt(r2);
         const double s = (ci * (double)hct_deriv<R>(r, r2, ri, rj) + cj * (double)hct_deriv<R>(r, r2, rj, ri)) /
                          (double)r;
         gx += s * dx;

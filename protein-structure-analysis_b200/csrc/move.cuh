@@ -440,15 +440,11 @@ __device__ __forceinline__ void sasa_row(const MoveCtx &C, int s, int k, bool sh
             const double rn = sqrt(d2_of(pin, pjn));
             if (rn < dc) { hn = true; cn = cs * ((dc - rn) / (2.0 * rsi)); }
         }
-        unsigned mo = __ballot_sync(0xffffffffu, ho), mn = __ballot_sync(0xffffffffu, hn);
-        while (mo | mn) {  // independent recurrences: interleaved
-            const int lo2 = mo ? __ffs(mo) - 1 : 0, ln2 = mn ? __ffs(mn) - 1 : 0;
-            const double c_o = __shfl_sync(0xffffffffu, co, lo2), c_n = __shfl_sync(0xffffffffu, cn, ln2);
-            if (mo) sao -= fmin(sao * 0.85, c_o);
-            if (mn) san -= fmin(san * 0.85, c_n);
-            mo &= mo - 1;
-            mn &= mn - 1;
-        }
+        const unsigned mo = __ballot_sync(0xffffffffu, ho), mn = __ballot_sync(0xffffffffu, hn);
+        if (cached)  // independent recurrences, in row order (interleaved when both run)
+            san = sasa_chunk(san, mn, cn, lane);
+        else
+            sasa_chunk2(sao, mo, co, san, mn, cn, lane);
     }
     if (lane == 0) {
         const double tn = C.P.gamma_sa * fmax(0.0, san);
@@ -589,7 +585,7 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
             prm_of<R>(b.prm, b.prm64, j, qj, rj, ej);
             const double r2d = d2_of(pm, pos_new_eager(b.xyz, w.xyz_new, w.group, j));
             const R r2 = (R)r2d;
-            sum += (double)hct_term<R>(m_sqrt(r2), r2, rm, rj);
+            sum += (double)hct_term<R>(f_sqrt(r2), r2, rm, rj);
         }
         sum = warp_sum(sum);
         if (lane == 0) {
@@ -692,9 +688,9 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
                 }
                 acc += pair_delta<R>(C.P, r2o, r2n, qp, sig, ep, amo * ajo, amn * ajn, sig64, eps64);
             } else if (ino) {
-                acc -= (double)pair_energy<R>(C.P, (R)r2o, qp, sig, ep, amo, ajo);
+                acc -= (double)pair_energy<R>(C.P, r2o, qp, sig, ep, amo, ajo);
             } else {
-                acc += (double)pair_energy<R>(C.P, (R)r2n, qp, sig, ep, amn, ajn);
+                acc += (double)pair_energy<R>(C.P, r2n, qp, sig, ep, amn, ajn);
             }
         };
         const unsigned below = (1u << lane) - 1u;
@@ -829,7 +825,7 @@ __device__ inline void move_finish(const MoveCtx &C, const MoveDesc &M, int s, i
                 R qj, rj, ej;
                 prm_of<R>(C.b.prm, C.b.prm64, j, qj, rj, ej);
                 const R r2 = (R)d2_of(pm, ld_xyz(w.xyz_new, j));
-                sum += (double)hct_term<R>(m_sqrt(r2), r2, rm, rj);
+                sum += (double)hct_term<R>(f_sqrt(r2), r2, rm, rj);
             }
             sum = warp_sum(sum);
             if (lane == 0) C.b.born[m] = 1.0 / fmax(1.0 / C.b.prm64[4 * (size_t)m + 1] - 0.5 * sum, 2.0);
