@@ -48,13 +48,18 @@ def build(force=False, verbose=False):
     os.makedirs(objdir, exist_ok=True)
     objs = []
     procs = []
+    headers = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(INCLUDE, "*.h"))
+    newest_header = max((os.path.getmtime(h) for h in headers), default=0.0)
     for src in sources():
         obj = os.path.join(objdir, os.path.basename(src) + ".o")
+        objs.append(obj)
+        # an object is rebuilt when its source or any header is newer than it
+        if not force and os.path.exists(obj) and os.path.getmtime(obj) > max(os.path.getmtime(src), newest_header):
+            continue
         cmd = [NVCC, *ARCH, *FLAGS, "-I" + INCLUDE, "-I" + CSRC, "-c", src, "-o", obj]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
         procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))
-        objs.append(obj)
     failed = []
     for src, p in procs:
         out, _ = p.communicate()

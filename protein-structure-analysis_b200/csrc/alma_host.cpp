@@ -105,14 +105,19 @@ int alma_topo_sides_compact(int32_t n, const int64_t *adj_ptr, const int32_t *ad
                             int64_t *ex_ptr, int32_t *ex_idx, int64_t ex_cap) {
     if (n < 0 || nb < 0 || !adj_ptr || (nb > 0 && (!bonds || !lo_out || !hi_out || !count || !ex_ptr)))
         return alma_set_error(ALMA_EINVAL, "alma_topo_sides_compact: bad arguments");
+    // The side's atoms are marked in `stamp` by the walk; its sorted order,
+    // its longest run of consecutive indices and the remainder all come
+    // from one scan of the marks over [min, max] (no sort: for a residue-
+    // ordered chain that span is the side itself).
     std::vector<uint32_t> stamp((size_t)n, 0u);
-    std::vector<int32_t> stk, side;
+    std::vector<int32_t> stk;
     int64_t k = 0;
     ex_ptr[0] = 0;
     for (int32_t b = 0; b < nb; ++b) {
         const int32_t bi = bonds[2 * b], bj = bonds[2 * b + 1];
         const uint32_t mark = (uint32_t)b + 1u;
-        side.clear();
+        int64_t cnt = 0;
+        int32_t mn = n, mx = -1;
         if (bi >= 0 && bi < n && bj >= 0 && bj < n) {
             stamp[(size_t)bi] = mark;
             stk.clear();
@@ -122,30 +127,35 @@ int alma_topo_sides_compact(int32_t n, const int64_t *adj_ptr, const int32_t *ad
                 stk.pop_back();
                 if (stamp[(size_t)cur] == mark) continue;
                 stamp[(size_t)cur] = mark;
-                side.push_back(cur);
+                ++cnt;
+                mn = std::min(mn, cur);
+                mx = std::max(mx, cur);
                 for (int64_t e = adj_ptr[cur]; e < adj_ptr[cur + 1]; ++e) stk.push_back(adj_idx[e]);
             }
+            // the axis atom i carries the mark too but is not on the side
+            stamp[(size_t)bi] = 0u;
         }
-        std::sort(side.begin(), side.end());
-        // longest run of consecutive indices
-        size_t best_b = 0, best_len = 0;
-        for (size_t s0 = 0; s0 < side.size();) {
-            size_t s1 = s0 + 1;
-            while (s1 < side.size() && side[s1] == side[s1 - 1] + 1) ++s1;
-            if (s1 - s0 > best_len) { best_len = s1 - s0; best_b = s0; }
-            s0 = s1;
+        // longest run of consecutive marked indices (first one on ties)
+        int32_t best_lo = 0, best_len = 0;
+        for (int32_t a = mn; a <= mx;) {
+            if (stamp[(size_t)a] != mark) { ++a; continue; }
+            int32_t e = a + 1;
+            while (e <= mx && stamp[(size_t)e] == mark) ++e;
+            if (e - a > best_len) { best_len = e - a; best_lo = a; }
+            a = e;
         }
-        count[b] = (int64_t)side.size();
+        count[b] = cnt;
         if (best_len >= 2) {
-            lo_out[b] = side[best_b];
-            hi_out[b] = side[best_b] + (int32_t)best_len;
+            lo_out[b] = best_lo;
+            hi_out[b] = best_lo + best_len;
         } else {
             lo_out[b] = hi_out[b] = 0;
             best_len = 0;
         }
-        for (size_t s0 = 0; s0 < side.size(); ++s0) {
-            if (best_len && s0 >= best_b && s0 < best_b + best_len) continue;
-            if (k < ex_cap && ex_idx) ex_idx[k] = side[s0];
+        for (int32_t a = mn; a <= mx; ++a) {
+            if (stamp[(size_t)a] != mark) continue;
+            if (best_len && a >= best_lo && a < best_lo + best_len) continue;
+            if (k < ex_cap && ex_idx) ex_idx[k] = a;
             ++k;
         }
         ex_ptr[b + 1] = k;

@@ -27,9 +27,8 @@ _CACHE = {}
 
 
 def _golden(name):
-    if name not in _CACHE:
+    if name not in _CACHE:  # the topology of the 65k-atom chain takes a while to build: once
         g = Golden(name)
-        _CACHE.clear()  # one chain held at a time (the largest is 65k atoms)
         _CACHE[name] = (g, g.topology())
     return _CACHE[name]
 
