@@ -883,7 +883,8 @@ def run_profile_case(args):
     proposals per chain.  "forces": the single chain, one energy evaluation
     and one alma_forces call (4 gradient kernels).  "energy": the first 48
     chains of the batched workload, one neighbor-list build, one full energy
-    evaluation and one gradient (alma_forces)."""
+    evaluation and one gradient (alma_forces).  The measured part sits
+    between cudaProfilerStart/Stop (ncu --profile-from-start off)."""
     import torch
     sys.path.insert(0, PKG)
     from protein_physics_b200.device import DeviceBatch
@@ -897,15 +898,21 @@ def run_profile_case(args):
                               spec_teams=1)
             runner.run(20)
             lim = int(runner.state()["step"].max()) + 20
+            torch.cuda.synchronize()
+            torch.cuda.profiler.start()  # ncu --profile-from-start off: only this launch
             runner.launch(lim)
             torch.cuda.synchronize()
+            torch.cuda.profiler.stop()
             print(json.dumps({"profile_case": "mc-batched", "systems": len(chains), "atoms": batch.natoms,
                               "proposals": int(runner.state()["step"].sum())}))
             return
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
         batch.build_nl()
         terms = batch.energy_terms()
         batch.forces()
         torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
         print(json.dumps({"profile_case": "energy", "systems": len(chains), "atoms": batch.natoms,
                           "half_entries": int(batch.half_len.sum()), "full_entries": int(batch.full_len.sum()),
                           "total_energy": float(terms[:, 4].sum())}))
@@ -926,8 +933,11 @@ def run_profile_case(args):
                       threads=nt, spec_teams=k)
     runner.run(100)
     lim = int(runner.state()["step"].max()) + 200
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
     runner.launch(lim)
     torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
     st = runner.state()
     print(json.dumps({"profile_case": "single chain", "atoms": batch.natoms, "steps_done": int(st["step"][0]),
                       "cluster": cl, "threads": nt, "spec_teams": k}))

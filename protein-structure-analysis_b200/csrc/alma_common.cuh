@@ -94,10 +94,12 @@ __device__ __forceinline__ double f_sqrt(double x) { return sqrt(x); }
 // One nonbonded pair: Debye-Hückel + GB + LJ 12-6 + smooth capped hard core.
 // r2d is the FP64 squared distance; q = qi*qj product; the caller has
 // already applied the exclusion and 12 Å tests.  FP32: the fast forms
-// above, and LJ + hard core in FP64 inside sigma (the steep terms).
+// above, and LJ + hard core in FP64 with the FP64 sigma / epsilon product
+// (sig64, eps64) inside sigma (the steep terms: a clash's r^-12 would
+// amplify the FP32 rounding of sigma twelvefold).
 template <typename R>
 __device__ __forceinline__ R pair_energy(const DevParams &P, double r2d, R qp, R sig, R eps_prod,
-                                         R ai, R aj) {
+                                         R ai, R aj, double sig64, double eps64) {
     if constexpr (sizeof(R) == 4) {
         const float r2 = (float)r2d;
         const float rinv = rsqrtf(r2), r = r2 * rinv;
@@ -105,11 +107,11 @@ __device__ __forceinline__ R pair_energy(const DevParams &P, double r2d, R qp, R
         const float aa = ai * aj;
         const float f2 = r2 + aa * __expf(-0.25f * __fdividef(r2, aa));
         const float egb = (float)P.gb_coef * qp * rsqrtf(f2);
-        const double sig2 = (double)sig * (double)sig;
+        const double sig2 = sig64 * sig64;
         if (r2d < sig2) {
             const double s2 = sig2 / r2d, s6 = s2 * s2 * s2;
-            double lj = 4.0 * sqrt((double)eps_prod) * (s6 * s6 - s6);
-            const double rc = (double)sig * P.hard_frac, rc2 = rc * rc;
+            double lj = 4.0 * sqrt(eps64) * (s6 * s6 - s6);
+            const double rc = sig64 * P.hard_frac, rc2 = rc * rc;
             if (r2d < rc2) {
                 const double t2 = rc2 / r2d, t6 = t2 * t2 * t2, x = t6 * t6 - 1.0;
                 lj += fmin(P.hard_scale * x * x, P.hard_cap);

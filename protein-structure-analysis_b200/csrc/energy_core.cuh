@@ -59,7 +59,8 @@ __device__ __forceinline__ void pair_sasa_atom(const DevParams &P, int i, int la
     load_prm<R>(prm, prm64, i, qi, ri, ei);
     const R ai = (R)born[i];
     const double4 pi = ld_xyz(xyz, i);
-    const double rsi = prm64[4 * (size_t)i + 1] + P.probe_r;
+    const double ri64 = prm64[4 * (size_t)i + 1], ei64 = prm64[4 * (size_t)i + 2];
+    const double rsi = ri64 + P.probe_r;
     const double cap_scale = 2.0 * 3.14159265358979323846 * rsi * rsi;
     double sa = 4.0 * 3.14159265358979323846 * rsi * rsi;
     double e = 0.0;
@@ -72,7 +73,8 @@ __device__ __forceinline__ void pair_sasa_atom(const DevParams &P, int i, int la
             const uint32_t ent = half_cols[k];
             const int j = (int)(ent & ALMA_IDX_MASK);
             const double r2d = d2_of(pi, ld_xyz(xyz, j));
-            const double rsj = prm64[4 * (size_t)j + 1] + P.probe_r;
+            const double4 pj64 = *reinterpret_cast<const double4 *>(prm64 + 4 * (size_t)j);
+            const double rsj = pj64.y + P.probe_r;
             const double r = sqrt(r2d), dc = rsi + rsj;
             if (r < dc) {
                 hit = true;
@@ -81,7 +83,8 @@ __device__ __forceinline__ void pair_sasa_atom(const DevParams &P, int i, int la
             if (!(use_excl && (ent & ALMA_EXCL_BIT)) && r2d <= P.pair_cut2) {
                 R qj, rj, ej;
                 load_prm<R>(prm, prm64, j, qj, rj, ej);
-                e += (double)pair_energy<R>(P, r2d, qi * qj, ri + rj, ei * ej, ai, (R)born[j]);
+                e += (double)pair_energy<R>(P, r2d, qi * qj, ri + rj, ei * ej, ai, (R)born[j], ri64 + pj64.y,
+                                            ei64 * pj64.z);
             }
         }
         sa = sasa_chunk(sa, __ballot_sync(0xffffffffu, hit), cap, lane);  // in row order

@@ -678,19 +678,19 @@ __device__ MoveResult move_eval(const MoveCtx &C, const MoveDesc &M, int s, doub
             const R qp = qm * qj, sig = rm + rj, ep = em * ej;
             const R ajo = (R)b.born[j];
             const R ajn = gj ? (R)born_new_of(w, b.prm64, j, wph) : ajo;
+            // FP64 sigma/epsilon only for contacts inside sigma (steep LJ)
+            double sig64 = (double)sig, eps64 = (double)ep;
+            if (fmin(ino ? r2o : r2n, inn ? r2n : r2o) < 1.0001 * sig64 * sig64) {
+                const double4 pj64 = *reinterpret_cast<const double4 *>(b.prm64 + 4 * (size_t)j);
+                sig64 = rm64 + pj64.y;
+                eps64 = em64 * pj64.z;
+            }
             if (ino && inn) {
-                // FP64 sigma/epsilon only for contacts inside sigma (steep LJ)
-                double sig64 = (double)sig, eps64 = (double)ep;
-                if (fmin(r2o, r2n) < 1.0001 * sig64 * sig64) {
-                    const double4 pj64 = *reinterpret_cast<const double4 *>(b.prm64 + 4 * (size_t)j);
-                    sig64 = rm64 + pj64.y;
-                    eps64 = em64 * pj64.z;
-                }
                 acc += pair_delta<R>(C.P, r2o, r2n, qp, sig, ep, amo * ajo, amn * ajn, sig64, eps64);
             } else if (ino) {
-                acc -= (double)pair_energy<R>(C.P, r2o, qp, sig, ep, amo, ajo);
+                acc -= (double)pair_energy<R>(C.P, r2o, qp, sig, ep, amo, ajo, sig64, eps64);
             } else {
-                acc += (double)pair_energy<R>(C.P, r2n, qp, sig, ep, amn, ajn);
+                acc += (double)pair_energy<R>(C.P, r2n, qp, sig, ep, amn, ajn, sig64, eps64);
             }
         };
         const unsigned below = (1u << lane) - 1u;

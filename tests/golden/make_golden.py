@@ -130,7 +130,8 @@ def topo_record(pp, sysd):
         ss=np.array(list(T.disulfide_pairs), np.int32).reshape(-1, 2))
 
 
-def golden_system(name, sysd, R, pp, rng, n_torsion=24, n_crank=8, full_nl=False, inputs=True, fixture=None):
+def golden_system(name, sysd, R, pp, rng, n_torsion=24, n_crank=8, full_nl=False, inputs=True, fixture=None,
+                  n_policy=0):
     from oracle import RefEngine  # noqa: F401
     out = {}
     T, trec = topo_record(pp, sysd)
@@ -153,6 +154,14 @@ def golden_system(name, sysd, R, pp, rng, n_torsion=24, n_crank=8, full_nl=False
     for _ in range(n_torsion):
         k = int(rng.integers(0, nrb))
         d = float(rng.uniform(-0.5236, 0.5236))
+        dE, terms, _, _ = R.move_dE(x, q, r, e, rt, 0, k, d)
+        moves.append((0, k, d, dE, *terms))
+    # moves of the size the samplers propose (generate_ensemble's first
+    # max_angle, 0.12 rad, x the lever scale, x2.5 for sidechain bonds)
+    for _ in range(n_policy):
+        k = int(rng.integers(0, nrb))
+        lim = 0.12 * float(trec["rot_bond_scale"][k]) * (2.5 if int(trec["rb"][k, 2]) == 2 else 1.0)
+        d = float(rng.uniform(-lim, lim))
         dE, terms, _, _ = R.move_dE(x, q, r, e, rt, 0, k, d)
         moves.append((0, k, d, dE, *terms))
     for _ in range(n_crank if ncp else 0):
@@ -187,7 +196,8 @@ def workload_goldens(R, pp, names=None):
     """Goldens of the benchmark chains (workloads/*.npz, written by
     workloads/make_workloads.py): the same reference outputs as for the
     other systems, without a copy of the inputs (the tests read them from
-    the fixture) and with 16 torsion + 8 crankshaft replays."""
+    the fixture) and with 16 torsion moves of up to 30 degrees, 16 of the
+    samplers' own size and 8 crankshaft replays."""
     rng = np.random.default_rng(20261204)
     for name, fname in WORKLOAD_FIXTURES.items():
         if names and name not in names:
@@ -200,7 +210,7 @@ def workload_goldens(R, pp, names=None):
         sysd = dict(xyz=d["xyz"].astype(np.float64), q=d["charge"], r=d["radius"], eps=d["epsilon"],
                     resnames=[str(v) for v in d["resnames"]], atomnames=[str(v) for v in d["atomnames"]],
                     res_idx=[int(v) for v in d["res_idx"]], ss=[])
-        golden_system(name, sysd, R, pp, rng, n_torsion=16, n_crank=8, inputs=False, fixture=fname)
+        golden_system(name, sysd, R, pp, rng, n_torsion=16, n_crank=8, inputs=False, fixture=fname, n_policy=16)
 
 
 def main():

@@ -10,8 +10,14 @@ Bars, as on the smaller goldens:
   * Born radii: 1e-12 (FP64) / 2e-6 (mixed) relative;
   * total energy with and without topology: 1e-10 (FP64) / 1e-6 (mixed)
     relative; SASA, dihedral and disulfide terms 1e-10 (FP64 always);
-  * ΔE of 16 torsion + 8 crankshaft moves replayed by the reference:
-    1e-7 kcal/mol (FP64) / 1e-4 kcal/mol + 1e-14 x sum|terms| (mixed).
+  * ΔE of 16 torsion moves of up to 30 degrees, 16 of the samplers' own
+    size (0.12 rad x lever scale) and 8 crankshaft moves, replayed by the
+    reference: FP64 1e-7 kcal/mol + 1e-11 relative (the reference sums the
+    before and after cross energies separately, with -ffast-math); mixed
+    1e-4 kcal/mol + 1e-14 x sum|terms| for |ΔE| <= 1e3 kcal/mol, and 1e-6
+    relative above — turning half of a compact chain by 30 degrees drives
+    atoms through each other (ΔE up to ~1e21 kcal/mol), a move the
+    Metropolis test rejects at any temperature whatever its last digits.
 """
 import hashlib
 
@@ -82,7 +88,9 @@ def test_move_dE_matches_reference(name, precision):
         dE, dterms = b.move_dE([k], [a], [[delta, 0.0]])
         dE = float(dE[0].item())
         if precision == "fp64":
-            assert dE == pytest.approx(dE_ref, abs=1e-7 + 1e-12 * abs(dE_ref))
-        else:
+            assert abs(dE - dE_ref) <= 1e-7 + 1e-11 * abs(dE_ref), (kind, code, dE, dE_ref)
+        elif abs(dE_ref) <= 1e3:
             assert abs(dE - dE_ref) <= 1e-4 + 1e-14 * np.sum(np.abs(terms_ref)), (kind, code, dE, dE_ref)
+        else:
+            assert abs(dE - dE_ref) <= 1e-6 * abs(dE_ref), (kind, code, dE, dE_ref)
         np.testing.assert_allclose(dterms[0].cpu().numpy()[1:], terms_ref[1:], atol=1e-8, rtol=1e-11)
