@@ -404,6 +404,13 @@ typedef struct {
                                   /* list, Born radii and energy inside the   */
                                   /* persistent kernel (one team); NULL: it   */
                                   /* stops for the host rebuild                */
+    const int32_t *sys_order;     /* optional [nsys] device permutation: the  */
+                                  /* order in which systems take CTAs (the   */
+                                  /* hardware starts CTAs in index order, so */
+                                  /* largest-first packs uneven chains onto  */
+                                  /* the SMs with the shortest tail); NULL:  */
+                                  /* system s on CTA s.  Results do not      */
+                                  /* depend on it.                           */
 } AlmaMCConfig;
 
 /* Per-system chain state, device memory, one per system (72 bytes). */
@@ -455,6 +462,14 @@ int alma_mc_after_rebuild(AlmaChainState *states, const double *terms, const uin
 int alma_replica_exchange(int32_t nsys, const double *terms, AlmaChainState *mc_states, AlmaMalaState *mala_states,
                           int32_t *sys_of_temp, uint64_t seed, int64_t round, unsigned long long *attempts,
                           unsigned long long *accepts, void *stream);
+
+/* Size in bytes of each ABI struct, for bindings that mirror them (ctypes,
+ * cgo, JNA) to check their layout against the library's: which = 0
+ * AlmaParams, 1 AlmaBatch, 2 AlmaTopo, 3 AlmaNL, 4 AlmaMCConfig,
+ * 5 AlmaChainState, 6 AlmaTorsionTree, 7 AlmaMalaState, 8 AlmaMalaConfig;
+ * 0 for any other value.  No counterpart in the reference (its binding is
+ * pybind11, which checks types at compile time). */
+size_t alma_struct_size(int32_t which);
 
 #ifdef __cplusplus
 }

@@ -228,3 +228,18 @@ int alma_torsion_tree(int32_t natoms, int32_t nrb, const int32_t *rb_ij, const i
 }
 
 }  // extern "C"
+
+extern "C" size_t alma_struct_size(int32_t which) {
+    switch (which) {
+        case 0: return sizeof(AlmaParams);
+        case 1: return sizeof(AlmaBatch);
+        case 2: return sizeof(AlmaTopo);
+        case 3: return sizeof(AlmaNL);
+        case 4: return sizeof(AlmaMCConfig);
+        case 5: return sizeof(AlmaChainState);
+        case 6: return sizeof(AlmaTorsionTree);
+        case 7: return sizeof(AlmaMalaState);
+        case 8: return sizeof(AlmaMalaConfig);
+        default: return 0;
+    }
+}

@@ -60,6 +60,7 @@ struct MCConfigDev {
     double target_lo, target_hi, scale_up, scale_down, angle_max, angle_min;
     double sidechain_mult, crank_prob, concerted_prob, fixed_delta;
     const int32_t *moveset_off, *moveset;
+    const int32_t *sys_order;  // CTA (team) -> system, or nullptr: identity
     RebuildWS rw;         // rw.ccount == nullptr: no in-kernel rebuild
     double reach_pad;     // short-row reach padding of the list build
 };
@@ -361,7 +362,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) mc_kernel(MoveCtx C, MCConfigDev
     __shared__ double rsm[192], rpart[8];
     __shared__ int64_t ssm[33];
     const Team<CL> T;
-    const int s = blockIdx.x / CL;
+    const int s = cfg.sys_order ? cfg.sys_order[blockIdx.x / CL] : (int)(blockIdx.x / CL);
     if (threadIdx.x == 0) S = states[s];
     __syncthreads();
     bool rows_ok = system_within_skin(C, s);
@@ -567,7 +568,7 @@ mc_spec_kernel(MoveCtx C, MCConfigDev cfg, AlmaChainState *__restrict__ states, 
     __shared__ int did_move, acc_sh, a_sh, abort_sh;
     const Team<CL> T;
     const int grp = blockIdx.x / CL;
-    const int s = grp / teams, q = grp % teams;
+    const int s = cfg.sys_order ? cfg.sys_order[grp / teams] : grp / teams, q = grp % teams;
     MoveCtx Cq = C;
     Cq.w = scratch_at(C.w, (size_t)q * team_stride);
     SpecRound *Rd = rounds + s;
@@ -794,6 +795,7 @@ extern "C" int alma_mc_run(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *
     d.fixed_delta = cfg->fixed_delta;
     d.moveset_off = cfg->moveset_off;
     d.moveset = cfg->moveset;
+    d.sys_order = cfg->sys_order;
     d.reach_pad = 2.0 * p->probe_r + 2.0 * sqrt(p->half_skin2) + 1e-6;  // as alma_nl_build
     d.rw = carve_rebuild(cfg->rebuild_ws, b->natoms, b->nsys);
     cudaStream_t st = (cudaStream_t)stream;

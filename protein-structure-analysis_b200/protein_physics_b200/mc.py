@@ -46,6 +46,7 @@ def mc_config(seed, policy=0, tune_freq=200, max_angle_bounds=(0.004, 0.5), fixe
     cfg.moveset_off = cfg.moveset = None
     cfg.threads_per_system = 0
     cfg.cluster_size = 1
+    cfg.sys_order = None
     if moveset is not None:
         off = np.zeros(nsys + 1, np.int32)
         off[1:] = np.cumsum([len(m) for m in moveset])
@@ -105,6 +106,12 @@ class MCRunner:
             need = self.L.alma_mc_scratch_bytes(batch.natoms, batch.nsys, int(spec_teams))
             if batch.scratch.numel() < need:
                 batch.scratch = torch.zeros(need, dtype=torch.uint8, device="cuda")
+        # largest systems take the first CTAs: when a batch has more systems
+        # than resident CTAs, the long chains start first and the short ones
+        # fill the SMs they free (the tail of the launch shortens)
+        order = np.argsort(-np.diff(batch.atom_off_h), kind="stable").astype(np.int32)
+        self._order = _t(order, torch.int32)
+        self.cfg.sys_order = _ptr(self._order)
         T = np.broadcast_to(np.asarray(temperatures, np.float64), (batch.nsys,)).copy()
         if np.any(T <= 0):
             raise ValueError("temperature must be positive")

@@ -119,3 +119,18 @@ def test_bench_reference_inputs_load_nothing_of_the_package():
             "assert len(temps) == 2 and abs(temps[0] - 280 * 0.0019872) < 1e-12; print('ok')" % ROOT)
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stderr[-2000:]
+
+
+def test_ctypes_structs_match_the_library_layout():
+    """Every struct the Python binding mirrors has the size the library
+    was compiled with (alma_struct_size): a field added on one side only
+    would shift every later field."""
+    from protein_physics_b200 import _lib
+    L = _lib.lib()
+    L.alma_struct_size.restype = ctypes.c_size_t
+    L.alma_struct_size.argtypes = [ctypes.c_int32]
+    mirrors = [_lib.AlmaParams, _lib.AlmaBatch, _lib.AlmaTopo, _lib.AlmaNL, _lib.AlmaMCConfig, _lib.AlmaChainState,
+               _lib.AlmaTorsionTree, _lib.AlmaMalaState, _lib.AlmaMalaConfig]
+    for which, cls in enumerate(mirrors):
+        assert L.alma_struct_size(which) == ctypes.sizeof(cls), cls.__name__
+    assert L.alma_struct_size(99) == 0
