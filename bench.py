@@ -51,6 +51,10 @@ FP32_PEAK_NOMINAL = 148 * 128 * 2 * 1.965e9  # ops/s: SMs x FP32 lanes x FMA x m
 OPS_PAIR, OPS_HCT, OPS_SASA = 47.0, 21.0, 11.0  # algorithmic ops per unit (FP32 + MUFU)
 C3_CHAINS, C3_PER_STEP, C2_PER_STEP = 256, 100, 1000
 L2_NOTE = "inputs larger than L2 (lists of 1.36 M atoms) and a 256 MiB L2 flush between GPU steps"
+# DRAM bytes (read + write) per proposal of the MC kernel, from one ncu capture
+# of a smaller case of the same workload, scaled by the proposals of a launch:
+# profiles/mc_kernel_batched_48_chains.md (200.5 MB / 288 proposals)
+DRAM_BYTES_PER_PROPOSAL = {"batched": 200.5e6 / 288}
 
 
 def rank_info():
@@ -240,7 +244,7 @@ def _timed_mc(runner, batch, args, per_step, full_energy, world, local, flush):
                 rebuilds=runner.rebuilds - rebuild0, clocks=sampler.summary())
 
 
-def _kernel_roofline(runner, batch, tuned, proposals_per_launch):
+def _kernel_roofline(runner, batch, tuned, proposals_per_launch, workload=None):
     """One extra MC launch alone (no host rebuild step), timed with events
     on its stream; algorithmic ops from the kernel's own work counters."""
     import numpy as np
@@ -262,13 +266,19 @@ def _kernel_roofline(runner, batch, tuned, proposals_per_launch):
     achieved = ops / (k_ms * 1e-3)
     name = ("mc_spec_kernel<float,%d,%d> x %d teams" % (tuned[1], tuned[0], tuned[2]) if tuned[2] > 1 else
             "mc_kernel<float,%d,%d>" % (tuned[1] or 512, tuned[0]))
+    nprop = float(np.sum(st1["step"] - st0["step"]))
+    per = DRAM_BYTES_PER_PROPOSAL.get(workload)
+    traffic = per * nprop if per else None
     return {"bound": "fp32", "kernel": name, "achieved": achieved / 1e12, "peak": FP32_PEAK_NOMINAL / 1e12,
             "unit": "TOP/s (FP32+MUFU ops)", "frac": achieved / FP32_PEAK_NOMINAL,
             "peak_source": "nominal 148 SM x 128 FP32 lanes x 2 x 1965 MHz (no measured FP32 peak in "
                            "MEASURED_PEAKS.json; the kernel is neither HBM- nor tensor-bound)",
             "work_per_launch": {"pair_terms": float(d[0]), "hct": float(d[1]), "sasa_visits": float(d[2]),
-                                "moved_atoms": float(d[3]), "proposals": float(np.sum(st1["step"] - st0["step"]))},
-            "kernel_ms": k_ms, "traffic": None}
+                                "moved_atoms": float(d[3]), "proposals": nprop},
+            "kernel_ms": k_ms, "traffic": traffic,
+            "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum per proposal of a 48-chain capture "
+                               "(profiles/mc_kernel_batched_48_chains.md) x this launch's proposals; "
+                               "%.1f GB/s achieved" % (traffic / (k_ms * 1e-3) / 1e9)) if traffic else None}
 
 
 def run_ours(args, rank, world, local):
@@ -303,7 +313,7 @@ def run_ours(args, rank, world, local):
     t = _timed_mc(runner, batch, args, per_step, full_energy, world, local, flush)
     from protein_physics_b200.dist import reduce_timing
     ms_max, prop_total = reduce_timing(t["ms"], t["proposals"], device="cuda")
-    roof = _kernel_roofline(runner, batch, tuned, 200 if policy == 2 else 50)
+    roof = _kernel_roofline(runner, batch, tuned, 200 if policy == 2 else 50, args.workload)
     # e2e through the public API, host buffers in and out every step
     if args.workload == "batched":
         e2e = e2e_batched(systems, temps, tuned, args, world)
