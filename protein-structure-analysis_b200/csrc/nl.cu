@@ -15,6 +15,8 @@
 //   bin    : atom -> cell, cell histogram
 //   scan   : cell starts
 //   scatter: atoms into cells, then a per-cell rank sort (ascending index)
+//   cellpos: FP32 positions (relative to the grid origin) and R* in cell
+//            order, so the row scan streams its candidates coalesced
 //   rows   : warp per atom — one scan stages the row in shared memory,
 //            takes space from the system's cursors, writes the four rows
 //            ballot-compacted in scan order
@@ -36,6 +38,7 @@ struct NLWork {
     int32_t *cell_fill;   // [max_cells]
     int64_t *cell_start;  // [max_cells+1]
     int32_t *cell_atoms;  // [natoms]
+    float4 *cell_pos;     // [natoms] per cell slot: FP32 position relative to the grid origin, R*
     int32_t *sort_spill;  // [natoms] rank-sort space for oversized cells
     int64_t *tile_sums;   // scan scratch
     int64_t *total_cells; // [1]
@@ -62,6 +65,7 @@ static size_t carve(NLWork *w, char *base, int32_t nsys, int32_t natoms, int64_t
     t.cell_fill = (int32_t *)take(sizeof(int32_t) * (size_t)max_cells);
     t.cell_start = (int64_t *)take(sizeof(int64_t) * (size_t)(max_cells + 1));
     t.cell_atoms = (int32_t *)take(sizeof(int32_t) * (size_t)natoms);
+    t.cell_pos = (float4 *)take(sizeof(float4) * (size_t)natoms);
     t.sort_spill = (int32_t *)take(sizeof(int32_t) * (size_t)natoms);
     t.tile_sums = (int64_t *)take(sizeof(int64_t) * (size_t)ntiles);
     t.total_cells = (int64_t *)take(sizeof(int64_t));
@@ -193,6 +197,28 @@ __global__ void nl_cellsort_kernel(const int64_t *__restrict__ total_cells, cons
     }
 }
 
+// Cell-ordered copy of the candidates' positions for the row scan: slot k
+// of cell_atoms gets its atom's position relative to its system's grid
+// origin in FP32 and its R* (the SASA-reach radius).  The 27-cell scan then
+// reads each 32-candidate chunk as one coalesced 512-byte load instead of
+// 32 scattered FP64 gathers; FP64 decides only inside the margin.
+__global__ void nl_cellpos_kernel(const int32_t *__restrict__ atom_off, int nsys, int natoms,
+                                  const int64_t *__restrict__ total_cells, const int32_t *__restrict__ ok,
+                                  const int64_t *__restrict__ cell_start, const int32_t *__restrict__ cell_atoms,
+                                  const SysGrid *__restrict__ grid, const double *__restrict__ xyz,
+                                  const double *__restrict__ prm64, float4 *__restrict__ cell_pos) {
+    if (!*ok) return;
+    const int64_t used = cell_start[*total_cells];
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < used && k < natoms;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const int j = cell_atoms[k];
+        const SysGrid g = grid[sys_of_atom(atom_off, nsys, j)];
+        const double4 p = ld_xyz(xyz, j);
+        cell_pos[k] = make_float4((float)(p.x - g.xlo), (float)(p.y - g.ylo), (float)(p.z - g.zlo),
+                                  prm64 ? (float)prm64[4 * (size_t)j + 1] : 0.0f);
+    }
+}
+
 // Entries of one row staged per warp in shared memory by the one-pass
 // build (48 KB per 8-warp block); a longer row is scanned a second time.
 constexpr int NL_STAGE = 1536;
@@ -213,8 +239,9 @@ nl_rows_onepass_kernel(const int32_t *__restrict__ atom_off, int nsys, int natom
                        const double *__restrict__ xyz, double rcut2, const SysGrid *__restrict__ grid,
                        const int32_t *__restrict__ ok, const int32_t *__restrict__ cell_of,
                        const int64_t *__restrict__ cell_start, const int32_t *__restrict__ cell_atoms,
-                       const double *__restrict__ prm64, double reach_pad, const int64_t *__restrict__ excl_ptr,
-                       const int32_t *__restrict__ excl_cols, AlmaNL nl, int64_t *__restrict__ cursor) {
+                       const float4 *__restrict__ cell_pos, const double *__restrict__ prm64, double reach_pad,
+                       const int64_t *__restrict__ excl_ptr, const int32_t *__restrict__ excl_cols, AlmaNL nl,
+                       int64_t *__restrict__ cursor) {
     extern __shared__ uint32_t nl_stage_smem[];
     const int warps_per_block = blockDim.x >> 5;
     const int i = blockIdx.x * warps_per_block + (threadIdx.x >> 5);
@@ -229,6 +256,11 @@ nl_rows_onepass_kernel(const int32_t *__restrict__ atom_off, int nsys, int natom
     const int cx = c % g.nx, cy = (c / g.nx) % g.ny, cz = c / (g.nx * g.ny);
     const double4 pi = ld_xyz(xyz, i);
     const double ri_pad = shorts ? prm64[4 * (size_t)i + 1] + reach_pad : 0.0;
+    // the FP32 frame of the cell copy; r² within margin2 of a cutoff is
+    // decided in FP64, so the rows are those of the FP64 test bit for bit
+    const float pfx = (float)(pi.x - g.xlo), pfy = (float)(pi.y - g.ylo), pfz = (float)(pi.z - g.zlo);
+    const float m2 = g.margin2, cut_lo = (float)rcut2 - m2, cut_hi = (float)rcut2 + m2;
+    const float rpad_f = (float)ri_pad;
     int nfull = 0, nhalf = 0, nsfull = 0, nshalf = 0;
     int jmin = 0x7fffffff, jmax = -1;
     const unsigned lt = (1u << lane) - 1u;
@@ -249,11 +281,27 @@ nl_rows_onepass_kernel(const int32_t *__restrict__ atom_off, int nsys, int natom
                     bool in = false, sh = false;
                     if (k < end) {
                         j = cell_atoms[k];
-                        const double r2 = d2_of(pi, ld_xyz(xyz, j));
-                        in = (j != i) && r2 < rcut2;
-                        if (in && shorts) {
-                            const double reach = ri_pad + prm64[4 * (size_t)j + 1];
-                            sh = r2 < reach * reach;
+                        const float4 q = cell_pos[k];
+                        const float dx = q.x - pfx, dy = q.y - pfy, dz = q.z - pfz;
+                        const float r2f = dx * dx + dy * dy + dz * dz;
+                        if (r2f < cut_hi && j != i) {
+                            double r2 = -1.0;  // FP64 r², computed only when a test needs it
+                            if (r2f > cut_lo) {
+                                r2 = d2_of(pi, ld_xyz(xyz, j));
+                                in = r2 < rcut2;
+                            } else {
+                                in = true;
+                            }
+                            if (in && shorts) {
+                                const float rf = rpad_f + q.w, rf2 = rf * rf;
+                                if (r2f < rf2 - m2) {
+                                    sh = true;
+                                } else if (r2f <= rf2 + m2) {
+                                    if (r2 < 0.0) r2 = d2_of(pi, ld_xyz(xyz, j));
+                                    const double reach = ri_pad + prm64[4 * (size_t)j + 1];
+                                    sh = r2 < reach * reach;
+                                }
+                            }
                         }
                     }
                     const unsigned mf = __ballot_sync(0xffffffffu, in);
@@ -407,14 +455,16 @@ extern "C" int alma_nl_build(const AlmaBatch *b, const AlmaTopo *t, AlmaNL *nl, 
                                          w.cell_fill, w.cell_atoms);
     // oversized cells (> SORT_SMEM atoms) sort through the spill space
     nl_cellsort_kernel<<<1184, 256, 0, st>>>(w.total_cells, w.ok, w.cell_start, w.cell_atoms, w.sort_spill);
+    nl_cellpos_kernel<<<nb, tb, 0, st>>>(b->atom_off, nsys, natoms, w.total_cells, w.ok, w.cell_start, w.cell_atoms,
+                                         w.grid, b->xyz, b->prm64, w.cell_pos);
     const int wpb = 8, rb = (natoms + wpb - 1) / wpb;
     const int64_t *ep = t ? t->excl_ptr : nullptr;
     const int32_t *ec = t ? t->excl_cols : nullptr;
     ALMA_CUDA_TRY(cudaMemsetAsync(w.cursor, 0, sizeof(int64_t) * 4 * (size_t)nsys, st));
     nl_rows_onepass_kernel<<<rb, wpb * 32, sizeof(uint32_t) * NL_STAGE * wpb, st>>>(
         b->atom_off, nsys, natoms, sys_mask, b->xyz, rcut2, w.grid, w.ok, w.cell_of, w.cell_start, w.cell_atoms,
-        b->prm64, reach_pad, ep, ec, *nl, w.cursor);
+        w.cell_pos, b->prm64, reach_pad, ep, ec, *nl, w.cursor);
     nl_finalize_kernel<<<(nsys + 255) / 256, 256, 0, st>>>(nsys, sys_mask, w.ok, w.cursor, *nl, b->status);
-    ALMA_LAUNCH_CHECK_N("alma_nl_build", 10);
+    ALMA_LAUNCH_CHECK_N("alma_nl_build", 11);
     return ALMA_OK;
 }

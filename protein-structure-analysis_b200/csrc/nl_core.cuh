@@ -8,10 +8,23 @@ namespace alma {
 
 struct SysGrid {
     double xlo, ylo, zlo, cs;
-    int32_t nx, ny, nz, pad;
+    int32_t nx, ny, nz;
+    float margin2;     // FP32 prefilter margin on r² (Å²), see fp32_margin2
     int64_t cell_off;  // first global cell of this system
     int64_t ncell;
 };
+
+// Margin on r² within which an FP32 distance test (coordinates relative to
+// the grid origin, so |x| <= the grid's extent E) cannot decide a 14 Å or
+// SASA-reach cutoff and the FP64 test runs.  Each coordinate carries at
+// most E 2^-24 of rounding, a difference twice that plus its own rounding,
+// so near a cutoff r <= 14 Å the squared distance is off by at most
+// 2 (2 E 2^-24) sqrt(3) 14 plus a few ulps of 196; the margin takes 16x
+// that (0.05 Å² at E = 1,000 Å) and never less than 0.01 Å².
+__device__ __forceinline__ float fp32_margin2(double extent) {
+    const double d = 2.0 * extent * 5.9604644775390625e-8 + 1e-6;
+    return (float)fmax(0.01, 16.0 * (2.0 * d * 1.7320508075688772 * 14.0 + 3.0e-5));
+}
 
 // Grid of one system from its bounding box (physics_engine.cpp:299-316):
 // cells of 14 Å + 1e-6, the box padded by one cell on every side.
@@ -25,7 +38,7 @@ __device__ __forceinline__ SysGrid grid_from_box(const double lo[3], const doubl
     g.ny = max(1, (int)ceil(ly / g.cs));
     g.nz = max(1, (int)ceil(lz / g.cs));
     if (natoms <= 0) { g.nx = g.ny = g.nz = 1; }
-    g.pad = 0;
+    g.margin2 = fp32_margin2(fmax(g.nx, fmax(g.ny, g.nz)) * g.cs);
     g.ncell = (int64_t)g.nx * g.ny * g.nz;
     g.cell_off = 0;
     return g;
