@@ -32,9 +32,11 @@ __global__ void born_kernel(int natoms, const int32_t *__restrict__ atom_off, in
 }
 
 // Warp per atom: pair energy and SASA of row i.  atom_e[2*i] = pair sum of
-// row i, atom_e[2*i+1] = gamma * max(0, sa_i).
+// row i, atom_e[2*i+1] = gamma * max(0, sa_i).  Held to 64 registers (four
+// 256-thread blocks per SM): the row gathers are latency bound and need the
+// resident warps.
 template <typename R>
-__global__ void pair_sasa_kernel(DevParams P, int natoms, const int32_t *__restrict__ atom_off, int nsys,
+__global__ void __launch_bounds__(256, 4) pair_sasa_kernel(DevParams P, int natoms, const int32_t *__restrict__ atom_off, int nsys,
                                  const uint8_t *__restrict__ mask, const double *__restrict__ xyz,
                                  const float *__restrict__ prm,
                                  const double *__restrict__ prm64, const double *__restrict__ born,

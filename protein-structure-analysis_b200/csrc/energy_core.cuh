@@ -73,8 +73,8 @@ __device__ __forceinline__ void pair_sasa_atom(const DevParams &P, int i, int la
             const uint32_t ent = half_cols[k];
             const int j = (int)(ent & ALMA_IDX_MASK);
             const double r2d = d2_of(pi, ld_xyz(xyz, j));
-            const double4 pj64 = *reinterpret_cast<const double4 *>(prm64 + 4 * (size_t)j);
-            const double rsj = pj64.y + P.probe_r;
+            const double rj64 = prm64[4 * (size_t)j + 1];
+            const double rsj = rj64 + P.probe_r;
             const double r = sqrt(r2d), dc = rsi + rsj;
             if (r < dc) {
                 hit = true;
@@ -83,8 +83,11 @@ __device__ __forceinline__ void pair_sasa_atom(const DevParams &P, int i, int la
             if (!(use_excl && (ent & ALMA_EXCL_BIT)) && r2d <= P.pair_cut2) {
                 R qj, rj, ej;
                 load_prm<R>(prm, prm64, j, qj, rj, ej);
-                e += (double)pair_energy<R>(P, r2d, qi * qj, ri + rj, ei * ej, ai, (R)born[j], ri64 + pj64.y,
-                                            ei64 * pj64.z);
+                // FP64 sigma from the radii already loaded; the FP64 epsilon
+                // product only for a contact inside sigma (steep LJ)
+                const double sig64 = ri64 + rj64;
+                const double eps64 = r2d < sig64 * sig64 ? ei64 * prm64[4 * (size_t)j + 2] : 0.0;
+                e += (double)pair_energy<R>(P, r2d, qi * qj, ri + rj, ei * ej, ai, (R)born[j], sig64, eps64);
             }
         }
         sa = sasa_chunk(sa, __ballot_sync(0xffffffffu, hit), cap, lane);  // in row order
