@@ -29,8 +29,12 @@ __device__ __forceinline__ void born_atom(int i, int lane, const double *__restr
     load_prm<R>(prm, prm64, i, qi, ri, ei);
     const double4 pi = ld_xyz(xyz, i);
     double sum = 0.0;
-    for (int64_t k = full_ptr[i] + lane; k < full_ptr[i] + full_len[i]; k += 32) {
-        const int j = (int)(full_cols[k] & ALMA_IDX_MASK);
+    const int64_t end = full_ptr[i] + full_len[i];
+    int64_t k = full_ptr[i] + lane;
+    uint32_t nxt = k < end ? full_cols[k] : 0u;  // the next entry is fetched while this one is evaluated
+    for (; k < end; k += 32) {
+        const int j = (int)(nxt & ALMA_IDX_MASK);
+        if (k + 32 < end) nxt = full_cols[k + 32];
         R qj, rj, ej;
         load_prm<R>(prm, prm64, j, qj, rj, ej);
         const double r2d = d2_of(pi, ld_xyz(xyz, j));
@@ -65,15 +69,24 @@ __device__ __forceinline__ void pair_sasa_atom(const DevParams &P, int i, int la
     double sa = 4.0 * 3.14159265358979323846 * rsi * rsi;
     double e = 0.0;
     const int64_t beg = half_ptr[i], end = half_ptr[i] + half_len[i];
+    // the next chunk's entry is fetched while this one is evaluated, and all
+    // of an entry's gathers are issued together (one dependent round trip
+    // per chunk; the 12-14 Å entries load parameters they do not use)
+    uint32_t nxt = beg + lane < end ? half_cols[beg + lane] : 0u;
     for (int64_t k0 = beg; k0 < end; k0 += 32) {
         const int64_t k = k0 + lane;
         double cap = 0.0;
         bool hit = false;
         if (k < end) {
-            const uint32_t ent = half_cols[k];
+            const uint32_t ent = nxt;
+            if (k + 32 < end) nxt = half_cols[k + 32];
             const int j = (int)(ent & ALMA_IDX_MASK);
-            const double r2d = d2_of(pi, ld_xyz(xyz, j));
+            const double4 pj = ld_xyz(xyz, j);
             const double rj64 = prm64[4 * (size_t)j + 1];
+            R qj, rj, ej;
+            load_prm<R>(prm, prm64, j, qj, rj, ej);
+            const R aj = (R)born[j];
+            const double r2d = d2_of(pi, pj);
             const double rsj = rj64 + P.probe_r;
             const double r = sqrt(r2d), dc = rsi + rsj;
             if (r < dc) {
@@ -81,13 +94,11 @@ __device__ __forceinline__ void pair_sasa_atom(const DevParams &P, int i, int la
                 cap = cap_scale * ((dc - r) / (2.0 * rsi));
             }
             if (!(use_excl && (ent & ALMA_EXCL_BIT)) && r2d <= P.pair_cut2) {
-                R qj, rj, ej;
-                load_prm<R>(prm, prm64, j, qj, rj, ej);
                 // FP64 sigma from the radii already loaded; the FP64 epsilon
                 // product only for a contact inside sigma (steep LJ)
                 const double sig64 = ri64 + rj64;
                 const double eps64 = r2d < sig64 * sig64 ? ei64 * prm64[4 * (size_t)j + 2] : 0.0;
-                e += (double)pair_energy<R>(P, r2d, qi * qj, ri + rj, ei * ej, ai, (R)born[j], sig64, eps64);
+                e += (double)pair_energy<R>(P, r2d, qi * qj, ri + rj, ei * ej, ai, aj, sig64, eps64);
             }
         }
         sa = sasa_chunk(sa, __ballot_sync(0xffffffffu, hit), cap, lane);  // in row order
