@@ -167,20 +167,24 @@ __global__ void __launch_bounds__(256, 4) grad_pair_kernel(DevParams P, int nato
     const R ai = (R)born[i];
     double gx = 0.0, gy = 0.0, gz = 0.0, da = 0.0;
     const int64_t beg = full_ptr[i], end = beg + full_len[i];
+    // the next entry is fetched while this one is evaluated, and an entry's
+    // gathers are issued together (one dependent round trip per entry)
+    uint32_t nxt = beg + lane < end ? full_cols[beg + lane] : 0u;
     for (int64_t k = beg + lane; k < end; k += 32) {
-        const uint32_t ent = full_cols[k];
+        const uint32_t ent = nxt;
+        if (k + 32 < end) nxt = full_cols[k + 32];
         if (use_excl && (ent & ALMA_EXCL_BIT)) continue;
         const int j = (int)(ent & ALMA_IDX_MASK);
         const double4 pj = ld_xyz(xyz, j);
+        R qj, rj, ej;
+        load_prm_g<R>(prm, prm64, j, qj, rj, ej);
+        const double rj64 = prm64[4 * (size_t)j + 1], ej64 = prm64[4 * (size_t)j + 2];
+        const double bj = born[j];
         const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
         const double r2 = dx * dx + dy * dy + dz * dz;
         if (r2 > P.pair_cut2) continue;
-        R qj, rj, ej;
-        load_prm_g<R>(prm, prm64, j, qj, rj, ej);
-        const double4 p64j = *reinterpret_cast<const double4 *>(prm64 + 4 * (size_t)j);
-        const double bj = born[j];
         double fr, dEdA;
-        pair_grad<R>(P, r2, qi * qj, ri + rj, ei * ej, ai, (R)bj, p64i.y + p64j.y, p64i.z * p64j.z, fr, dEdA);
+        pair_grad<R>(P, r2, qi * qj, ri + rj, ei * ej, ai, (R)bj, p64i.y + rj64, p64i.z * ej64, fr, dEdA);
         gx += fr * dx;
         gy += fr * dy;
         gz += fr * dz;
@@ -390,14 +394,17 @@ __global__ void grad_born_kernel(int natoms, const int32_t *__restrict__ atom_of
     const double ci = ai < 0.5 ? 0.5 * dEda[i] * ai * ai : 0.0;
     double gx = 0.0, gy = 0.0, gz = 0.0;
     const int64_t beg = full_ptr[i], end = beg + full_len[i];
+    uint32_t nxt = beg + lane < end ? full_cols[beg + lane] : 0u;  // next entry in flight
     for (int64_t k = beg + lane; k < end; k += 32) {
-        const int j = (int)(full_cols[k] & ALMA_IDX_MASK);
-        const double aj = born[j];
-        const double cj = aj < 0.5 ? 0.5 * dEda[j] * aj * aj : 0.0;
-        if (ci == 0.0 && cj == 0.0) continue;
+        const int j = (int)(nxt & ALMA_IDX_MASK);
+        if (k + 32 < end) nxt = full_cols[k + 32];
+        // every gather of the entry issued together (one round trip)
+        const double aj = born[j], dj = dEda[j];
         R qj, rj, ej;
         load_prm_g<R>(prm, prm64, j, qj, rj, ej);
         const double4 pj = ld_xyz(xyz, j);
+        const double cj = aj < 0.5 ? 0.5 * dj * aj * aj : 0.0;
+        if (ci == 0.0 && cj == 0.0) continue;
         const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
         const R r2 = (R)(dx * dx + dy * dy + dz * dz);
         const R r = f_sqrt(r2);
