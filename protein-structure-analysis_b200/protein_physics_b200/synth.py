@@ -241,14 +241,26 @@ def _intra_pairs(res, order):
     return _INTRA[res]
 
 
+# Sidechain packing scores overlaps against the force field's own contact
+# distance R*_i + R*_j: a pair closer than PACK_FRAC of it (C-C 2.85 Å, H-H
+# 2.2 Å, O to an aliphatic H 2.4 Å) counts by its depth.  Real contacts sit
+# above that (C-C >= 3.4 Å); the energy model's r^-12 term makes anything
+# below it cost tens to thousands of kcal/mol.
+PACK_FRAC = 0.75
+
+
+def _radius(res, name):
+    return float(_FF["%s:%s" % (res, name)][1])
+
+
 def _intra_cost(res, order, P, heavy_cut, any_cut):
     pr = _intra_pairs(res, order)
     if len(pr) == 0:
-        return 0
+        return 0.0
     d = np.linalg.norm(P[pr[:, 0]] - P[pr[:, 1]], axis=1)
-    hv = np.array([not nm.startswith("H") for nm in order])
-    hh = hv[pr[:, 0]] & hv[pr[:, 1]]
-    return int(np.sum(d < any_cut) + np.sum((d < heavy_cut) & hh & (d >= any_cut)))
+    rad = np.array([_radius(res, nm) for nm in order])
+    over = PACK_FRAC * (rad[pr[:, 0]] + rad[pr[:, 1]]) - d
+    return float(np.sum(over[over > 0]))
 
 
 class _Grid:
@@ -260,12 +272,12 @@ class _Grid:
         self.cells = {}
         self.by_res = {}  # residue -> [(cell key, x, y, z, heavy)]
 
-    def add(self, P, hv, r):
+    def add(self, P, hv, r, rad=None):
         ent = []
         for k in range(P.shape[0]):
             x, y, z = float(P[k][0]), float(P[k][1]), float(P[k][2])
             key = (math.floor(x / self.cell), math.floor(y / self.cell), math.floor(z / self.cell))
-            item = (x, y, z, bool(hv[k]), r)
+            item = (x, y, z, bool(hv[k]), r, float(rad[k]) if rad is not None else 0.0)
             self.cells.setdefault(key, []).append(item)
             ent.append((key, item))
         self.by_res.setdefault(r, []).extend(ent)
@@ -275,21 +287,29 @@ class _Grid:
             lst = self.cells[key]
             lst.remove(item)
 
-    def cost(self, P, hv, r, heavy_cut, any_cut, min_gap=2):
-        c = 0
+    def cost(self, P, hv, r, heavy_cut, any_cut, min_gap=2, rad=None):
+        """Clashes of points P (residue r) with the stored points of
+        residues >= min_gap away: a count by the heavy / any cutoffs, or,
+        with radii, the summed depth below PACK_FRAC (R*_i + R*_j)."""
+        c = 0.0 if rad is not None else 0
         a2, h2 = any_cut * any_cut, heavy_cut * heavy_cut
         for k in range(P.shape[0]):
             x, y, z = float(P[k][0]), float(P[k][1]), float(P[k][2])
             kx, ky, kz = math.floor(x / self.cell), math.floor(y / self.cell), math.floor(z / self.cell)
             hk = bool(hv[k])
+            rk = float(rad[k]) if rad is not None else 0.0
             for dx in (-1, 0, 1):
                 for dy in (-1, 0, 1):
                     for dz in (-1, 0, 1):
-                        for (px, py, pz, ph, pr) in self.cells.get((kx + dx, ky + dy, kz + dz), ()):
+                        for (px, py, pz, ph, pr, prad) in self.cells.get((kx + dx, ky + dy, kz + dz), ()):
                             if abs(pr - r) < min_gap:
                                 continue
                             d2 = (x - px) ** 2 + (y - py) ** 2 + (z - pz) ** 2
-                            if d2 < a2 or (d2 < h2 and hk and ph):
+                            if rad is not None:
+                                lim = PACK_FRAC * (rk + prad)
+                                if d2 < lim * lim:
+                                    c += lim - math.sqrt(d2)
+                            elif d2 < a2 or (d2 < h2 and hk and ph):
                                 c += 1
         return c
 
@@ -318,9 +338,10 @@ def grow(sequence, draw_phipsi, rng, tries=12, heavy_cut=2.2, any_cut=1.3, back=
     def backbone_atoms(r, N, CA, C, ph, ps):
         order, P = _place_residue(sequence[r], N, CA, C, ph, ps, None)
         keep = [k for k, nm in enumerate(order) if nm in _BB_ATOMS and not (nm == "CD" and sequence[r] != "PRO")]
-        return P[keep], np.array([not order[k].startswith("H") for k in keep])
+        return (P[keep], np.array([not order[k].startswith("H") for k in keep]),
+                np.array([_radius(sequence[r], order[k]) for k in keep]))
 
-    grid = _Grid(max(heavy_cut, any_cut))
+    grid = _Grid(max(heavy_cut, any_cut, 2.0 * PACK_FRAC * max(v[1] for v in _FF.values())))
     grid_upto = -1
     r = 0
     while r < n_res:
@@ -329,7 +350,7 @@ def grow(sequence, draw_phipsi, rng, tries=12, heavy_cut=2.2, any_cut=1.3, back=
             grid_upto -= 1
         while grid_upto < r - 2:
             grid_upto += 1
-            grid.add(bbpos[grid_upto][0], bbpos[grid_upto][1], grid_upto)
+            grid.add(bbpos[grid_upto][0], bbpos[grid_upto][1], grid_upto, rad=bbpos[grid_upto][2])
         best = None
         for t in range(tries):
             ph, ps = draw_phipsi(r)
@@ -350,17 +371,17 @@ def grow(sequence, draw_phipsi, rng, tries=12, heavy_cut=2.2, any_cut=1.3, back=
                 N = _place(pN, pCA, pC, bb["b_c_n"], bb["a_ca_c_n"], ps_prev)
                 CA = _place(pCA, pC, N, bb["b_n_ca"], bb["a_c_n_ca"], 180.0)
                 C = _place(pC, N, CA, bb["b_ca_c"], bb["a_n_ca_c"], ph)
-            P, hv = backbone_atoms(r, N, CA, C, ph, ps)
-            cost = grid.cost(P, hv, r, heavy_cut, any_cut) if r >= 2 else 0
+            P, hv, rad = backbone_atoms(r, N, CA, C, ph, ps)
+            cost = grid.cost(P, hv, r, heavy_cut, any_cut, rad=rad) if r >= 2 else 0
             if r >= 3 and ps_prev != psi[r - 1]:  # the redrawn psi moves residue r-1's O too: check it again
                 pN, pCA, pC = frames[r - 1]
-                Pp, hvp = backbone_atoms(r - 1, pN, pCA, pC, phi[r - 1], ps_prev)
-                cost += grid.cost(Pp, hvp, r - 1, heavy_cut, any_cut)
+                Pp, hvp, radp = backbone_atoms(r - 1, pN, pCA, pC, phi[r - 1], ps_prev)
+                cost += grid.cost(Pp, hvp, r - 1, heavy_cut, any_cut, rad=radp)
             if best is None or cost < best[0]:
-                best = (cost, ph, ps, ps_prev, P, hv, (N, CA, C))
+                best = (cost, ph, ps, ps_prev, P, hv, rad, (N, CA, C))
             if cost == 0:
                 break
-        cost, ph, ps, ps_prev, P, hv, frame = best
+        cost, ph, ps, ps_prev, P, hv, rad, frame = best
         budget -= 1
         if cost > 0 and budget > 0 and r >= 2:
             fails[r] += 1
@@ -371,7 +392,7 @@ def grow(sequence, draw_phipsi, rng, tries=12, heavy_cut=2.2, any_cut=1.3, back=
             pN, pCA, pC = frames[r - 1]
             bbpos[r - 1] = backbone_atoms(r - 1, pN, pCA, pC, phi[r - 1], ps_prev)
         phi[r], psi[r] = ph, ps
-        bbpos[r], frames[r] = (P, hv), frame
+        bbpos[r], frames[r] = (P, hv, rad), frame
         r += 1
     return pack_sidechains(sequence, phi, psi, frames, bbpos, rng, heavy_cut, any_cut)
 
@@ -379,12 +400,16 @@ def grow(sequence, draw_phipsi, rng, tries=12, heavy_cut=2.2, any_cut=1.3, back=
 def pack_sidechains(sequence, phi, psi, frames, bbpos, rng, heavy_cut=2.2, any_cut=1.3):
     """Greedy seeded sidechain placement on a fixed backbone: in a random
     residue order, keep the drawn chis when clash-free, else try every well
-    combination of the first three chis and keep the least clashing."""
+    combination of the first three chis and keep the least clashing.  A
+    clash is an overlap below PACK_FRAC of the force field's contact
+    distance, weighed by its depth."""
     n_res = len(sequence)
     chis = [_draw_chis(res, rng) for res in sequence]
-    grid = _Grid(max(heavy_cut, any_cut))
+    # the contact test reaches PACK_FRAC x the largest R* pair
+    grid = _Grid(max(heavy_cut, any_cut, 2.0 * PACK_FRAC * max(v[1] for v in _FF.values())))
     for rr in range(n_res):
-        grid.add(bbpos[rr][0], bbpos[rr][1], rr)
+        P0, hv0 = bbpos[rr][0], bbpos[rr][1]
+        grid.add(P0, hv0, rr, rad=bbpos[rr][2] if len(bbpos[rr]) > 2 else np.full(len(P0), 1.7))
     for rr in rng.permutation(n_res):
         res = sequence[rr]
         m = n_chi(res)
@@ -394,7 +419,9 @@ def pack_sidechains(sequence, phi, psi, frames, bbpos, rng, heavy_cut=2.2, any_c
         if not sc:
             continue
         hv = np.array([not order[k].startswith("H") for k in sc])
-        cost = grid.cost(P[sc], hv, rr, heavy_cut, any_cut, min_gap=1) + _intra_cost(res, order, P, heavy_cut, any_cut)
+        rad = np.array([_radius(res, order[k]) for k in sc])
+        cost = grid.cost(P[sc], hv, rr, heavy_cut, any_cut, min_gap=1, rad=rad) + \
+            _intra_cost(res, order, P, heavy_cut, any_cut)
         if cost and m:
             best = (cost, chis[rr], P)
             for combo in np.ndindex(*([3] * min(m, 3))):
@@ -402,14 +429,14 @@ def pack_sidechains(sequence, phi, psi, frames, bbpos, rng, heavy_cut=2.2, any_c
                 for q, w in enumerate(combo):
                     trial[q] = ROTAMER_WELLS[w] + rng.uniform(-10.0, 10.0)
                 _, P2 = _place_residue(res, N, CA, C, phi[rr], psi[rr], trial)
-                c2 = (grid.cost(P2[sc], hv, rr, heavy_cut, any_cut, min_gap=1)
+                c2 = (grid.cost(P2[sc], hv, rr, heavy_cut, any_cut, min_gap=1, rad=rad)
                       + _intra_cost(res, order, P2, heavy_cut, any_cut))
                 if c2 < best[0]:
                     best = (c2, trial, P2)
                 if c2 == 0:
                     break
             chis[rr], P = best[1], best[2]
-        grid.add(P[sc], hv, rr)
+        grid.add(P[sc], hv, rr, rad=rad)
     return build(sequence, phi, psi, chis=chis)
 
 
@@ -462,7 +489,8 @@ def _frames(ch):
         names = ch.atomnames[a0:a1]
         frames.append((ch.xyz[a0], ch.xyz[a0 + 1], ch.xyz[a0 + 2]))
         keep = [k for k, nm in enumerate(names) if nm in _BB_ATOMS and not (nm == "CD" and res != "PRO")]
-        bbpos.append((ch.xyz[a0:a1][keep], np.array([not names[k].startswith("H") for k in keep])))
+        bbpos.append((ch.xyz[a0:a1][keep], np.array([not names[k].startswith("H") for k in keep]),
+                      np.array([_radius(res, names[k]) for k in keep])))
     return frames, bbpos
 
 
@@ -479,35 +507,45 @@ _N_SIDECHAIN = {"GLY": 0, "ALA": 1, "SER": 2, "CYS": 2, "VAL": 3, "THR": 3, "PRO
 
 
 class _BeadChain:
-    """Collapse model of a built chain: per residue N, CA, a sidechain bead
-    and C (in that order, so every torsion moves a suffix of the points),
-    each a soft sphere; the backbone phi / psi are the degrees of freedom
-    (omega and the bond geometry stay as built)."""
+    """Collapse model of a built chain: per residue N, CA, a sidechain bead,
+    C and the carbonyl O (in that order, so every torsion moves a suffix of
+    the points), each a soft sphere; the backbone phi / psi are the degrees
+    of freedom (omega and the bond geometry stay as built).  The O atoms
+    keep neighbouring backbone turns at hydrogen-bond distance or more
+    (without them a collapse packs carbonyls into each other)."""
+
+    PER_RES = 5
 
     def __init__(self, ch, radius_scale):
         n_res = len(ch.sequence)
         ridx = np.asarray(ch.res_idx)
-        first = np.searchsorted(ridx, np.arange(n_res + 1))[:-1]
-        N, CA, C = ch.xyz[first], ch.xyz[first + 1], ch.xyz[first + 2]
+        first = np.searchsorted(ridx, np.arange(n_res + 1))
+        N, CA, C = ch.xyz[first[:-1]], ch.xyz[first[:-1] + 1], ch.xyz[first[:-1] + 2]
+        names = np.asarray(ch.atomnames)
+        O = np.empty_like(N)
+        for r in range(n_res):
+            k = np.flatnonzero(names[first[r]:first[r + 1]] == "O")
+            O[r] = ch.xyz[first[r] + k[0]] if len(k) else C[r]
         nsc = np.array([_N_SIDECHAIN[r] for r in ch.sequence])
         # bead on the ideal C-beta direction, further out for larger sidechains
         b, c = CA - N, C - CA
         d = -0.58273431 * np.cross(b, c) + 0.56802827 * b - 0.54067466 * c
         d /= np.linalg.norm(d, axis=1, keepdims=True)
         B = CA + np.minimum(1.53 + 0.45 * np.maximum(nsc - 1, 0), 4.0)[:, None] * d
-        self.X0 = np.stack([N, CA, B, C], 1).reshape(-1, 3)
+        P = self.PER_RES
+        self.X0 = np.stack([N, CA, B, C, O], 1).reshape(-1, 3)
         self.rad = radius_scale * np.stack([np.full(n_res, 1.6), np.full(n_res, 1.9),
                                             np.where(nsc > 0, 1.9 + 0.35 * np.sqrt(nsc), 0.0),
-                                            np.full(n_res, 1.7)], 1).reshape(-1)
-        self.res = np.repeat(np.arange(n_res), 4)
-        self.bead = np.tile(np.arange(4) == 2, n_res)
+                                            np.full(n_res, 1.7), np.full(n_res, 1.5)], 1).reshape(-1)
+        self.res = np.repeat(np.arange(n_res), P)
+        self.bead = np.tile(np.arange(P) == 2, n_res)
         self.real = np.flatnonzero(self.rad > 0)
         tors = []
         for r in range(n_res):
             if r > 0 and ch.sequence[r] != "PRO":
-                tors.append((4 * r, 4 * r + 1, 4 * r + 2))  # phi about N-CA: moves the bead, C and beyond
+                tors.append((P * r, P * r + 1, P * r + 2))  # phi about N-CA: moves the bead, C, O and beyond
             if r < n_res - 1:
-                tors.append((4 * r + 1, 4 * r + 3, 4 * r + 4))  # psi about CA-C: moves the next residue on
+                tors.append((P * r + 1, P * r + 3, P * r + 4))  # psi about CA-C: moves O and the next residues
         self.tors = np.array(tors, dtype=np.int64).reshape(-1, 3)
         self.owner = np.searchsorted(self.tors[:, 2], np.arange(self.X0.shape[0]), side="right") - 1
 
@@ -581,7 +619,7 @@ class _BeadChain:
 
 def collapse(ch: Chain, seed, rg_target, iters=6000, k_rg=5.0, k_rep=10.0, radius_scale=0.85, domains=None):
     """Seeded backbone collapse: L-BFGS over every backbone phi / psi of a
-    soft-sphere bead model (N, CA, C and one sidechain bead per residue) on
+    soft-sphere bead model (N, CA, C, O and one sidechain bead per residue) on
     k_rg (Rg - rg_target)^2 plus the overlap penalty, then a rebuild from
     the resulting phi / psi and a seeded sidechain packing.  The restraint
     target sits below the Rg wanted: the overlap penalty holds the chain
@@ -590,8 +628,9 @@ def collapse(ch: Chain, seed, rg_target, iters=6000, k_rg=5.0, k_rep=10.0, radiu
     from scipy.optimize import minimize
     rng = np.random.default_rng(seed)
     model = _BeadChain(ch, radius_scale)
+    P = _BeadChain.PER_RES
     if domains:
-        groups = [np.intersect1d(model.real, np.arange(4 * r0, 4 * r1)) for r0, r1 in domains]
+        groups = [np.intersect1d(model.real, np.arange(P * r0, P * r1)) for r0, r1 in domains]
     else:
         groups = [model.real]
 
@@ -602,7 +641,7 @@ def collapse(ch: Chain, seed, rg_target, iters=6000, k_rg=5.0, k_rep=10.0, radiu
 
     res = minimize(f, np.zeros(len(model.tors)), jac=True, method="L-BFGS-B",
                    options={"maxiter": int(iters), "maxfun": 2 * int(iters)})
-    X = model.coords(res.x).reshape(-1, 4, 3)
+    X = model.coords(res.x).reshape(-1, P, 3)
     N, CA, C = X[:, 0], X[:, 1], X[:, 3]
     n_res = len(ch.sequence)
     phi, psi = ch.phi.copy(), ch.psi.copy()
