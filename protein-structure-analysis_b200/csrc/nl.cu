@@ -305,21 +305,36 @@ nl_rows_onepass_kernel(const int32_t *__restrict__ atom_off, int nsys, int natom
                         }
                     }
                     const unsigned mf = __ballot_sync(0xffffffffu, in);
+                    const int at = nfull + __popc(mf & lt);
                     if (in) {
                         jmin = min(jmin, j);
                         jmax = max(jmax, j);
-                        const int at = nfull + __popc(mf & lt);
                         if (at < NL_STAGE)
                             stage[at] = (uint32_t)j | (excluded(excl_ptr, excl_cols, i, j) ? ALMA_EXCL_BIT : 0u) |
                                         (sh ? NL_SHORT_BIT : 0u);
                     }
+                    // the other row kinds are counted from the stage after the
+                    // scan; only entries past its end (a rare long row) here
+                    if (nfull + __popc(mf) > NL_STAGE) {
+                        const bool over = in && at >= NL_STAGE;
+                        nhalf += __popc(__ballot_sync(0xffffffffu, over && j > i));
+                        nsfull += __popc(__ballot_sync(0xffffffffu, over && sh));
+                        nshalf += __popc(__ballot_sync(0xffffffffu, over && sh && j > i));
+                    }
                     nfull += __popc(mf);
-                    nhalf += __popc(__ballot_sync(0xffffffffu, in && j > i));
-                    nsfull += __popc(__ballot_sync(0xffffffffu, sh));
-                    nshalf += __popc(__ballot_sync(0xffffffffu, sh && j > i));
                 }
             }
         }
+    }
+    __syncwarp();
+    for (int t0 = 0; t0 < min(nfull, NL_STAGE); t0 += 32) {  // half / short counts of the staged entries
+        const int t = t0 + lane;
+        const uint32_t st = t < min(nfull, NL_STAGE) ? stage[t] : 0u;
+        const bool v = t < min(nfull, NL_STAGE);
+        const bool hf = v && (int)(st & ALMA_IDX_MASK & ~NL_SHORT_BIT) > i, sh = v && (st & NL_SHORT_BIT);
+        nhalf += __popc(__ballot_sync(0xffffffffu, hf));
+        nsfull += __popc(__ballot_sync(0xffffffffu, sh));
+        nshalf += __popc(__ballot_sync(0xffffffffu, hf && sh));
     }
     // space in the system's regions (relative offsets; -1: does not fit)
     int64_t off[4] = {0, 0, 0, 0};
