@@ -494,6 +494,11 @@ def _frames(ch):
     return frames, bbpos
 
 
+def _wrap(deg):
+    """An angle difference in degrees, wrapped to [-180, 180)."""
+    return (deg + 180.0) % 360.0 - 180.0
+
+
 def _torsion(a, b, c, d):
     b1, b2, b3 = b - a, c - b, d - c
     n1, n2 = np.cross(b1, b2), np.cross(b2, b3)
@@ -539,6 +544,7 @@ class _BeadChain:
                                             np.full(n_res, 1.7), np.full(n_res, 1.5)], 1).reshape(-1)
         self.res = np.repeat(np.arange(n_res), P)
         self.bead = np.tile(np.arange(P) == 2, n_res)
+        self.carbonyl = np.tile(np.arange(P) == 4, n_res)
         self.real = np.flatnonzero(self.rad > 0)
         tors = []
         for r in range(n_res):
@@ -548,6 +554,36 @@ class _BeadChain:
                 tors.append((P * r + 1, P * r + 3, P * r + 4))  # psi about CA-C: moves O and the next residues
         self.tors = np.array(tors, dtype=np.int64).reshape(-1, 3)
         self.owner = np.searchsorted(self.tors[:, 2], np.arange(self.X0.shape[0]), side="right") - 1
+        # residues before a proline: psi held in the PPII / beta basin (the
+        # proline's ring sits against the residue before it for other psi;
+        # the bead model does not carry the ring)
+        psi_k = {int(t[0]) // P: k for k, t in enumerate(self.tors) if t[2] % P == 4}
+        self.prepro = [(psi_k[r], P * r, P * r + 1, P * r + 3, P * (r + 1)) for r in range(n_res - 1)
+                       if ch.sequence[r + 1] == "PRO" and r in psi_k]
+        self.prepro_sign = np.ones(len(self.prepro))
+        if self.prepro:  # d psi / d theta of each such torsion (+1 or -1), from a small turn
+            th = np.zeros(len(self.tors))
+            for q, (k, a, b, c, d) in enumerate(self.prepro):
+                th[k] = 1e-3
+            X1 = self.coords(th)
+            for q, (k, a, b, c, d) in enumerate(self.prepro):
+                dpsi = _wrap(_torsion(X1[a], X1[b], X1[c], X1[d]) - _torsion(self.X0[a], self.X0[b], self.X0[c],
+                                                                             self.X0[d]))
+                self.prepro_sign[q] = 1.0 if dpsi > 0 else -1.0
+
+    PREPRO_PSI, PREPRO_HALF = 140.0, 45.0  # degrees: the allowed psi band before a proline
+
+    def prepro_terms(self, X, k_pp):
+        """(energy, [(torsion, dE/dtheta)]) of the flat-bottom psi restraint
+        k_pp (degrees outside the band)^2 on the residues before a proline."""
+        E, out = 0.0, []
+        for q, (k, a, b, c, d) in enumerate(self.prepro):
+            off = _wrap(_torsion(X[a], X[b], X[c], X[d]) - self.PREPRO_PSI)
+            viol = abs(off) - self.PREPRO_HALF
+            if viol > 0:
+                E += k_pp * viol * viol
+                out.append((k, 2.0 * k_pp * viol * math.copysign(1.0, off) * self.prepro_sign[q] * 180.0 / math.pi))
+        return E, out
 
     def coords(self, theta):
         """Points after turning torsion k by theta[k] (radians), axes as built:
@@ -593,7 +629,7 @@ class _BeadChain:
         pr = cKDTree(P).query_pairs(2.0 * self.rad.max(), output_type="ndarray")
         i, j = self.real[pr[:, 0]], self.real[pr[:, 1]]
         dr = np.abs(self.res[i] - self.res[j])
-        keep = (dr >= 2) | ((dr == 1) & self.bead[i] & self.bead[j])
+        keep = (dr >= 2) | ((dr == 1) & ((self.bead[i] & self.bead[j]) | (self.carbonyl[i] & self.carbonyl[j])))
         i, j = i[keep], j[keep]
         v = X[i] - X[j]
         dist = np.sqrt((v * v).sum(1))
@@ -637,7 +673,11 @@ def collapse(ch: Chain, seed, rg_target, iters=6000, k_rg=5.0, k_rep=10.0, radiu
     def f(theta):
         X = model.coords(theta)
         E, g = model.energy(X, groups, rg_target, k_rg, k_rep)
-        return E, model.torsion_grad(X, g)
+        gt = model.torsion_grad(X, g)
+        Ep, gp = model.prepro_terms(X, 0.05)
+        for k, v in gp:
+            gt[k] += v
+        return E + Ep, gt
 
     res = minimize(f, np.zeros(len(model.tors)), jac=True, method="L-BFGS-B",
                    options={"maxiter": int(iters), "maxfun": 2 * int(iters)})
