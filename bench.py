@@ -53,8 +53,8 @@ C3_CHAINS, C3_PER_STEP, C2_PER_STEP = 256, 100, 1000
 L2_NOTE = "inputs larger than L2 (lists of 1.36 M atoms) and a 256 MiB L2 flush between GPU steps"
 # DRAM bytes (read + write) per proposal of the MC kernel, from one ncu capture
 # of a smaller case of the same workload, scaled by the proposals of a launch:
-# profiles/mc_kernel_batched_48_chains.md (200.5 MB / 288 proposals)
-DRAM_BYTES_PER_PROPOSAL = {"batched": 200.5e6 / 288}
+# profiles/mc_kernel_batched_48_chains.md (168.8 MB / 266 proposals)
+DRAM_BYTES_PER_PROPOSAL = {"batched": 168.8e6 / 266}
 
 
 def rank_info():
