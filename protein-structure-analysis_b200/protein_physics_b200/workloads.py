@@ -9,8 +9,9 @@ restraint k (Rg - target)^2 over all atoms:
    gradient of alma_forces projected on the torsions by alma_torsion_grad,
    each bond's step scaled by the inverse inertia of its moving side),
    with +-120 degree rotamer jumps tried every 250 steps on sidechain bonds
-   that move a clashing atom; this clears the clashes the bead model
-   leaves;
+   that move a clashing atom, and every 1,000 steps a search over all well
+   combinations of the first three chis of each residue holding a
+   clashing atom; this clears the clashes the bead model leaves;
 2. seeded Metropolis moves at 300 K (single-bond torsion moves with the
    reference's step rule: uniform in +-cur_max x lever scale, x2.5 for
    sidechain bonds, cur_max adapted to 28-52 % acceptance), each scored
@@ -22,6 +23,7 @@ numpy alone can read back.
 """
 from __future__ import annotations
 
+import itertools
 import math
 
 import numpy as np
@@ -168,11 +170,43 @@ def relax(ch, rg_target, k_rg=200.0, descent_steps=4000, mc_moves=2000, temperat
     eta = 0.05
     nb = ts.nrb
     kinds = np.asarray(F.rb_kind)
-    jumps = 0
+    jumps = repacked = 0
+    chis = {}  # residue -> its sidechain bonds, in topology order (chi1 first)
+    for k in np.flatnonzero(kinds == 2):
+        chis.setdefault(int(ridx[int(F.rb_i[k])]), []).append(int(k))
     for it in range(int(descent_steps)):
         if it % 50 == 0:
             inv_I = torch.as_tensor(1.0 / _side_inertia(b.coords(0), F), device="cuda")
-        if it % 250 == 125:  # rotamer jumps: +-120 deg on sidechain bonds that move a clashing atom
+        if it % 1000 == 500:  # rotamer search: every well combination of a clashing residue's first three chis
+            x = b.coords(0)
+            bad = _clashing_atoms(x, F, np.asarray(ch.radius), ratio=1.5)
+            for r in sorted(set(ridx[bad].tolist())):
+                ks = chis.get(r, [])[:3]
+                if not ks:
+                    continue
+                best = None
+                for combo in itertools.product((0.0, 2.0 * math.pi / 3.0, -2.0 * math.pi / 3.0), repeat=len(ks)):
+                    if not any(combo):
+                        continue
+                    xyz_old.copy_(b.xyz)
+                    born_old.copy_(b.born)
+                    step = torch.zeros(max(nb, 1), dtype=torch.float64, device="cuda")
+                    for k, a in zip(ks, combo):
+                        step[k] = a
+                    ts.apply(step)
+                    En = float(R.energy(with_grad=False))
+                    b.xyz.copy_(xyz_old)
+                    b.born.copy_(born_old)
+                    b.invalidate_sasa()
+                    if math.isfinite(En) and En < E and (best is None or En < best[0]):
+                        best = (En, step)
+                if best is not None:
+                    ts.apply(best[1])
+                    E = best[0]
+                    repacked += 1
+            E = float(R.energy())
+            g_cur = R.g.clone()
+        elif it % 250 == 125:  # rotamer jumps: +-120 deg on sidechain bonds that move a clashing atom
             x = b.coords(0)
             bad = _clashing_atoms(x, F, np.asarray(ch.radius))
             for k in np.flatnonzero(kinds == 2):
@@ -217,6 +251,7 @@ def relax(ch, rg_target, k_rg=200.0, descent_steps=4000, mc_moves=2000, temperat
             eta = max(eta * 0.5, 1e-6)
     info["E_descent"] = E
     info["rotamer_jumps"] = jumps
+    info["residues_repacked"] = repacked
     info["rg_descent"] = R.rg()
     # 2) restrained Metropolis moves (reference step rule, one bond a move)
     rng = np.random.default_rng(seed)
