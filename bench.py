@@ -156,7 +156,7 @@ def rg_of(xyz):
     return float(np.sqrt((c * c).sum(1).mean()))
 
 
-def c3_inputs(rank, n_chains=C3_CHAINS):
+def c3_inputs(rank, n_chains=C3_CHAINS, world=1):
     """The batched workload: chain sizes U{50..600} residues and per-chain
     seeds, helix/coil chains (synth.coil_chain), temperatures geometric over
     280-400 K (kcal/mol)."""
@@ -165,7 +165,8 @@ def c3_inputs(rank, n_chains=C3_CHAINS):
     rng = np.random.default_rng(seed_of(3, rank))
     sizes = rng.integers(50, 601, size=C3_CHAINS)[:n_chains]
     jobs = [(int(n), seed_of(k, rank)) for k, n in enumerate(sizes)]
-    with mp.get_context("spawn").Pool(max(1, min(32, os.cpu_count() or 1))) as pool:  # host Python: all cores
+    procs = max(1, min(32, (os.cpu_count() or 1) // max(1, world)))  # host Python: the cores, shared by the ranks
+    with mp.get_context("spawn").Pool(procs) as pool:
         chains = pool.starmap(_coil_chain_job, jobs, chunksize=1)
     temps = list(280.0 * (400.0 / 280.0) ** (np.arange(C3_CHAINS) / (C3_CHAINS - 1)) * KB)[:n_chains]
     return chains, temps
@@ -292,7 +293,7 @@ def run_ours(args, rank, world, local):
         from protein_physics_b200.dist import init
         init("nccl", timeout_s=120)
     if args.workload == "batched":
-        chains, temps = c3_inputs(rank)
+        chains, temps = c3_inputs(rank, world=world)
         policy, per_step, full_energy = 0, C3_PER_STEP, False
     else:
         chains, temps = [fixture("c2_chain_300res.npz")], [300.0 * KB]
