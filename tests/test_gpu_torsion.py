@@ -173,8 +173,10 @@ def test_mala_log_alpha_matches_host(oracle):
     m = sig > 0
     sg = sig[m]
 
-    def drift(g):  # truncated at ±sigma (drift_clip 1)
-        return np.clip(-0.5 * sg ** 2 * beta * g, -sg, sg)
+    c = R.cfg.drift_clip
+
+    def drift(g):  # truncated at ±drift_clip·sigma
+        return np.clip(-0.5 * sg ** 2 * beta * g, -c * sg, c * sg)
     fwd = np.sum((delta[m] - drift(g0[m])) ** 2 / (2 * sg ** 2))
     rev = np.sum((-delta[m] - drift(g1[m])) ** 2 / (2 * sg ** 2))
     la = -beta * (E1 - E0) - rev + fwd
