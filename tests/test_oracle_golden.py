@@ -97,3 +97,37 @@ def test_move_dE(golden, oracle):
         dE, terms, _, _ = oracle.move_dE(x, q, r, e, nl, a, TA, rots, group)
         assert dE == pytest.approx(dE_ref, abs=1e-8 + 1e-11 * abs(dE_ref)), (kind, code)
         np.testing.assert_allclose(terms, terms_ref, atol=1e-8, rtol=1e-11)
+
+
+def test_grid_face_tie_follows_the_reference(oracle):
+    """The list grid starts one cell below the lowest coordinate
+    (src/physics_engine.cpp:293-342), so the extreme atom of each axis lies
+    on a cell face and the rounding of (x - xlo) / cs picks its cell.  A
+    1e-13 A change of the coordinates can therefore reorder rows (same
+    neighbour sets) and move the order-dependent SASA sum by ~1e-5
+    kcal/mol.  The oracle reproduces the reference's rows bit for bit at
+    every perturbed point, ties included."""
+    from oracle import RefEngine, ref_so_path
+    if ref_so_path() is None:
+        pytest.skip("reference engine not built (oracle/_ref)")
+    from conftest import Golden
+    R = RefEngine()
+    g = Golden("insulin")
+    x0 = np.asarray(g["xyz"], np.float64)
+    p0, c0 = R.nl(x0)
+    s0 = oracle.calculate_potential(x0, g["q"], g["r"], g["eps"])[0]
+    rng = np.random.default_rng(0)
+    reordered = 0
+    for _ in range(6):
+        x = x0 + rng.normal(size=x0.shape) * 1e-13
+        pr, cr = R.nl(x)
+        po, co = oracle.nl_build(x)
+        assert np.array_equal(pr, po) and np.array_equal(cr, co)
+        assert np.array_equal(pr, p0)
+        if not np.array_equal(cr, c0):
+            reordered += 1
+            rows = [i for i in range(len(p0) - 1) if not np.array_equal(cr[pr[i]:pr[i + 1]], c0[p0[i]:p0[i + 1]])]
+            assert all(set(cr[pr[i]:pr[i + 1]]) == set(c0[p0[i]:p0[i + 1]]) for i in rows)
+            s = oracle.calculate_potential(x, g["q"], g["r"], g["eps"])[0]
+            assert 1e-7 < abs(s - s0) < 1e-3
+    assert reordered > 0
