@@ -411,6 +411,13 @@ typedef struct {
                                   /* the SMs with the shortest tail); NULL:  */
                                   /* system s on CTA s.  Results do not      */
                                   /* depend on it.                           */
+    int32_t launch_systems;       /* > 0 (needs sys_order): only the first   */
+                                  /* launch_systems entries of sys_order get */
+                                  /* CTAs; the other systems do not advance  */
+                                  /* in this launch.  0: every system.  Lets */
+                                  /* the last chains of a run take wider     */
+                                  /* clusters and more teams                 */
+    int32_t pad2;
 } AlmaMCConfig;
 
 /* Per-system chain state, device memory, one per system (72 bytes). */

@@ -778,6 +778,10 @@ extern "C" int alma_mc_run(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *
     if (rc) return rc;
     if (!cfg || !states) return alma_set_error(ALMA_EINVAL, "alma_mc_run: null config/states");
     if (cfg->policy < 0 || cfg->policy > 2) return alma_set_error(ALMA_EINVAL, "alma_mc_run: bad policy");
+    // systems that get CTAs in this launch: the first nl_sys entries of sys_order
+    if (cfg->launch_systems < 0 || cfg->launch_systems > b->nsys || (cfg->launch_systems > 0 && !cfg->sys_order))
+        return alma_set_error(ALMA_EINVAL, "alma_mc_run: launch_systems must be 0..nsys, and > 0 needs sys_order");
+    const int nl_sys = cfg->launch_systems > 0 ? cfg->launch_systems : b->nsys;
     const MoveCtx C = alma_make_move_ctx(b, t, nl, p, scratch);
     MCConfigDev d;
     d.seed = cfg->seed;
@@ -807,7 +811,7 @@ extern "C" int alma_mc_run(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *
         int dev = 0, sms = 148;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        nt = b->nsys <= sms ? 512 : 256;
+        nt = nl_sys <= sms ? 512 : 256;
     }
     const int cl = cfg->cluster_size <= 0 ? 1 : cfg->cluster_size;
     if (nt != 256 && nt != 512) return alma_set_error(ALMA_EINVAL, "alma_mc_run: threads_per_system must be 0, 256 or 512");
@@ -823,11 +827,11 @@ extern "C" int alma_mc_run(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *
         bool fits = true;
 #define ALMA_SPEC_CASE(R, NT)                                                                                   \
     switch (cl) {                                                                                               \
-        case 1: e = launch_mc_spec<R, NT, 1>(C, d, states, step_limit, b->nsys, teams, stride, rounds, st, &fits); break;   \
-        case 2: e = launch_mc_spec<R, NT, 2>(C, d, states, step_limit, b->nsys, teams, stride, rounds, st, &fits); break;   \
-        case 4: e = launch_mc_spec<R, NT, 4>(C, d, states, step_limit, b->nsys, teams, stride, rounds, st, &fits); break;   \
-        case 8: e = launch_mc_spec<R, NT, 8>(C, d, states, step_limit, b->nsys, teams, stride, rounds, st, &fits); break;   \
-        default: e = launch_mc_spec<R, NT, 16>(C, d, states, step_limit, b->nsys, teams, stride, rounds, st, &fits); break; \
+        case 1: e = launch_mc_spec<R, NT, 1>(C, d, states, step_limit, nl_sys, teams, stride, rounds, st, &fits); break;   \
+        case 2: e = launch_mc_spec<R, NT, 2>(C, d, states, step_limit, nl_sys, teams, stride, rounds, st, &fits); break;   \
+        case 4: e = launch_mc_spec<R, NT, 4>(C, d, states, step_limit, nl_sys, teams, stride, rounds, st, &fits); break;   \
+        case 8: e = launch_mc_spec<R, NT, 8>(C, d, states, step_limit, nl_sys, teams, stride, rounds, st, &fits); break;   \
+        default: e = launch_mc_spec<R, NT, 16>(C, d, states, step_limit, nl_sys, teams, stride, rounds, st, &fits); break; \
     }
         if (prec == ALMA_PREC_FP64) {
             if (nt == 512) { ALMA_SPEC_CASE(double, 512) } else { ALMA_SPEC_CASE(double, 256) }
@@ -838,17 +842,22 @@ extern "C" int alma_mc_run(const AlmaBatch *b, const AlmaTopo *t, const AlmaNL *
         if (e != cudaSuccess) return alma_cuda_error(e, "alma_mc_run launch");
         if (!fits)
             return alma_set_error(ALMA_EINVAL, "alma_mc_run: %d systems x %d teams x %d CTAs cannot all be resident",
-                                  b->nsys, teams, cl);
+                                  nl_sys, teams, cl);
         ALMA_LAUNCH_CHECK("alma_mc_run");
+        // In a scratch sized for more teams, the round buffers of a K-team
+        // launch lie over the start of team K's move scratch, whose flags
+        // must read zero between proposals: leave them zeroed, so a later
+        // launch with more teams finds team K clean.
+        ALMA_CUDA_TRY(cudaMemsetAsync(rounds, 0, sizeof(SpecRound) * (size_t)b->nsys, st));
         return ALMA_OK;
     }
 #define ALMA_MC_CASE(R, NT)                                                              \
     switch (cl) {                                                                        \
-        case 1: e = launch_mc<R, NT, 1>(C, d, states, step_limit, b->nsys, st); break;   \
-        case 2: e = launch_mc<R, NT, 2>(C, d, states, step_limit, b->nsys, st); break;   \
-        case 4: e = launch_mc<R, NT, 4>(C, d, states, step_limit, b->nsys, st); break;   \
-        case 8: e = launch_mc<R, NT, 8>(C, d, states, step_limit, b->nsys, st); break;   \
-        default: e = launch_mc<R, NT, 16>(C, d, states, step_limit, b->nsys, st); break; \
+        case 1: e = launch_mc<R, NT, 1>(C, d, states, step_limit, nl_sys, st); break;   \
+        case 2: e = launch_mc<R, NT, 2>(C, d, states, step_limit, nl_sys, st); break;   \
+        case 4: e = launch_mc<R, NT, 4>(C, d, states, step_limit, nl_sys, st); break;   \
+        case 8: e = launch_mc<R, NT, 8>(C, d, states, step_limit, nl_sys, st); break;   \
+        default: e = launch_mc<R, NT, 16>(C, d, states, step_limit, nl_sys, st); break; \
     }
     if (prec == ALMA_PREC_FP64) {
         if (nt == 512) { ALMA_MC_CASE(double, 512) } else { ALMA_MC_CASE(double, 256) }

@@ -74,7 +74,8 @@ class AlmaMCConfig(C.Structure):
                 ("sidechain_mult", C.c_double), ("crank_prob", C.c_double),
                 ("concerted_prob", C.c_double), ("fixed_delta", C.c_double),
                 ("moveset_off", _p), ("moveset", _p), ("threads_per_system", _i32), ("cluster_size", _i32),
-                ("spec_teams", _i32), ("pad", _i32), ("rebuild_ws", _p), ("sys_order", _p)]
+                ("spec_teams", _i32), ("pad", _i32), ("rebuild_ws", _p), ("sys_order", _p),
+                ("launch_systems", _i32), ("pad2", _i32)]
 
 
 class AlmaChainState(C.Structure):

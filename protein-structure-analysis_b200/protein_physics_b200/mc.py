@@ -27,6 +27,7 @@ from .engine import particle_arrays, particles_from
 from .topology import flatten
 
 K_BOLTZMANN = 0.0019872  # kcal mol^-1 K^-1 (temperatures in K -> kcal/mol)
+TAIL_MAX_TEAMS = 4  # speculative teams per chain a tail launch may use (auto_shape's maximum)
 
 
 def mc_config(seed, policy=0, tune_freq=200, max_angle_bounds=(0.004, 0.5), fixed_delta=0.0, moveset=None,
@@ -75,7 +76,8 @@ class MCRunner:
     initial max angle (the reference's max_angle)."""
 
     def __init__(self, batch: DeviceBatch, temperatures, seed, policy=0, cur_max0=0.12, tune_freq=200,
-                 fixed_delta=0.0, moveset=None, cluster_size=None, threads=0, spec_teams=None, device_rebuild=False):
+                 fixed_delta=0.0, moveset=None, cluster_size=None, threads=0, spec_teams=None, device_rebuild=False,
+                 tail_shape=True):
         self.b = batch
         self.L = batch.L
         self._keep = []
@@ -100,10 +102,18 @@ class MCRunner:
             self.rebuild_ws = torch.empty(self.L.alma_mc_rebuild_bytes(batch.natoms, batch.nsys), dtype=torch.uint8,
                                           device="cuda")
             self.cfg.rebuild_ws = _ptr(self.rebuild_ws)
-        if spec_teams > 1:
+        # tail_shape: once at most half the SMs' worth of chains still have
+        # proposals to make before the step limit, those chains alone are
+        # launched, on wider clusters and more teams (auto_shape of their
+        # count), instead of one CTA each beside idle SMs.  The chains are
+        # the same: every shape draws and decides the same proposals.
+        self.tail_shape = bool(tail_shape) and self.rebuild_ws is None and batch.nsys > 1
+        self._sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+        teams_max = max(int(spec_teams), TAIL_MAX_TEAMS if self.tail_shape else 1)
+        if teams_max > 1:
             # K teams per system: K move scratches plus the round buffers, team 0
             # at the start (the batch's counters and single-move calls use it)
-            need = self.L.alma_mc_scratch_bytes(batch.natoms, batch.nsys, int(spec_teams))
+            need = self.L.alma_mc_scratch_bytes(batch.natoms, batch.nsys, teams_max)
             if batch.scratch.numel() < need:
                 batch.scratch = torch.zeros(need, dtype=torch.uint8, device="cuda")
         # largest systems take the first CTAs: when a batch has more systems
@@ -121,6 +131,7 @@ class MCRunner:
         self.states = torch.from_numpy(st.view(np.uint8).copy()).to("cuda")
         self.terms = torch.zeros((batch.nsys, 5), dtype=torch.float64, device="cuda")
         self.rebuilds = 0
+        self.tail_launches = 0
         batch.build_nl()
         self.reset_energy()
 
@@ -134,14 +145,46 @@ class MCRunner:
     def state(self):
         return self.states.cpu().numpy().view(_lib.STATE_DTYPE).copy()
 
-    def launch(self, step_limit):
+    def _run(self, cfg, step_limit):
         b = self.b
-        rc = self.L.alma_mc_run(C.byref(b.batch_s), C.byref(b.topo_s), C.byref(b.nl_s), C.byref(b.params), b.prec,
-                                _ptr(b.scratch), C.byref(self.cfg), _ptr(self.states), int(step_limit), b._sp())
+        return self.L.alma_mc_run(C.byref(b.batch_s), C.byref(b.topo_s), C.byref(b.nl_s), C.byref(b.params), b.prec,
+                                  _ptr(b.scratch), C.byref(cfg), _ptr(self.states), int(step_limit), b._sp())
+
+    def launch(self, step_limit, tail=None):
+        """One persistent launch; tail = (order, n, cluster, teams) from
+        _tail_plan launches only those chains, in that shape."""
+        if tail is not None:
+            order, n, cl, k = tail
+            cfg = _lib.AlmaMCConfig.from_buffer_copy(self.cfg)
+            self._tail_order = _t(order, torch.int32)  # alive until the state read after the launch
+            cfg.sys_order, cfg.launch_systems = _ptr(self._tail_order), int(n)
+            cfg.cluster_size, cfg.spec_teams, cfg.threads_per_system = int(cl), int(k), 512
+            rc = self._run(cfg, step_limit)
+            if rc == _lib.ALMA_EINVAL and k > 1 and b"resident" in self.L.alma_last_error():
+                cfg.spec_teams = 1
+                rc = self._run(cfg, step_limit)
+            _lib.check(rc, "alma_mc_run")
+            self.tail_launches += 1
+            return
+        rc = self._run(self.cfg, step_limit)
         if rc == _lib.ALMA_EINVAL and self.cfg.spec_teams > 1 and b"resident" in self.L.alma_last_error():
             self.cfg.spec_teams = 1  # the teams would not all fit on the GPU at once: one team
             return self.launch(step_limit)
         _lib.check(rc, "alma_mc_run")
+
+    def _tail_plan(self, st, step_limit):
+        """(order, n, cluster, teams) for the chains still short of
+        step_limit, or None when the batch's own shape is the one to use."""
+        if not self.tail_shape:
+            return None
+        active = np.nonzero(st["step"] < step_limit)[0]
+        n = len(active)
+        if n == 0 or 2 * n > self._sms:
+            return None
+        cl, k = auto_shape(n)
+        size = np.diff(self.b.atom_off_h)[active]
+        order = active[np.argsort(-size, kind="stable")].astype(np.int32)
+        return order, n, cl, k
 
     def run(self, nsteps):
         """Advances every system by nsteps proposals (host loop over rebuilds)."""
@@ -162,27 +205,29 @@ class MCRunner:
         h = self._host.numpy()
         return h[:n].view(_lib.STATE_DTYPE).copy(), int(h[n:].view(np.int32)[0])
 
-    def _need_mask(self):
-        """Device-side system mask of the chains whose need_rebuild is set."""
-        off = _lib.STATE_DTYPE.fields["need_rebuild"][1]
-        rows = self.states.view(self.b.nsys, _lib.STATE_DTYPE.itemsize)[:, off:off + 4]
-        return rows.view(torch.int32).reshape(self.b.nsys).ne(0).to(torch.uint8)
-
     def run_to(self, step_limit):
+        tail = None
         while True:
-            self.launch(step_limit)
+            self.launch(step_limit, tail)
             st, status = self._read_state()
-            if self.cfg.spec_teams > 1 and status & _lib.ST_SPEC_ABORT:
+            if status & _lib.ST_SPEC_ABORT:
                 raise RuntimeError("alma_mc_run: a speculative round timed out (teams not co-resident)")
+            # Every drifted chain rebuilds now, also one flagged on its last
+            # proposal: the reference rebuilds at the start of the chain's
+            # next step (physics_engine.cpp:2506-2510), the same list from the
+            # same coordinates, but here the list stays valid for energies
+            # taken after the run (n_rebuild counts it at once).
             need = st["need_rebuild"] != 0
             if need.any():
-                mask = self._need_mask()
+                mask = torch.from_numpy(need.astype(np.uint8)).to(self.states.device)
                 self.b.build_nl(sys_mask=mask)
                 self.reset_energy(sys_mask=mask)
                 self.rebuilds += int(need.sum())
+                tail = self._tail_plan(st, step_limit)
                 continue
             if np.all(st["step"] >= step_limit):
                 return st
+            tail = self._tail_plan(st, step_limit)
 
 
 _TUNED = {}

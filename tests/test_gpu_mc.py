@@ -22,13 +22,13 @@ def _setup(name):
 
 
 def _gpu_run(g, F, nsys, seed, steps, precision="fp64", policy=0, fixed_delta=0.0, moveset=None, T=0.6,
-             cluster_size=None, spec_teams=1, device_rebuild=True, runner=False):
+             cluster_size=None, spec_teams=1, device_rebuild=True, runner=False, tail_shape=True):
     from protein_physics_b200.device import DeviceBatch
     from protein_physics_b200.mc import MCRunner
     b = DeviceBatch([(g["xyz"], g["q"], g["r"], g["eps"], F)] * nsys, precision=precision)
     R = MCRunner(b, T, seed, policy=policy, fixed_delta=fixed_delta,
                  moveset=[moveset] * nsys if moveset is not None else None, cluster_size=cluster_size,
-                 spec_teams=spec_teams, device_rebuild=device_rebuild)
+                 spec_teams=spec_teams, device_rebuild=device_rebuild, tail_shape=tail_shape)
     st = R.run_to(steps)
     return (b, st, R) if runner else (b, st)
 
@@ -150,6 +150,72 @@ def test_spec_teams_bitwise_equal_one_team():
     for k in ("cur_max", "n_accepted", "n_proposed", "n_rebuild", "step"):
         assert st1[k][0] == st4[k][0], k
     assert abs(st1["energy"][0] - st4["energy"][0]) <= 1e-12 * abs(st1["energy"][0])
+
+
+def test_tail_launches_follow_the_oracle():
+    """Once few chains are short of the step limit, MCRunner launches only
+    them, on 16-CTA clusters with speculative teams: every chain is still
+    the oracle's, through many host rebuilds."""
+    g, F = _setup("insulin")
+    n = 12
+    b, st, R = _gpu_run(g, F, n, 7, 120, fixed_delta=0.6, T=50.0, cluster_size=1, spec_teams=1,
+                        device_rebuild=False, runner=True)
+    assert R.tail_launches > 0 and R.rebuilds > 0
+    for s in range(n):
+        x_o, st_o, _ = _oracle_run(g, F, 7, 120, fixed_delta=0.6, T=50.0, sys_index=s)
+        assert st["step"][s] == 120
+        # a chain that drifted on its last proposal is rebuilt when the run
+        # ends; the oracle leaves the flag for the chain's next step
+        assert st["n_rebuild"][s] == st_o["n_rebuild"] + (st_o["need_rebuild"] != 0)
+        assert st["n_accepted"][s] == st_o["n_accepted"]
+        np.testing.assert_allclose(b.coords(s), x_o, rtol=0, atol=1e-8)
+
+
+def test_tail_launches_bitwise_equal_fixed_shape():
+    """Mixed precision, the same batch with and without tail launches: the
+    same decisions and the same coordinates bit for bit.  The running
+    energies agree to 1e-9 relative: kernels of different cluster sizes are
+    separate instantiations, whose FP32 pair arithmetic the compiler may
+    contract differently (an ulp of a pair term)."""
+    g, F = _setup("xq8")
+    kw = dict(precision="mixed", fixed_delta=0.4, T=30.0, cluster_size=1, spec_teams=1, device_rebuild=False)
+    b1, st1, R1 = _gpu_run(g, F, 6, 3, 300, tail_shape=False, runner=True, **kw)
+    b2, st2, R2 = _gpu_run(g, F, 6, 3, 300, tail_shape=True, runner=True, **kw)
+    assert R1.tail_launches == 0 < R2.tail_launches
+    for s in range(6):
+        assert np.array_equal(b1.coords(s), b2.coords(s)), s
+        for k in ("cur_max", "n_accepted", "n_proposed", "n_rebuild", "step"):
+            assert st1[k][s] == st2[k][s], (s, k)
+        assert abs(st1["energy"][s] - st2["energy"][s]) <= 1e-9 * abs(st1["energy"][s])
+
+
+def test_team_counts_mixed_on_one_scratch():
+    """A 2-team run, then a 4-team run on the same batch scratch (sized for
+    four teams): the 2-team launches' round buffers lie over team 2's move
+    scratch and are left zeroed, so the 4-team run is the oracle's chain."""
+    from protein_physics_b200.device import DeviceBatch
+    from protein_physics_b200.mc import MCRunner
+    from oracle import Oracle, oracle_mc
+    g, F = _setup("insulin")
+    b = DeviceBatch([(g["xyz"], g["q"], g["r"], g["eps"], F)], precision="fp64")
+    MCRunner(b, 0.6, 5, cluster_size=8, spec_teams=2).run_to(60)
+    x_mid = b.coords(0).copy()
+    R = MCRunner(b, 0.6, 9, cluster_size=8, spec_teams=4)
+    st = R.run_to(150)
+    x_o, st_o, _ = oracle_mc(Oracle(), F, x_mid, g["q"], g["r"], g["eps"], 9, 150, temperature=0.6)
+    assert st["n_accepted"][0] == st_o["n_accepted"]
+    np.testing.assert_allclose(b.coords(0), x_o, rtol=0, atol=1e-9)
+
+
+def test_launch_systems_rejects_bad_counts():
+    from protein_physics_b200 import _lib
+    g, F = _setup("insulin")
+    b, st, R = _gpu_run(g, F, 2, 1, 1, cluster_size=1, spec_teams=1, device_rebuild=False, runner=True)
+    cfg = _lib.AlmaMCConfig.from_buffer_copy(R.cfg)
+    cfg.launch_systems = 3  # more than the batch holds
+    assert R._run(cfg, 2) == _lib.ALMA_EINVAL
+    cfg.launch_systems, cfg.sys_order = 1, None  # a count needs an order
+    assert R._run(cfg, 2) == _lib.ALMA_EINVAL
 
 
 # ---- rebuilds inside the persistent kernel ----------------------------------
