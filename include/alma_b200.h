@@ -116,7 +116,24 @@ typedef struct {
     int32_t ncsp;
     const int32_t *csp_off;   /* [nsys+1] concerted sidechain pairs         */
     const int32_t *csp;       /* [ncsp*2]                                   */
+    const uint32_t *excl_win; /* optional [4*natoms] exclusion windows from */
+                              /* alma_excl_window (the list build then tests */
+                              /* one bit per pair instead of searching the  */
+                              /* CSR rows); NULL: CSR search                 */
 } AlmaTopo;
+
+/* Exclusion window of every atom from the CSR exclusions (excl_ptr,
+ * excl_cols: rows of j > i, global atom indices): win[4*i .. 4*i+3] is a
+ * 128-bit mask whose bit d + 64 is set when atoms i and i + d are excluded
+ * (0 < |d| < 64); bit 64 (d = 0) is set when atom i has an exclusion
+ * partner outside the window, which the CSR rows then decide; bit 0 is
+ * unused.
+ * Fills win (device, 16 bytes per atom) on `stream`.  Exclusions depend on
+ * the topology only: build once, point AlmaTopo.excl_win at it.  Replaces
+ * the per-pair search of BondTopology::is_excluded (physics_engine.cpp:
+ * 1700-1705) in the list build; the exclusion flags are the same. */
+int alma_excl_window(const int64_t *excl_ptr, const int32_t *excl_cols, int32_t natoms, uint32_t *win,
+                     void *stream);
 
 /* Neighbor list: for every atom a full row (all j != i with r² < 14²) and
  * a half row (j > i), both in the reference's cell-scan order

@@ -275,7 +275,7 @@ __device__ bool team_rebuild(const MoveCtx &C, const MCConfigDev &cfg, int s, co
     for (int i = a0 + wid; i < a1; i += nw) {
         int nf, nh, nsf, nsh;
         nl_row_atom<0>(i, lane, g, b.xyz, rcut2, ws.cell_of, ws.cstart, ws.cell_atoms, b.prm64, cfg.reach_pad, ep, ec,
-                       nl, nf, nh, nsf, nsh);
+                       C.t.excl_win, nl, nf, nh, nsf, nsh);
         if (lane == 0) {
             ws.cnt[i] = nf;
             ws.cnt[(size_t)NA + i] = nh;
@@ -316,7 +316,7 @@ __device__ bool team_rebuild(const MoveCtx &C, const MCConfigDev &cfg, int s, co
     for (int i = a0 + wid; i < a1; i += nw) {
         int nf, nh, nsf, nsh;
         nl_row_atom<1>(i, lane, g, b.xyz, rcut2, ws.cell_of, ws.cstart, ws.cell_atoms, b.prm64, cfg.reach_pad, ep, ec,
-                       nl, nf, nh, nsf, nsh);
+                       C.t.excl_win, nl, nf, nh, nsf, nsh);
     }
     T.sync();
     for (int i = a0 + wid; i < a1; i += nw)

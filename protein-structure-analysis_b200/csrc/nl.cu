@@ -240,8 +240,8 @@ nl_rows_onepass_kernel(const int32_t *__restrict__ atom_off, int nsys, int natom
                        const int32_t *__restrict__ ok, const int32_t *__restrict__ cell_of,
                        const int64_t *__restrict__ cell_start, const int32_t *__restrict__ cell_atoms,
                        const float4 *__restrict__ cell_pos, const double *__restrict__ prm64, double reach_pad,
-                       const int64_t *__restrict__ excl_ptr, const int32_t *__restrict__ excl_cols, AlmaNL nl,
-                       int64_t *__restrict__ cursor) {
+                       const int64_t *__restrict__ excl_ptr, const int32_t *__restrict__ excl_cols,
+                       const uint32_t *__restrict__ excl_win, AlmaNL nl, int64_t *__restrict__ cursor) {
     extern __shared__ uint32_t nl_stage_smem[];
     const int warps_per_block = blockDim.x >> 5;
     const int i = blockIdx.x * warps_per_block + (threadIdx.x >> 5);
@@ -256,6 +256,7 @@ nl_rows_onepass_kernel(const int32_t *__restrict__ atom_off, int nsys, int natom
     const int cx = c % g.nx, cy = (c / g.nx) % g.ny, cz = c / (g.nx * g.ny);
     const double4 pi = ld_xyz(xyz, i);
     const double ri_pad = shorts ? prm64[4 * (size_t)i + 1] + reach_pad : 0.0;
+    const uint4 ew = excl_window_of(excl_win, i);
     // the FP32 frame of the cell copy; r² within margin2 of a cutoff is
     // decided in FP64, so the rows are those of the FP64 test bit for bit
     const float pfx = (float)(pi.x - g.xlo), pfy = (float)(pi.y - g.ylo), pfz = (float)(pi.z - g.zlo);
@@ -310,7 +311,8 @@ nl_rows_onepass_kernel(const int32_t *__restrict__ atom_off, int nsys, int natom
                         jmin = min(jmin, j);
                         jmax = max(jmax, j);
                         if (at < NL_STAGE)
-                            stage[at] = (uint32_t)j | (excluded(excl_ptr, excl_cols, i, j) ? ALMA_EXCL_BIT : 0u) |
+                            stage[at] = (uint32_t)j |
+                                        (excluded_w(excl_win, ew, excl_ptr, excl_cols, i, j) ? ALMA_EXCL_BIT : 0u) |
                                         (sh ? NL_SHORT_BIT : 0u);
                     }
                     // the other row kinds are counted from the stage after the
@@ -368,7 +370,7 @@ nl_rows_onepass_kernel(const int32_t *__restrict__ atom_off, int nsys, int natom
         __syncwarp();
         int a, bb, cc, dd;
         nl_row_atom<1>(i, lane, g, xyz, rcut2, cell_of, cell_start, cell_atoms, prm64, reach_pad, excl_ptr, excl_cols,
-                       nl, a, bb, cc, dd);
+                       excl_win, nl, a, bb, cc, dd);
         return;
     }
     __syncwarp();
@@ -423,9 +425,43 @@ __global__ void nl_finalize_kernel(int nsys, const uint8_t *__restrict__ mask, c
     if (!fits) set_status(status, ALMA_ST_NL_OVERFLOW);
 }
 
+// Exclusion windows (alma_excl_window): thread per atom over its CSR row
+// (partners j > i); each pair sets its bit in both atoms' windows, or the
+// far flag (bit 64) of both when j - i >= EXCL_WIN.
+__global__ void excl_window_kernel(const int64_t *__restrict__ excl_ptr, const int32_t *__restrict__ excl_cols,
+                                   int natoms, uint32_t *__restrict__ win) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= natoms) return;
+    for (int64_t k = excl_ptr[i]; k < excl_ptr[i + 1]; ++k) {
+        const int j = excl_cols[k];
+        if (j < 0 || j >= natoms || j == i) continue;
+        const int d = j - i;
+        if (d > -EXCL_WIN && d < EXCL_WIN) {
+            const unsigned bi = (unsigned)(d + EXCL_WIN), bj = (unsigned)(EXCL_WIN - d);
+            atomicOr(&win[4 * (size_t)i + (bi >> 5)], 1u << (bi & 31u));
+            atomicOr(&win[4 * (size_t)j + (bj >> 5)], 1u << (bj & 31u));
+        } else {
+            atomicOr(&win[4 * (size_t)i + 2], 1u);
+            atomicOr(&win[4 * (size_t)j + 2], 1u);
+        }
+    }
+}
+
 }  // namespace alma
 
 using namespace alma;
+
+extern "C" int alma_excl_window(const int64_t *excl_ptr, const int32_t *excl_cols, int32_t natoms, uint32_t *win,
+                                void *stream) {
+    if (natoms < 0 || (natoms > 0 && (!excl_ptr || !excl_cols || !win)))
+        return alma_set_error(ALMA_EINVAL, "alma_excl_window: bad arguments");
+    if (natoms == 0) return ALMA_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    ALMA_CUDA_TRY(cudaMemsetAsync(win, 0, sizeof(uint32_t) * 4 * (size_t)natoms, st));
+    excl_window_kernel<<<(natoms + 255) / 256, 256, 0, st>>>(excl_ptr, excl_cols, natoms, win);
+    ALMA_LAUNCH_CHECK("alma_excl_window");
+    return ALMA_OK;
+}
 
 extern "C" size_t alma_nl_workspace_bytes(int32_t nsys, int32_t natoms, int64_t max_cells) {
     return carve(nullptr, nullptr, nsys, natoms, max_cells);
@@ -475,10 +511,11 @@ extern "C" int alma_nl_build(const AlmaBatch *b, const AlmaTopo *t, AlmaNL *nl, 
     const int wpb = 8, rb = (natoms + wpb - 1) / wpb;
     const int64_t *ep = t ? t->excl_ptr : nullptr;
     const int32_t *ec = t ? t->excl_cols : nullptr;
+    const uint32_t *ew = t && t->excl_ptr ? t->excl_win : nullptr;
     ALMA_CUDA_TRY(cudaMemsetAsync(w.cursor, 0, sizeof(int64_t) * 4 * (size_t)nsys, st));
     nl_rows_onepass_kernel<<<rb, wpb * 32, sizeof(uint32_t) * NL_STAGE * wpb, st>>>(
         b->atom_off, nsys, natoms, sys_mask, b->xyz, rcut2, w.grid, w.ok, w.cell_of, w.cell_start, w.cell_atoms,
-        w.cell_pos, b->prm64, reach_pad, ep, ec, *nl, w.cursor);
+        w.cell_pos, b->prm64, reach_pad, ep, ec, ew, *nl, w.cursor);
     nl_finalize_kernel<<<(nsys + 255) / 256, 256, 0, st>>>(nsys, sys_mask, w.ok, w.cursor, *nl, b->status);
     ALMA_LAUNCH_CHECK_N("alma_nl_build", 11);
     return ALMA_OK;

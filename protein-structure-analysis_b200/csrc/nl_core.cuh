@@ -64,6 +64,30 @@ __device__ __forceinline__ bool excluded(const int64_t *__restrict__ excl_ptr, c
     return lo < excl_ptr[lo_i + 1] && excl_cols[lo] == hi_j;
 }
 
+// Exclusion window (alma_excl_window): bit d + 64 of atom i's 128-bit word
+// marks i and i + d as excluded, |d| < 64; bit 64 (d = 0, never a pair)
+// marks an exclusion partner outside the window (bit 0 stays unused).  Bonded exclusions
+// lie within a few residues, so nearly every pair is decided by one bit of
+// a word the warp loaded once; only atoms with a far partner (disulfides)
+// search their CSR row for pairs outside the window.
+constexpr int EXCL_WIN = 64;
+
+__device__ __forceinline__ uint4 excl_window_of(const uint32_t *__restrict__ win, int i) {
+    return win ? __ldg(reinterpret_cast<const uint4 *>(win) + i) : make_uint4(0u, 0u, 0u, 0u);
+}
+
+__device__ __forceinline__ bool excluded_w(const uint32_t *win, uint4 w, const int64_t *__restrict__ excl_ptr,
+                                           const int32_t *__restrict__ excl_cols, int i, int j) {
+    if (!win) return excluded(excl_ptr, excl_cols, i, j);
+    const int d = j - i;
+    if (d > -EXCL_WIN && d < EXCL_WIN) {
+        const unsigned b = (unsigned)(d + EXCL_WIN);
+        const uint32_t word = b < 64u ? (b < 32u ? w.x : w.y) : (b < 96u ? w.z : w.w);
+        return (word >> (b & 31u)) & 1u;
+    }
+    return (w.z & 1u) && excluded(excl_ptr, excl_cols, i, j);
+}
+
 // The rows of atom i, one warp (27 cells in (dz, dy, dx) order, ascending
 // atoms per cell, ballot-compacted).  PASS 0 counts (full, half, short full,
 // short half); PASS 1 writes the rows at the list's pointers and ref_xyz.
@@ -74,9 +98,10 @@ __device__ __forceinline__ void nl_row_atom(int i, int lane, const SysGrid &g, c
                                             const int64_t *__restrict__ cell_start,
                                             const int32_t *__restrict__ cell_atoms, const double *__restrict__ prm64,
                                             double reach_pad, const int64_t *__restrict__ excl_ptr,
-                                            const int32_t *__restrict__ excl_cols, const AlmaNL &nl, int &nfull,
-                                            int &nhalf, int &nsfull, int &nshalf) {
+                                            const int32_t *__restrict__ excl_cols, const uint32_t *excl_win,
+                                            const AlmaNL &nl, int &nfull, int &nhalf, int &nsfull, int &nshalf) {
     const int c = cell_of[i];
+    const uint4 ew = excl_window_of(excl_win, i);
     const int cx = c % g.nx, cy = (c / g.nx) % g.ny, cz = c / (g.nx * g.ny);
     const double4 pi = ld_xyz(xyz, i);
     const bool shorts = nl.sfull_cols != nullptr;
@@ -125,7 +150,8 @@ __device__ __forceinline__ void nl_row_atom(int i, int lane, const SysGrid &g, c
                         jmin = min(jmin, j);
                         jmax = max(jmax, j);
                         const unsigned lt = (1u << lane) - 1u;
-                        const uint32_t e = (uint32_t)j | (excluded(excl_ptr, excl_cols, i, j) ? ALMA_EXCL_BIT : 0u);
+                        const uint32_t e =
+                            (uint32_t)j | (excluded_w(excl_win, ew, excl_ptr, excl_cols, i, j) ? ALMA_EXCL_BIT : 0u);
                         nl.full_cols[fo + nfull + __popc(mf & lt)] = e;
                         if (j > i) nl.half_cols[ho + nhalf + __popc(mh & lt)] = e;
                         if (sh) {

@@ -54,7 +54,7 @@ class AlmaTopo(C.Structure):
                 ("term_n", _p), ("term_gamma", _p),
                 ("nss", _i32), ("ss_off", _p), ("ss_ij", _p),
                 ("ncp", _i32), ("cp_off", _p), ("cp", _p),
-                ("ncsp", _i32), ("csp_off", _p), ("csp", _p)]
+                ("ncsp", _i32), ("csp_off", _p), ("csp", _p), ("excl_win", _p)]
 
 
 class AlmaNL(C.Structure):
@@ -143,6 +143,7 @@ def lib():
     L.alma_topo_sides.argtypes = [_i32, _p, _p, _i32, _p, _p, _p, _i64]
     L.alma_topo_sides_compact.argtypes = [_i32, _p, _p, _i32, _p, _p, _p, _p, _p, _p, _i64]
     L.alma_nl_build.argtypes = [_p, _p, _p, _p, _p, _p, _i64, _p]
+    L.alma_excl_window.argtypes = [_p, _p, _i32, _p, _p]
     L.alma_born_radii.argtypes = [_p, _p, _p, C.c_int, _p, _p]
     L.alma_energy.argtypes = [_p, _p, _p, _p, C.c_int, _p, _p, _p, _p]
     L.alma_forces_workspace_bytes.restype = C.c_size_t

@@ -180,6 +180,12 @@ class DeviceBatch:
         self.topos = topos
         tp = _lib.AlmaTopo()
         tp.excl_ptr, tp.excl_cols = _ptr(self.t_excl_ptr), _ptr(self.t_excl_cols)
+        # per-atom exclusion windows: the list build tests one bit per pair
+        self.t_excl_win = torch.zeros(4 * max(self.natoms, 1), dtype=torch.int32, device=_DEV)
+        if self.t_excl_cols.numel() > 0:
+            _lib.check(self.L.alma_excl_window(_ptr(self.t_excl_ptr), _ptr(self.t_excl_cols), self.natoms,
+                                               _ptr(self.t_excl_win), self._sp()), "alma_excl_window")
+        tp.excl_win = _ptr(self.t_excl_win)  # all zero without exclusions: no pair excluded
         tp.nrb, tp.rb_off, tp.rb_ij = int(rb_off[-1]), _ptr(self.t_rb_off), _ptr(self.t_rb_ij)
         tp.rb_kind, tp.rb_scale = _ptr(self.t_rb_kind), _ptr(self.t_rb_scale)
         tp.side_ptr, tp.side_idx = _ptr(self.t_side_ptr), _ptr(self.t_side_idx)
