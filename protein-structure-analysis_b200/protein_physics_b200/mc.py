@@ -59,11 +59,12 @@ def mc_config(seed, policy=0, tune_freq=200, max_angle_bounds=(0.004, 0.5), fixe
     return cfg
 
 
-def auto_shape(nsys):
+def auto_shape(nsys, sms=None):
     """(cluster size, speculative teams) MCRunner picks for nsys systems:
     the largest cluster with every system on its own SMs, then up to four
-    teams per system while the SMs last."""
-    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    teams per system while the SMs last (sms: the device's SM count)."""
+    if sms is None:
+        sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
     cl = next((c for c in (16, 8, 4, 2) if nsys * c <= sms), 1)
     k = next(k for k in (4, 2, 1) if k == 1 or k * nsys * cl <= sms)
     return cl, k
@@ -181,7 +182,7 @@ class MCRunner:
         n = len(active)
         if n == 0 or 2 * n > self._sms:
             return None
-        cl, k = auto_shape(n)
+        cl, k = auto_shape(n, self._sms)
         size = np.diff(self.b.atom_off_h)[active]
         order = active[np.argsort(-size, kind="stable")].astype(np.int32)
         return order, n, cl, k

@@ -84,6 +84,24 @@ def oracle():
     return Oracle()
 
 
+def excl_window_np(ptr, cols, n):
+    """Exclusion windows (alma_excl_window) restated from CSR rows of
+    partners j > i: bit d + 64 of atom i's four words for 0 < |d| < 64, bit
+    64 for a partner farther away."""
+    w = np.zeros((n, 4), np.uint32)
+    for i in range(n):
+        for j in cols[ptr[i]:ptr[i + 1]].tolist():
+            d = j - i
+            if 0 < abs(d) < 64:
+                for a, dd in ((i, d), (j, -d)):
+                    bit = dd + 64
+                    w[a, bit >> 5] |= np.uint32(1 << (bit & 31))
+            else:
+                w[i, 2] |= np.uint32(1)
+                w[j, 2] |= np.uint32(1)
+    return w
+
+
 def gpu_available():
     try:
         import torch

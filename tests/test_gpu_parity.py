@@ -298,29 +298,14 @@ def test_nl_overflow_regrows_and_rebuilds(oracle):
     assert np.array_equal(rp, ptr) and np.array_equal(cols, ocols)
 
 
-def _window_np(ptr, cols, n):
-    """The exclusion windows restated from the CSR rows (j > i)."""
-    w = np.zeros((n, 4), np.uint32)
-    for i in range(n):
-        for j in cols[ptr[i]:ptr[i + 1]].tolist():
-            d = j - i
-            if 0 < abs(d) < 64:
-                for a, dd in ((i, d), (j, -d)):
-                    bit = dd + 64
-                    w[a, bit >> 5] |= np.uint32(1 << (bit & 31))
-            else:
-                w[i, 2] |= np.uint32(1)
-                w[j, 2] |= np.uint32(1)
-    return w
-
-
 def test_exclusion_window(golden):
     """alma_excl_window against its restatement from the CSR rows, and the
     list rows with the windows equal to those of the per-pair CSR search,
     flags and order included (insulin's disulfides take the far path)."""
+    from conftest import excl_window_np
     from protein_physics_b200.device import _ptr
     b = _batch(golden)
-    ref = _window_np(b.t_excl_ptr.cpu().numpy(), b.t_excl_cols.cpu().numpy(), b.natoms)
+    ref = excl_window_np(b.t_excl_ptr.cpu().numpy(), b.t_excl_cols.cpu().numpy(), b.natoms)
     got = b.t_excl_win.cpu().numpy().view(np.uint32).reshape(-1, 4)[:b.natoms]
     assert np.array_equal(got, ref)
     if len(golden.d["ss_in"]):

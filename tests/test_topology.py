@@ -115,3 +115,25 @@ def test_flatten_cache_follows_mutations(golden):
     assert c is not b and len(c.conc_sc) == len(T.concerted_sidechain_pairs)
     T.build(golden.resnames[:10], golden.atomnames[:10], golden.res_idx[:10])
     assert flatten(T).n == 10
+
+
+def test_exclusion_windows_restate_is_excluded(golden):
+    """The exclusion windows the list build reads (restated from the flat
+    CSR rows) give BondTopology.is_excluded for every pair within 63
+    indices, and flag exactly the atoms with a partner farther away."""
+    from conftest import excl_window_np
+    from protein_physics_b200.topology import flatten
+    T = golden.topology()
+    F = flatten(T)
+    w = excl_window_np(F.excl_ptr, F.excl_cols, F.n)
+    bits = np.unpackbits(w.view(np.uint8).reshape(F.n, 16), axis=1, bitorder="little")
+    for i in range(F.n):
+        for d in range(-63, 64):
+            j = i + d
+            if d == 0 or not 0 <= j < F.n:
+                assert d == 0 or bits[i, d + 64] == 0
+                continue
+            assert bits[i, d + 64] == int(T.is_excluded(i, j)), (i, j)
+        far = any(T.is_excluded(i, j) for j in range(F.n) if abs(j - i) >= 64)
+        assert bits[i, 64] == int(far), i
+        assert bits[i, 0] == 0
