@@ -175,12 +175,14 @@ class MCRunner:
 
     def _tail_plan(self, st, step_limit):
         """(order, n, cluster, teams) for the chains still short of
-        step_limit, or None when the batch's own shape is the one to use."""
+        step_limit, or None when the batch's own shape is the one to use:
+        while every chain is left (the shape the caller or the autotuner
+        chose for the batch) or more than half the SMs' worth."""
         if not self.tail_shape:
             return None
         active = np.nonzero(st["step"] < step_limit)[0]
         n = len(active)
-        if n == 0 or 2 * n > self._sms:
+        if n == 0 or n == len(st) or 2 * n > self._sms:
             return None
         cl, k = auto_shape(n, self._sms)
         size = np.diff(self.b.atom_off_h)[active]

@@ -58,3 +58,13 @@ def test_tail_plan_keeps_the_batch_shape_while_the_sms_are_busy():
     assert MCRunner._tail_plan(R, _states(steps), 100)[1:] == (74, 2, 1)
     assert MCRunner._tail_plan(R, _states(np.full(256, 100)), 100) is None  # none left
     assert MCRunner._tail_plan(_runner(sizes, tail_shape=False), _states(steps), 100) is None
+
+
+def test_tail_plan_leaves_a_small_batch_its_own_shape_until_a_chain_is_done():
+    sizes = np.full(16, 65000)
+    R = _runner(sizes)
+    assert MCRunner._tail_plan(R, _states(np.full(16, 40)), 100) is None  # the caller's / the tuner's shape
+    steps = np.full(16, 40)
+    steps[3] = 100
+    assert MCRunner._tail_plan(R, _states(steps), 100)[1:] == (15,) + auto_shape(15, 148)
+
