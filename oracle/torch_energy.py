@@ -130,9 +130,9 @@ class TorchEnergy:
             phi = _dihedral(x, *[torch.from_numpy(abcd[:, k]) for k in range(4)])
             off = np.asarray(f.term_off, np.int64)
             rec = torch.from_numpy(np.repeat(np.arange(len(abcd)), np.diff(off)))
-            v2 = torch.as_tensor(np.asarray(f.term_v2, np.float64))
-            nn = torch.as_tensor(np.asarray(f.term_n, np.float64))
-            gm = torch.as_tensor(np.asarray(f.term_gamma, np.float64))
+            v2 = torch.tensor(np.asarray(f.term_v2, np.float64))  # copies: the topology's arrays are read-only
+            nn = torch.tensor(np.asarray(f.term_n, np.float64))
+            gm = torch.tensor(np.asarray(f.term_gamma, np.float64))
             E = (v2 * (1.0 + torch.cos(nn * phi[rec] - gm))).sum()
         ss = np.asarray(f.ss, np.int64).reshape(-1, 2)
         Ess = x.new_zeros(())

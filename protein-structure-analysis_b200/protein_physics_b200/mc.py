@@ -74,7 +74,10 @@ class MCRunner:
     """Device MC over every system of `batch`.
 
     temperatures: kcal/mol, one per system (scalar broadcast).  cur_max0:
-    initial max angle (the reference's max_angle)."""
+    initial max angle (the reference's max_angle).  cluster_size, threads,
+    spec_teams: the launch shape (None / 0: chosen from the batch size).
+    tail_shape: once some chain has finished and few are left, launch only
+    those, on wider clusters and more teams (same chains, fewer idle SMs)."""
 
     def __init__(self, batch: DeviceBatch, temperatures, seed, policy=0, cur_max0=0.12, tune_freq=200,
                  fixed_delta=0.0, moveset=None, cluster_size=None, threads=0, spec_teams=None, device_rebuild=False,
