@@ -46,6 +46,11 @@ def test_errors_are_reported():
     assert b"alma_nl_build" in L.alma_last_error()
     with pytest.raises(ValueError):
         _lib.check(rc, "x")
+    # exclusion windows: arguments are checked before any device work
+    assert L.alma_excl_window(None, None, -1, None, None) == _lib.ALMA_EINVAL
+    assert L.alma_excl_window(None, None, 5, None, None) == _lib.ALMA_EINVAL
+    assert b"alma_excl_window" in L.alma_last_error()
+    assert L.alma_excl_window(None, None, 0, None, None) == _lib.ALMA_OK  # nothing to do
 
 
 def test_topo_sides_dfs_order():
